@@ -1,0 +1,86 @@
+// extern "C" entry points of libb2tomo and the per-thread error state.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "arith.h"
+#include "b2t_internal.h"
+#include "proj3d.h"
+
+namespace b2t {
+
+static thread_local std::string g_last_error;
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launches(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+
+b2t_status fail(b2t_status st, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+void clear_error() { g_last_error.clear(); }
+
+b2t_status cuda_fail(cudaError_t e, const char *where)
+{
+    const b2t_status st = (e == cudaErrorMemoryAllocation) ? B2T_ERR_NO_MEMORY : B2T_ERR_CUDA;
+    return fail(st, "%s: %s (%s)", where, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+}  // namespace b2t
+
+using namespace b2t;
+
+extern "C" {
+
+const char *b2t_last_error(void) { return g_last_error.c_str(); }
+
+int32_t b2t_version(void) { return 100; }
+
+uint64_t b2t_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+b2t_status b2t_set_device(int32_t device)
+{
+    clear_error();
+    B2T_CUDA_TRY(cudaSetDevice(device), "b2t_set_device");
+    return B2T_OK;
+}
+
+b2t_status b2t_fp3d(const b2t_geom3d *geom, const b2t_params3d *params, const void *vol, size_t vol_pitch,
+                    void *proj, size_t proj_pitch, int32_t dtype, int32_t mode, void *stream)
+{
+    clear_error();
+    return fp3d_impl(geom, params, vol, vol_pitch, proj, proj_pitch, dtype, mode,
+                     static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_bp3d(const b2t_geom3d *geom, const b2t_params3d *params, const void *proj, size_t proj_pitch,
+                    void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, void *stream)
+{
+    clear_error();
+    return bp3d_impl(geom, params, proj, proj_pitch, vol, vol_pitch, dtype, mode,
+                     static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_vec_op(int32_t op, float *out, const float *a, const float *b, float s, size_t n, void *stream)
+{
+    clear_error();
+    return vec_op_impl(op, out, a, b, s, n, static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_dot_f64(const void *a, const void *b, size_t n, int32_t dtype, double *result, void *stream)
+{
+    clear_error();
+    return dot_impl(a, b, n, dtype, result, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

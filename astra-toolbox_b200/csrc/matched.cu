@@ -1,0 +1,277 @@
+// Exact adjoint of the forward projector (projection kernel "matched_bp").
+//
+// The reference has a matched backprojector only for cyl_cone_vec
+// (cuda/3d/cone_cyl.cu:309-470, dispatched in cuda/3d/mem3d.cu:463-479): each
+// ray scatters its value back along the samples its forward projector read,
+// with atomic adds.  This module provides the same construction for the
+// flat-panel cone and parallel geometries: the transpose of fp3d_kernel,
+// sample for sample, so <A x, y> = <x, A^T y> holds to rounding.
+//
+// Layout: each marching direction scatters into a zero-padded FP32
+// accumulation volume with the same layout its forward pass reads (xyz copy
+// for y/z-major views, zxy copy for x-major views); a final pass drops the
+// padding, folds the two accumulators and applies SET/ADD.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "b2t_internal.h"
+#include "proj3d.h"
+
+namespace b2t {
+
+namespace {
+
+template <typename T> __device__ __forceinline__ float ldm(const T *p);
+template <> __device__ __forceinline__ float ldm<float>(const float *p) { return __ldg(p); }
+template <> __device__ __forceinline__ float ldm<__half>(const __half *p) { return __half2float(__ldg(p)); }
+template <> __device__ __forceinline__ float ldm<__nv_bfloat16>(const __nv_bfloat16 *p)
+{
+    return __bfloat162float(__ldg(p));
+}
+template <typename T> __device__ __forceinline__ float ldm_plain(const T *p);
+template <> __device__ __forceinline__ float ldm_plain<float>(const float *p) { return *p; }
+template <> __device__ __forceinline__ float ldm_plain<__half>(const __half *p) { return __half2float(*p); }
+template <> __device__ __forceinline__ float ldm_plain<__nv_bfloat16>(const __nv_bfloat16 *p)
+{
+    return __bfloat162float(*p);
+}
+template <typename T> __device__ __forceinline__ T tom(float v);
+template <> __device__ __forceinline__ float tom<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half tom<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 tom<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+__device__ __forceinline__ void split_texel_m(float qm, int &k, float &f)
+{
+    const float M = 12582912.0f;
+    float t = __fadd_rn(qm, M);
+    float r = __fadd_rn(t, -M);
+    k = __float_as_int(t) - 0x4B400000;
+    f = __fadd_rn(__fadd_rn(qm, -r), 0.5f);
+}
+
+__device__ __forceinline__ void clip_slices_m(float A, float B, float lo, float hi, float &smin, float &smax)
+{
+    if (fabsf(A) < 1e-12f) {
+        if (!(B >= lo && B <= hi)) {
+            smin = 1.0f;
+            smax = 0.0f;
+        }
+        return;
+    }
+    float s1 = (lo - B) / A, s2 = (hi - B) / A;
+    smin = fmaxf(smin, fminf(s1, s2));
+    smax = fminf(smax, fmaxf(s1, s2));
+}
+
+__device__ __forceinline__ bool texel_ok_m(float A, float B, int s, int n)
+{
+    int k;
+    float f;
+    split_texel_m(fmaf(A, (float)s, B), k, f);
+    return k >= -2 && k <= n;
+}
+
+// Transpose of fp3d_kernel: L.vol is the FP32 padded accumulator (written),
+// L.proj the input projections.  Same ray set-up, same slice range, same
+// weights; the four bilinear taps are scattered with atomic adds.
+template <typename T>
+__global__ void __launch_bounds__(256) fp3d_transpose_kernel(const __grid_constant__ FPLaunch L)
+{
+    const FPView &V = L.views[blockIdx.x];
+    const int u = blockIdx.y * 32 + threadIdx.x;
+    const int v = blockIdx.z * 8 + threadIdx.y;
+    if (u >= L.nu || v >= L.nv) return;
+    float *acc = const_cast<float *>(static_cast<const float *>(L.vol));
+    const T *pin = static_cast<const T *>(L.proj) + ((size_t)v * L.na + V.a) * L.proj_pitch + u;
+    float val = ldm(pin);
+    if (val == 0.0f) return;
+    const int R = L.rays;
+    if (R > 1) val /= (float)(R * R);
+    const long long st0 = L.st0, st2 = L.st2;
+    const float n0 = (float)L.n0;
+    for (int iu = 0; iu < R; ++iu) {
+        for (int iv = 0; iv < R; ++iv) {
+            float uu = (float)u + 0.5f - 0.5f * (float)L.nu;
+            float vv = (float)v + 0.5f - 0.5f * (float)L.nv;
+            if (R > 1) {
+                uu += -0.5f + (0.5f + (float)iu) / (float)R;
+                vv += -0.5f + (0.5f + (float)iv) / (float)R;
+            }
+            const float den = fmaf(vv, V.e[2], fmaf(uu, V.e[1], V.e[0]));
+            const float inv = 1.0f / den;
+            const float A1 = fmaf(vv, V.m1[2], fmaf(uu, V.m1[1], V.m1[0])) * inv;
+            const float A2 = fmaf(vv, V.m2[2], fmaf(uu, V.m2[1], V.m2[0])) * inv;
+            const float B1 = fmaf(vv, V.n1[2], fmaf(uu, V.n1[1], V.n1[0])) * inv;
+            const float B2 = fmaf(vv, V.n2[2], fmaf(uu, V.n2[1], V.n2[0])) * inv;
+            float smin = 0.0f, smax = n0 - 1.0f;
+            clip_slices_m(A1, B1, -1.6f, (float)L.n1 - 0.4f, smin, smax);
+            clip_slices_m(A2, B2, -1.6f, (float)L.n2 - 0.4f, smin, smax);
+            int s_lo = max(0, (int)ceilf(fmaxf(smin, -1.0f)));
+            int s_hi = min(L.n0 - 1, (int)floorf(fminf(smax, n0)));
+            for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
+                if (texel_ok_m(A1, B1, s_lo, L.n1) && texel_ok_m(A2, B2, s_lo, L.n2)) break;
+                ++s_lo;
+            }
+            for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
+                if (texel_ok_m(A1, B1, s_hi, L.n1) && texel_ok_m(A2, B2, s_hi, L.n2)) break;
+                --s_hi;
+            }
+            if (!(texel_ok_m(A1, B1, s_lo, L.n1) && texel_ok_m(A2, B2, s_lo, L.n2) &&
+                  texel_ok_m(A1, B1, s_hi, L.n1) && texel_ok_m(A2, B2, s_hi, L.n2)))
+                s_hi = s_lo - 1;
+            const float sc = sqrtf(fmaf(A1 * A1, L.f1, fmaf(A2 * A2, L.f2, 1.0f))) * L.mul;
+            const float w = val * sc;
+            for (int s = s_lo; s <= s_hi; ++s) {
+                int k1, k2;
+                float f1, f2;
+                split_texel_m(fmaf(A1, (float)s, B1), k1, f1);
+                split_texel_m(fmaf(A2, (float)s, B2), k2, f2);
+                float *p = acc + (long long)s * st0 + (long long)k2 * st2 + k1;
+                const float g1 = 1.0f - f1, g2 = 1.0f - f2;
+                atomicAdd(p, g1 * g2 * w);
+                atomicAdd(p + 1, f1 * g2 * w);
+                atomicAdd(p + st2, g1 * f2 * w);
+                atomicAdd(p + st2 + 1, f1 * f2 * w);
+            }
+        }
+    }
+}
+
+// out[z][y][x] (=|+=) accA[z+2][y+2][x+2] + accB[z+2][x+2][y+2]
+template <typename T>
+__global__ void fold_accumulators(const float *__restrict__ accA, const float *__restrict__ accB, int nx,
+                                  int ny, int nz, T *__restrict__ out, size_t pitch, int accumulate)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx) return;
+    const size_t px = nx + 4, py = ny + 4;
+    float r = 0.0f;
+    if (accA) r += accA[((size_t)(z + 2) * py + (y + 2)) * px + (x + 2)];
+    if (accB) r += accB[((size_t)(z + 2) * px + (x + 2)) * py + (y + 2)];
+    T *o = out + ((size_t)z * ny + y) * pitch + x;
+    if (accumulate) r += ldm_plain(o);
+    *o = tom<T>(r);
+}
+
+template <typename T> b2t_status launch_T(const FPLaunch &L, dim3 grid, cudaStream_t s)
+{
+    fp3d_transpose_kernel<T><<<grid, dim3(32, 8), 0, s>>>(L);
+    count_launches(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "matched bp kernel launch");
+    return B2T_OK;
+}
+
+template <typename T>
+b2t_status launch_fold(const float *a, const float *b, const b2t_dims3d &d, void *vol, size_t pitch,
+                       int accumulate, cudaStream_t s)
+{
+    dim3 grid((d.vol_x + 127) / 128, d.vol_y, d.vol_z);
+    fold_accumulators<T><<<grid, 128, 0, s>>>(a, b, d.vol_x, d.vol_y, d.vol_z, static_cast<T *>(vol), pitch,
+                                               accumulate);
+    count_launches(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "matched bp fold launch");
+    return B2T_OK;
+}
+
+}  // namespace
+
+b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *proj,
+                             size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype,
+                             int32_t mode, cudaStream_t s)
+{
+    const b2t_dims3d &d = g->dims;
+    if (p->det_supersample == 0 || p->det_supersample > 16)
+        return fail(B2T_ERR_INVALID_ARG, "b2t_bp3d(matched): detector supersampling must be 1..16");
+    if (vol_pitch == 0) vol_pitch = d.vol_x;
+    if (proj_pitch == 0) proj_pitch = d.det_u;
+    if (vol_pitch < d.vol_x || proj_pitch < d.det_u)
+        return fail(B2T_ERR_INVALID_ARG, "b2t_bp3d(matched): pitch below row length");
+    std::vector<int> dirs(d.angles);
+    bool need[3] = {false, false, false};
+    for (uint32_t a = 0; a < d.angles; ++a) {
+        dirs[a] = dominant_axis(g->kind, g->views[a], d);
+        need[dirs[a]] = true;
+    }
+    const size_t px = d.vol_x + 4, py = d.vol_y + 4, pz = d.vol_z + 4;
+    const size_t padded = px * py * pz;
+    Scratch sa, sb;
+    if (need[1] || need[2]) {
+        B2T_TRY(sa.alloc(padded * sizeof(float), s, "matched bp accumulator (xyz)"));
+        B2T_CUDA_TRY(cudaMemsetAsync(sa.as<void>(), 0, padded * sizeof(float), s), "matched bp memset");
+    }
+    if (need[0]) {
+        B2T_TRY(sb.alloc(padded * sizeof(float), s, "matched bp accumulator (zxy)"));
+        B2T_CUDA_TRY(cudaMemsetAsync(sb.as<void>(), 0, padded * sizeof(float), s), "matched bp memset");
+    }
+    FPLaunch *Lp = new FPLaunch;
+    FPLaunch &P = *Lp;
+    const bool force_noncube = p->det_supersample > 1;
+    for (int dir = 0; dir < 3; ++dir) {
+        if (!need[dir]) continue;
+        P.proj = const_cast<void *>(proj);
+        P.proj_pitch = (long long)proj_pitch;
+        P.nu = d.det_u;
+        P.nv = d.det_v;
+        P.na = d.angles;
+        P.rays = p->det_supersample;
+        P.accumulate = 0;
+        fp_scale(g->kind, dir, g->vol_scale, force_noncube, p->output_scale, P.f1, P.f2, P.mul);
+        float *base;
+        if (dir == 0) {
+            base = sb.as<float>();
+            P.n0 = d.vol_x; P.n1 = d.vol_y; P.n2 = d.vol_z;
+            P.st0 = (long long)py;
+            P.st2 = (long long)(px * py);
+            base += 2 * P.st2 + 2 * P.st0 + 2;
+        } else if (dir == 1) {
+            base = sa.as<float>();
+            P.n0 = d.vol_y; P.n1 = d.vol_x; P.n2 = d.vol_z;
+            P.st0 = (long long)px;
+            P.st2 = (long long)(px * py);
+            base += 2 * P.st2 + 2 * P.st0 + 2;
+        } else {
+            base = sa.as<float>();
+            P.n0 = d.vol_z; P.n1 = d.vol_x; P.n2 = d.vol_y;
+            P.st0 = (long long)(px * py);
+            P.st2 = (long long)px;
+            base += 2 * P.st0 + 2 * P.st2 + 2;
+        }
+        P.vol = base;
+        std::vector<int> views;
+        for (uint32_t a = 0; a < d.angles; ++a)
+            if (dirs[a] == dir) views.push_back((int)a);
+        for (size_t c0 = 0; c0 < views.size(); c0 += FP_MAX_VIEWS) {
+            const size_t cn = std::min(views.size() - c0, (size_t)FP_MAX_VIEWS);
+            P.nviews = (int)cn;
+            for (size_t i = 0; i < cn; ++i) {
+                const int a = views[c0 + i];
+                fp_view_coeffs(g->kind, g->views[a], d, dir, P.views[i]);
+                P.views[i].a = a;
+            }
+            dim3 grid((unsigned)cn, (d.det_u + 31) / 32, (d.det_v + 7) / 8);
+            b2t_status st;
+            if (dtype == B2T_F32) st = launch_T<float>(P, grid, s);
+            else if (dtype == B2T_F16) st = launch_T<__half>(P, grid, s);
+            else st = launch_T<__nv_bfloat16>(P, grid, s);
+            if (st != B2T_OK) {
+                delete Lp;
+                return st;
+            }
+        }
+    }
+    delete Lp;
+    const float *a = (need[1] || need[2]) ? sa.as<float>() : nullptr;
+    const float *b = need[0] ? sb.as<float>() : nullptr;
+    const int accumulate = (mode == B2T_MODE_ADD) ? 1 : 0;
+    if (dtype == B2T_F32) return launch_fold<float>(a, b, d, vol, vol_pitch, accumulate, s);
+    if (dtype == B2T_F16) return launch_fold<__half>(a, b, d, vol, vol_pitch, accumulate, s);
+    return launch_fold<__nv_bfloat16>(a, b, d, vol, vol_pitch, accumulate, s);
+}
+
+}  // namespace b2t

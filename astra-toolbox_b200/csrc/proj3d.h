@@ -1,0 +1,76 @@
+// Internal declarations of the 3D projector module (launch parameter blocks
+// and host entry points behind b2t_fp3d / b2t_bp3d).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "b2tomo.h"
+
+namespace b2t {
+
+// Per-view forward-projection coefficients in the view's dominant frame
+// (see fp_view_coeffs): den, slopes a1/a2 and offsets b1/b2 are affine in the
+// detector offset (u', v') and share the denominator.  64 bytes.
+struct FPView {
+    float e[3];
+    float m1[3], m2[3];
+    float n1[3], n2[3];
+    int a;  // global view index
+};
+
+// Views per forward-projection launch: the parameter block stays under the
+// 32764-byte kernel parameter limit.
+constexpr int FP_MAX_VIEWS = 448;
+
+struct FPLaunch {
+    const void *vol;        // padded volume, pointing at texel (s=0, k1=0, k2=0)
+    void *proj;             // output projections [v][angle][u]
+    long long proj_pitch;   // elements
+    long long st0, st2;     // element strides of the marching axis and axis 2 (axis 1 stride is 1)
+    int n0, n1, n2;         // extents along marching axis, axis 1, axis 2
+    int nu, nv, na;
+    int rays;               // detector supersampling per dimension
+    int accumulate;         // 1: proj += result, 0: proj = result
+    float f1, f2, mul;      // ray length factors and output scale
+    int nviews;
+    FPView views[FP_MAX_VIEWS];
+};
+
+// Per-view backprojection coefficients: texture u = nu.(x,y,z,1) / den.(x,y,z,1)
+// (cone) or nu.(x,y,z,1) (parallel, den.w = per-view weight).  48 bytes.
+struct BPView {
+    float4 nu, nv, den;
+};
+
+constexpr int BP_MAX_VIEWS = 640;
+
+struct BPLaunch {
+    const void *proj;       // padded projections, pointing at texel (u=0, angle 0, v=0)
+    long long pv;           // element stride between detector rows
+    int pu;                 // element stride between views
+    void *vol;
+    long long vol_pitch;
+    int nx, ny, nz, nu, nv;
+    int a0, nviews;         // first view of this launch and count
+    int rays;               // voxel supersampling per dimension
+    int accumulate;
+    float out_scale;
+    BPView views[BP_MAX_VIEWS];
+};
+
+int dominant_axis(int kind, const b2t_view3d &w, const b2t_dims3d &d);
+void fp_view_coeffs(int kind, const b2t_view3d &w, const b2t_dims3d &d, int dir, FPView &o);
+void fp_scale(int kind, int dir, const float *vs, bool force_noncube, float out_scale, float &f1,
+              float &f2, float &mul);
+void bp_view_coeffs(int kind, int kernel, const b2t_view3d &w, const float *vs, BPView &o);
+b2t_status validate3d(const b2t_geom3d *g, const char *who);
+
+b2t_status fp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch,
+                     void *proj, size_t proj_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
+b2t_status bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *proj, size_t proj_pitch,
+                     void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
+b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *proj,
+                             size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype,
+                             int32_t mode, cudaStream_t s);
+
+}  // namespace b2t

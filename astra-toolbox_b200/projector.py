@@ -1,0 +1,138 @@
+"""The 'cuda3d' and 'cuda' projector objects and the direct FP/BP calls.
+
+Mirrors the reference's CCudaProjector3D / CCudaProjector2D options
+(src/CudaProjector3D.cpp:94-118, src/CudaProjector2D.cpp:84-100) and
+astra.experimental.direct_FP3D / direct_BP3D
+(python/astra/experimental.pyx:172-227): data are torch tensors on a CUDA
+device (or numpy arrays, which are copied to the device and back), all work is
+done by libb2tomo kernels on the current torch stream.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import AstraError
+from .geometry import Geometry2D, Geometry3D, is_3d_vol
+
+_KERNELS = {
+    'default': _lib.KER_DEFAULT, 'sum_square_weights': _lib.KER_SUM_SQUARE_WEIGHTS,
+    '2d_weighting': _lib.KER_2D_WEIGHTING, 'matched_bp': _lib.KER_MATCHED_BP,
+    'fdk_weighting': _lib.KER_FDK_WEIGHTING,
+}
+
+_DTYPES = {torch.float32: _lib.F32, torch.float16: _lib.F16, torch.bfloat16: _lib.BF16}
+
+
+def stream_handle(device=None):
+    """cudaStream_t of torch's current stream on device, as an int."""
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _check_tensor(t, shape, name, device=None):
+    if not isinstance(t, torch.Tensor):
+        raise AstraError(1, "%s must be a torch tensor" % name)
+    if not t.is_cuda:
+        raise AstraError(1, "%s must be on a CUDA device" % name)
+    if tuple(t.shape) != tuple(shape):
+        raise AstraError(1, "%s has shape %s, geometry needs %s" % (name, tuple(t.shape), tuple(shape)))
+    if t.dtype not in _DTYPES:
+        raise AstraError(1, "%s must be float32, float16 or bfloat16" % name)
+    if not t.is_contiguous():
+        raise AstraError(1, "%s must be contiguous" % name)
+    if device is not None and t.device != device:
+        raise AstraError(1, "%s is on %s, expected %s" % (name, t.device, device))
+
+
+class Projector3D:
+    """A 'cuda3d' projector: geometry plus projection options."""
+
+    def __init__(self, proj_geom, vol_geom, options=None):
+        options = dict(options or {})
+        self.proj_geom = proj_geom
+        self.vol_geom = vol_geom
+        self.geom = Geometry3D(vol_geom, proj_geom)
+        kname = options.get('ProjectionKernel', 'default')
+        if kname not in _KERNELS:
+            raise AstraError(1, "Unknown ProjectionKernel %r" % kname)
+        self.kernel = _KERNELS[kname]
+        self.det_ss = int(options.get('DetectorSuperSampling', 1))
+        self.vox_ss = int(options.get('VoxelSuperSampling', 1))
+        self.gpu_index = int(options.get('GPUIndex', -1))
+        self.vol_shape = self.geom.vol_shape
+        self.proj_shape = self.geom.proj_shape
+
+    def params(self, output_scale=1.0, kernel=None):
+        return _lib.Params3D(self.det_ss, self.vox_ss, float(output_scale),
+                             self.kernel if kernel is None else kernel)
+
+    def device(self):
+        if self.gpu_index >= 0:
+            return torch.device('cuda', self.gpu_index)
+        return torch.device('cuda', torch.cuda.current_device())
+
+    def fp(self, vol, proj, mode=_lib.MODE_SET, output_scale=1.0, kernel=None):
+        """proj (=|+=) A vol on torch tensors."""
+        _check_tensor(vol, self.vol_shape, "volume")
+        _check_tensor(proj, self.proj_shape, "projection data", vol.device)
+        if vol.dtype != proj.dtype:
+            raise AstraError(1, "volume and projection data must have the same dtype")
+        p = self.params(output_scale, kernel)
+        with torch.cuda.device(vol.device):
+            _lib.call("b2t_fp3d", ctypes.byref(self.geom.c), ctypes.byref(p), vol.data_ptr(), 0,
+                      proj.data_ptr(), 0, _DTYPES[vol.dtype], mode, stream_handle(vol.device))
+        return proj
+
+    def bp(self, proj, vol, mode=_lib.MODE_SET, output_scale=1.0, kernel=None):
+        """vol (=|+=) B proj on torch tensors (B = ASTRA's BP, or A^T for matched_bp)."""
+        _check_tensor(vol, self.vol_shape, "volume")
+        _check_tensor(proj, self.proj_shape, "projection data", vol.device)
+        if vol.dtype != proj.dtype:
+            raise AstraError(1, "volume and projection data must have the same dtype")
+        p = self.params(output_scale, kernel)
+        with torch.cuda.device(vol.device):
+            _lib.call("b2t_bp3d", ctypes.byref(self.geom.c), ctypes.byref(p), proj.data_ptr(), 0,
+                      vol.data_ptr(), 0, _DTYPES[vol.dtype], mode, stream_handle(vol.device))
+        return vol
+
+
+def as_device_tensor(x, device, dtype=None):
+    """(tensor on device, copy_back) for a numpy array or torch tensor."""
+    if isinstance(x, np.ndarray):
+        if x.dtype != np.float32:
+            raise AstraError(1, "numpy data must be float32")
+        return torch.from_numpy(np.ascontiguousarray(x)).to(device), True
+    if isinstance(x, torch.Tensor):
+        if x.is_cuda:
+            return x, False
+        return x.to(device), True
+    raise AstraError(1, "data must be a numpy array or a torch tensor")
+
+
+def fp3d(projector, vol, proj, mode=_lib.MODE_SET):
+    """direct_FP3D semantics on numpy arrays or torch tensors (written in place)."""
+    dev = projector.device()
+    tv, _ = as_device_tensor(vol, dev)
+    tp, back = as_device_tensor(proj, dev)
+    projector.fp(tv, tp, mode=mode)
+    if back:
+        if isinstance(proj, np.ndarray):
+            proj[...] = tp.cpu().numpy()
+        else:
+            proj.copy_(tp.cpu())
+    return proj
+
+
+def bp3d(projector, vol, proj, mode=_lib.MODE_SET):
+    """direct_BP3D semantics on numpy arrays or torch tensors (vol written in place)."""
+    dev = projector.device()
+    tp, _ = as_device_tensor(proj, dev)
+    tv, back = as_device_tensor(vol, dev)
+    projector.bp(tp, tv, mode=mode)
+    if back:
+        if isinstance(vol, np.ndarray):
+            vol[...] = tv.cpu().numpy()
+        else:
+            vol.copy_(tv.cpu())
+    return vol

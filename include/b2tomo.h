@@ -1,0 +1,258 @@
+/*
+ * b2tomo.h -- C ABI of libb2tomo, a B200-native (sm_100a) implementation of
+ * the ASTRA Toolbox CUDA projection core.
+ *
+ * Conventions (the reference's own, kept so the library drops in for
+ * cuda/2d and cuda/3d):
+ *   - volume [z][y][x] (x fastest), projections [v][angle][u] (u fastest);
+ *     2D volume [row][col], sinogram [angle][det]
+ *     (python/astra/src/dlpack.cpp:145-147, cuda/3d/mem3d.cu:348-353).
+ *   - Row pitches are in ELEMENTS (>= the row length); pitch 0 means
+ *     "contiguous".  All data pointers are device pointers unless a function
+ *     says otherwise; all of them are caller-owned.
+ *   - mode B2T_MODE_ADD accumulates (+=) into the output, B2T_MODE_SET
+ *     overwrites it (CompositeGeometryManager.h:127-129 MODE_ADD / MODE_SET).
+ *   - Every call is stream-ordered on the given cudaStream_t (passed as
+ *     void*, NULL = the legacy default stream) and returns without a device
+ *     synchronisation unless it says it returns a host value.  Per-view
+ *     geometry travels in kernel parameters, so concurrent calls on different
+ *     streams do not share state (the reference's module-global __constant__
+ *     arrays, cuda/3d/cone_fp.cu:46-57, are gone).
+ *   - Every function returns a b2t_status and never aborts or traps;
+ *     b2t_last_error() gives the message of the last failure on the calling
+ *     thread (the reference returns bool and logs through ASTRA_ERROR,
+ *     cuda/2d/util.cu:359-375).
+ */
+#ifndef B2TOMO_H
+#define B2TOMO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* status, errors, version                                                 */
+/* ---------------------------------------------------------------------- */
+
+typedef int32_t b2t_status;
+enum {
+    B2T_OK = 0,
+    B2T_ERR_INVALID_ARG = 1,   /* bad geometry, sizes, pointers or options   */
+    B2T_ERR_UNSUPPORTED = 2,   /* combination the reference also refuses     */
+    B2T_ERR_CUDA = 3,          /* a CUDA runtime error                        */
+    B2T_ERR_NO_MEMORY = 4,     /* device allocation failed                    */
+    B2T_ERR_ABORTED = 5,       /* iteration stopped by b2t_request_abort      */
+    B2T_ERR_TIMEOUT = 6        /* a bounded device-side wait gave up          */
+};
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *b2t_last_error(void);
+/* Library version, e.g. 100 for 1.0.0. */
+int32_t b2t_version(void);
+/* Number of CUDA kernels this library has launched since it was loaded
+ * (all threads); lets callers verify which work ran on the device. */
+uint64_t b2t_kernel_launches(void);
+/* Select the CUDA device for this host thread (astraCUDA::setGPUIndex,
+ * cuda/2d/astra.cu:60-75). */
+b2t_status b2t_set_device(int32_t device);
+
+/* ---------------------------------------------------------------------- */
+/* enumerations                                                            */
+/* ---------------------------------------------------------------------- */
+
+enum { B2T_MODE_ADD = 0, B2T_MODE_SET = 1 };
+
+/* storage types of volume / projection data; all arithmetic is FP32 */
+enum { B2T_F32 = 0, B2T_F16 = 1, B2T_BF16 = 2 };
+
+/* geometry kinds */
+enum {
+    B2T_GEOM_PAR3D = 1,   /* parallel3d, parallel3d_vec -> SPar3DProjection  */
+    B2T_GEOM_CONE = 2,    /* cone, cone_vec            -> SConeProjection   */
+    B2T_GEOM_PAR2D = 3,   /* parallel, parallel_vec    -> SParProjection    */
+    B2T_GEOM_FAN2D = 4    /* fanflat, fanflat_vec      -> SFanProjection    */
+};
+
+/* projection kernels: Cuda3DProjectionKernel (cuda/3d/dims3d.h:45-51) */
+enum {
+    B2T_KER_DEFAULT = 0,
+    B2T_KER_SUM_SQUARE_WEIGHTS = 1,
+    B2T_KER_FDK_WEIGHTING = 2,
+    B2T_KER_2D_WEIGHTING = 3,
+    B2T_KER_MATCHED_BP = 4     /* exact transpose of the forward projector   */
+};
+
+/* filter types: E_FBPFILTER subset (include/astra/Filters.h:36-60) */
+enum { B2T_FILTER_NONE = 0, B2T_FILTER_RAMLAK = 1 };
+
+/* element-wise operations: processVol3D<op> (cuda/3d/arith3d.cu:44-111) */
+enum {
+    B2T_OP_SET = 0,          /* out = s                                     */
+    B2T_OP_MUL_SCALAR = 1,   /* out *= s                                    */
+    B2T_OP_MUL = 2,          /* out *= a                                    */
+    B2T_OP_ADD_MUL = 3,      /* out += a * b           (opAddMul)           */
+    B2T_OP_ADD_SCALED = 4,   /* out += a * s           (opAddScaled)        */
+    B2T_OP_SCALE_AND_ADD = 5,/* out = a + out * s      (opScaleAndAdd)      */
+    B2T_OP_INVERT = 6,       /* out = out > 1e-6 ? 1/out : 0 (opInvert)     */
+    B2T_OP_CLAMP_MIN = 7,    /* out = max(out, s)                           */
+    B2T_OP_CLAMP_MAX = 8,    /* out = min(out, s)                           */
+    B2T_OP_ADD = 9           /* out += a                                    */
+};
+
+/* ---------------------------------------------------------------------- */
+/* geometry                                                                */
+/* ---------------------------------------------------------------------- */
+
+/* One 3D view.  Same layout and meaning as SConeProjection / SPar3DProjection
+ * (include/astra/GeometryUtil3D.h:47-115): src = source position (cone) or
+ * ray direction (parallel); det_s = detector corner ("bottom left" of pixel
+ * (0,0)); det_u / det_v = one pixel step along u / v. */
+typedef struct b2t_view3d {
+    double src[3];
+    double det_s[3];
+    double det_u[3];
+    double det_v[3];
+} b2t_view3d;
+
+/* SDimensions3D (include/astra/GeometryUtil3D.h:150-157) */
+typedef struct b2t_dims3d {
+    uint32_t vol_x, vol_y, vol_z;
+    uint32_t angles, det_u, det_v;
+} b2t_dims3d;
+
+/* Normalised 3D geometry: views already translated/scaled to unit voxels
+ * centred on the origin.  Geometry3DParameters (GeometryUtil3D.h:172-227). */
+typedef struct b2t_geom3d {
+    int32_t kind;              /* B2T_GEOM_PAR3D or B2T_GEOM_CONE            */
+    b2t_dims3d dims;
+    float vol_scale[3];        /* SVolScale3D: voxel size x, y, z            */
+    const b2t_view3d *views;   /* host array of dims.angles views            */
+} b2t_geom3d;
+
+/* SProjectorParams3D (cuda/3d/dims3d.h:53-66) minus volScale */
+typedef struct b2t_params3d {
+    uint32_t det_supersample;    /* iRaysPerDetDim   (DetectorSuperSampling) */
+    uint32_t voxel_supersample;  /* iRaysPerVoxelDim (VoxelSuperSampling)    */
+    float output_scale;          /* fOutputScale                             */
+    int32_t kernel;              /* B2T_KER_*                                */
+} b2t_params3d;
+
+/* CVolumeGeometry3D window (src/VolumeGeometry3D.cpp:140-180): grid counts
+ * and window extents, float32 as the reference stores them. */
+typedef struct b2t_volgeom3d {
+    uint32_t cols, rows, slices;  /* x, y, z */
+    float min_x, max_x, min_y, max_y, min_z, max_z;
+} b2t_volgeom3d;
+
+/* genConeProjections (src/GeometryUtil3D.cpp:42-83). */
+b2t_status b2t_cone_views(uint32_t n_angles, uint32_t det_cols, uint32_t det_rows,
+                          float src_origin, float origin_det, float det_spacing_x,
+                          float det_spacing_y, const float *angles, b2t_view3d *out);
+/* genPar3DProjections (src/GeometryUtil3D.cpp:133-172). */
+b2t_status b2t_par3d_views(uint32_t n_angles, uint32_t det_cols, uint32_t det_rows,
+                           float det_spacing_x, float det_spacing_y, const float *angles,
+                           b2t_view3d *out);
+/* cone_vec / parallel3d_vec rows (12 doubles: src-or-ray, detector CENTRE, u,
+ * v) to corner-based views: CConeVecProjectionGeometry3D /
+ * CParallelVecProjectionGeometry3D initialisation
+ * (src/ConeVecProjectionGeometry3D.cpp:96-110). */
+b2t_status b2t_vec_views3d(uint32_t n_angles, uint32_t det_cols, uint32_t det_rows,
+                           const double *vectors, b2t_view3d *out);
+/* convertAstraGeometry_internal (src/GeometryUtil3D.cpp:569-593): translate by
+ * the float window centre, scale by the float inverse voxel size, in place.
+ * Writes the voxel size to vol_scale_out[3]. */
+b2t_status b2t_normalize_views3d(const b2t_volgeom3d *vol, int32_t kind, uint32_t n,
+                                 b2t_view3d *views, float *vol_scale_out);
+
+/* One 2D view: SFanProjection / SParProjection (GeometryUtil2D.h:53-105),
+ * float fields.  src = source (fan) or ray direction (parallel); det_s =
+ * detector start (pixel 0 corner); det_u = one detector pixel step. */
+typedef struct b2t_view2d {
+    float src[2];
+    float det_s[2];
+    float det_u[2];
+} b2t_view2d;
+
+/* SDimensions (include/astra/GeometryUtil2D.h:41-51) */
+typedef struct b2t_dims2d {
+    uint32_t vol_width, vol_height;
+    uint32_t angles, dets;
+} b2t_dims2d;
+
+/* Normalised 2D geometry: Geometry2DParameters (GeometryUtil2D.h:107-150). */
+typedef struct b2t_geom2d {
+    int32_t kind;              /* B2T_GEOM_PAR2D or B2T_GEOM_FAN2D            */
+    b2t_dims2d dims;
+    float output_scale;        /* pixel size (convertAstraGeometry, 2D)       */
+    const b2t_view2d *views;   /* host array of dims.angles views             */
+} b2t_geom2d;
+
+/* CVolumeGeometry2D window (src/VolumeGeometry2D.cpp:190-205). */
+typedef struct b2t_volgeom2d {
+    uint32_t cols, rows;
+    float min_x, max_x, min_y, max_y;
+} b2t_volgeom2d;
+
+/* genParProjections (src/GeometryUtil2D.cpp:40-78), no extra offsets. */
+b2t_status b2t_par_views(uint32_t n_angles, uint32_t n_dets, float det_width,
+                         const float *angles, b2t_view2d *out);
+/* genFanProjections (src/GeometryUtil2D.cpp:81-104). */
+b2t_status b2t_fan_views(uint32_t n_angles, uint32_t n_dets, float src_origin, float origin_det,
+                         float det_width, const float *angles, b2t_view2d *out);
+/* parallel_vec / fanflat_vec rows (6 doubles: src-or-ray, detector CENTRE,
+ * u) to corner-based views (src/FanFlatVecProjectionGeometry2D.cpp:108-124). */
+b2t_status b2t_vec_views2d(uint32_t n_angles, uint32_t n_dets, const double *vectors,
+                           b2t_view2d *out);
+/* convertAstraGeometry_internal, 2D (src/GeometryUtil2D.cpp:182-209); refuses
+ * non-square pixels as the reference does.  Writes the output scale. */
+b2t_status b2t_normalize_views2d(const b2t_volgeom2d *vol, int32_t kind, uint32_t n,
+                                 b2t_view2d *views, float *output_scale);
+
+/* ---------------------------------------------------------------------- */
+/* 3D projectors                                                           */
+/* ---------------------------------------------------------------------- */
+
+/* Forward projection proj (+)= A vol.  Replaces astraCUDA3d::FP
+ * (include/astra/cuda/3d/mem3d.h:107), ConeFP (cone_fp.h:33-36) and Par3DFP
+ * (par3d_fp.h:33-36).  Kernels: DEFAULT, 2D_WEIGHTING, FDK_WEIGHTING and
+ * MATCHED_BP project identically (cuda/3d/mem3d.cu:355-386).  vol and proj
+ * have storage type dtype (B2T_F32/F16/BF16). */
+b2t_status b2t_fp3d(const b2t_geom3d *geom, const b2t_params3d *params,
+                    const void *vol, size_t vol_pitch, void *proj, size_t proj_pitch,
+                    int32_t dtype, int32_t mode, void *stream);
+
+/* Backprojection vol (+)= B proj.  Replaces astraCUDA3d::BP (mem3d.h:109),
+ * ConeBP (cone_bp.h:33-36) and Par3DBP (par3d_bp.h:33-36).  kernel DEFAULT is
+ * ASTRA's voxel-driven BP (not the exact adjoint), FDK_WEIGHTING and
+ * 2D_WEIGHTING its weight variants (cone_bp.cu:99-123, 226-269), MATCHED_BP
+ * the exact transpose of b2t_fp3d (ker3d_matched_bp, mem3d.cu:463-479, which
+ * the reference implements only for cyl_cone_vec). */
+b2t_status b2t_bp3d(const b2t_geom3d *geom, const b2t_params3d *params,
+                    const void *proj, size_t proj_pitch, void *vol, size_t vol_pitch,
+                    int32_t dtype, int32_t mode, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* element-wise operations and reductions                                  */
+/* ---------------------------------------------------------------------- */
+
+/* out = op(out, a, b, s) over n contiguous f32 elements (processVol3D<op>,
+ * include/astra/cuda/3d/arith3d.h; processData<op>, cuda/2d/arith.cu). */
+b2t_status b2t_vec_op(int32_t op, float *out, const float *a, const float *b, float s, size_t n,
+                      void *stream);
+
+/* sum(a[i] * b[i]) over n elements accumulated in FP64, written to the DEVICE
+ * double *result.  b may equal a (squared norm).  Replaces dotProduct2D /
+ * dotProduct3D (cuda/2d/util.cu:304-357, cuda/3d/mem3d.cu:581-590), which
+ * accumulate in float32.  Uses a device scratch buffer that the call
+ * allocates and frees in stream order. */
+b2t_status b2t_dot_f64(const void *a, const void *b, size_t n, int32_t dtype, double *result,
+                       void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B2TOMO_H */

@@ -1,0 +1,173 @@
+"""ctypes wrapper of oracle/_ref/libastra_ref.so (the reference built from its
+own sources by oracle/ref.mk, plus oracle/ref_wrap.cu).
+
+TEST INFRASTRUCTURE ONLY (tests/, and the reference legs of bench.py).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(_HERE, "_ref", "libastra_ref.so")
+_lib = None
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+
+GEOM3D_TYPES = {'parallel3d': 0, 'cone': 1, 'parallel3d_vec': 2, 'cone_vec': 3}
+GEOM2D_TYPES = {'parallel': 0, 'fanflat': 1, 'parallel_vec': 2, 'fanflat_vec': 3}
+
+
+def available():
+    return os.path.exists(LIB)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(LIB)
+        L.ref_geom3d.argtypes = [_I, _I, _I, _I, _P, _I, _I, _I, _F, _F, _P, _F, _F, _P, _P, _P]
+        L.ref_geom2d.argtypes = [_I, _I, _I, _P, _I, _I, _F, _P, _F, _F, _P, _P, _P]
+        L.ref_cuda_fp3d.argtypes = [_I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _I, _P, _P]
+        L.ref_cuda_bp3d.argtypes = [_I, _I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _I, _P, _P]
+        L.ref_cuda_fdk.argtypes = [_P, _I, _I, _I, _I, _I, _I, _P, _I, _F, _P, _P]
+        L.ref_cuda_fp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _P, _P]
+        L.ref_cuda_bp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _I, _P, _P]
+        _lib = L
+    return _lib
+
+
+def geom3d(vol_geom, proj_geom):
+    """Reference convertAstraGeometry: ((n,12) float64 views, (3,) float32 voxel size)."""
+    t = proj_geom['type']
+    o = vol_geom['option']
+    win = np.array([o['WindowMinX'], o['WindowMaxX'], o['WindowMinY'], o['WindowMaxY'],
+                    o['WindowMinZ'], o['WindowMaxZ']], dtype=np.float32)
+    rows, cols = proj_geom['DetectorRowCount'], proj_geom['DetectorColCount']
+    if 'Vectors' in proj_geom:
+        vec = np.ascontiguousarray(proj_geom['Vectors'], dtype=np.float64)
+        na = vec.shape[0]
+        ang = np.zeros(1, dtype=np.float32)
+        sx = sy = sod = odd = 0.0
+    else:
+        ang = np.ascontiguousarray(proj_geom['ProjectionAngles'], dtype=np.float32).ravel()
+        na = ang.size
+        vec = np.zeros(12, dtype=np.float64)
+        sx, sy = proj_geom['DetectorSpacingX'], proj_geom['DetectorSpacingY']
+        sod = proj_geom.get('DistanceOriginSource', 0.0)
+        odd = proj_geom.get('DistanceOriginDetector', 0.0)
+    views = np.zeros((na, 12), dtype=np.float64)
+    vs = np.zeros(3, dtype=np.float32)
+    rc = lib().ref_geom3d(GEOM3D_TYPES[t], vol_geom['GridColCount'], vol_geom['GridRowCount'],
+                          vol_geom['GridSliceCount'], win.ctypes.data, na, rows, cols, sx, sy,
+                          ang.ctypes.data, sod, odd, vec.ctypes.data, views.ctypes.data, vs.ctypes.data)
+    assert rc == 0
+    return views, vs
+
+
+def geom2d(vol_geom, proj_geom):
+    """Reference 2D convertAstraGeometry: ((n,6) float32 views, output scale)."""
+    t = proj_geom['type']
+    o = vol_geom['option']
+    win = np.array([o['WindowMinX'], o['WindowMaxX'], o['WindowMinY'], o['WindowMaxY']], dtype=np.float32)
+    ndet = proj_geom['DetectorCount']
+    if 'Vectors' in proj_geom:
+        vec = np.ascontiguousarray(proj_geom['Vectors'], dtype=np.float64)
+        na = vec.shape[0]
+        ang = np.zeros(1, dtype=np.float32)
+        w = sod = odd = 0.0
+    else:
+        ang = np.ascontiguousarray(proj_geom['ProjectionAngles'], dtype=np.float32).ravel()
+        na = ang.size
+        vec = np.zeros(6, dtype=np.float64)
+        w = proj_geom['DetectorWidth']
+        sod = proj_geom.get('DistanceOriginSource', 0.0)
+        odd = proj_geom.get('DistanceOriginDetector', 0.0)
+    views = np.zeros((na, 6), dtype=np.float32)
+    sc = np.zeros(1, dtype=np.float32)
+    rc = lib().ref_geom2d(GEOM2D_TYPES[t], vol_geom['GridColCount'], vol_geom['GridRowCount'],
+                          win.ctypes.data, na, ndet, w, ang.ctypes.data, sod, odd, vec.ctypes.data,
+                          views.ctypes.data, sc.ctypes.data)
+    assert rc == 0
+    return views, float(sc[0])
+
+
+# ---------------------------------------------------------------------------
+# reference CUDA projectors (need a GPU; device pointers from torch tensors)
+# ---------------------------------------------------------------------------
+
+def cuda_fp3d(kind, views, vol, nu, nv, vol_scale=(1.0, 1.0, 1.0), out_scale=1.0, rays=1):
+    """Reference ConeFP / Par3DFP on a float32 CUDA tensor vol (z, y, x); returns a new tensor."""
+    import torch
+    views = np.ascontiguousarray(views, dtype=np.float64)
+    vs = np.ascontiguousarray(vol_scale, dtype=np.float32)
+    nz, ny, nx = vol.shape
+    na = views.shape[0]
+    proj = torch.zeros((nv, na, nu), dtype=torch.float32, device=vol.device)
+    torch.cuda.synchronize()
+    rc = lib().ref_cuda_fp3d(kind, views.ctypes.data, nx, ny, nz, na, nu, nv, vs.ctypes.data, out_scale,
+                             rays, vol.data_ptr(), proj.data_ptr())
+    assert rc == 0
+    torch.cuda.synchronize()
+    return proj
+
+
+def cuda_bp3d(kind, views, proj, vol_shape, vol_scale=(1.0, 1.0, 1.0), out_scale=1.0, kernel=0, rays=1):
+    import torch
+    views = np.ascontiguousarray(views, dtype=np.float64)
+    vs = np.ascontiguousarray(vol_scale, dtype=np.float32)
+    nv, na, nu = proj.shape
+    nz, ny, nx = vol_shape
+    vol = torch.zeros(vol_shape, dtype=torch.float32, device=proj.device)
+    torch.cuda.synchronize()
+    rc = lib().ref_cuda_bp3d(kind, kernel, views.ctypes.data, nx, ny, nz, na, nu, nv, vs.ctypes.data,
+                             out_scale, rays, proj.data_ptr(), vol.data_ptr())
+    assert rc == 0
+    torch.cuda.synchronize()
+    return vol
+
+
+def cuda_fdk(views, proj, vol_shape, vol_scale=(1.0, 1.0, 1.0), short_scan=False, out_scale=1.0):
+    """Reference FDK (Ram-Lak); proj is filtered in place (pass a copy)."""
+    import torch
+    views = np.ascontiguousarray(views, dtype=np.float64)
+    vs = np.ascontiguousarray(vol_scale, dtype=np.float32)
+    nv, na, nu = proj.shape
+    nz, ny, nx = vol_shape
+    vol = torch.zeros(vol_shape, dtype=torch.float32, device=proj.device)
+    torch.cuda.synchronize()
+    rc = lib().ref_cuda_fdk(views.ctypes.data, nx, ny, nz, na, nu, nv, vs.ctypes.data, int(short_scan),
+                            out_scale, proj.data_ptr(), vol.data_ptr())
+    assert rc == 0
+    torch.cuda.synchronize()
+    return vol
+
+
+def cuda_fp2d(kind, views, vol, ndet, out_scale=1.0, rays=1):
+    """kind 3 parallel, 4 fan; vol (rows, cols) float32 CUDA tensor."""
+    import torch
+    views = np.ascontiguousarray(views, dtype=np.float32)
+    H, W = vol.shape
+    na = views.shape[0]
+    sino = torch.zeros((na, ndet), dtype=torch.float32, device=vol.device)
+    torch.cuda.synchronize()
+    rc = lib().ref_cuda_fp2d(kind, views.ctypes.data, W, H, na, ndet, out_scale, rays, vol.data_ptr(),
+                             sino.data_ptr())
+    assert rc == 0
+    torch.cuda.synchronize()
+    return sino
+
+
+def cuda_bp2d(kind, views, sino, vol_shape, out_scale=1.0, rays=1, fbp=False):
+    import torch
+    views = np.ascontiguousarray(views, dtype=np.float32)
+    na, ndet = sino.shape
+    H, W = vol_shape
+    vol = torch.zeros(vol_shape, dtype=torch.float32, device=sino.device)
+    torch.cuda.synchronize()
+    rc = lib().ref_cuda_bp2d(kind, views.ctypes.data, W, H, na, ndet, out_scale, rays, int(fbp),
+                             sino.data_ptr(), vol.data_ptr())
+    assert rc == 0
+    torch.cuda.synchronize()
+    return vol

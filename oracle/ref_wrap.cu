@@ -1,0 +1,330 @@
+// ref_wrap.cu -- extern "C" entry points into the reference ASTRA Toolbox,
+// built from its own sources by oracle/build_ref.sh into oracle/_ref/.
+//
+// TEST INFRASTRUCTURE ONLY.  These wrappers let the tests (and the reference
+// leg of bench.py) call the reference's geometry conversion, its CUDA
+// projectors and its FDK on the same inputs as libb2tomo.  Nothing in
+// astra-toolbox_b200 links or calls this.
+//
+// Called reference functions:
+//   astra::convertAstraGeometry      src/GeometryUtil3D.cpp:754, GeometryUtil2D.cpp:357
+//   astraCUDA3d::ConeFP / Par3DFP    cuda/3d/cone_fp.cu:444, par3d_fp.cu:564
+//   astraCUDA3d::ConeBP / Par3DBP    cuda/3d/cone_bp.cu:380, par3d_bp.cu:318
+//   astraCUDA3d::FDK                 cuda/3d/fdk.cu:415
+//   astraCUDA::FP / FanFP            cuda/2d/par_fp.cu:340, fan_fp.cu:260
+//   astraCUDA::BP / FanBP            cuda/2d/par_bp.cu:224, fan_bp.cu:380
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "astra/cuda/gpu_runtime_wrapper.h"
+#include "astra/cuda/2d/util.h"
+#include "astra/cuda/3d/util3d.h"
+#include "astra/cuda/3d/dims3d.h"
+#include "astra/ConeProjectionGeometry3D.h"
+#include "astra/ConeVecProjectionGeometry3D.h"
+#include "astra/FanFlatProjectionGeometry2D.h"
+#include "astra/FanFlatVecProjectionGeometry2D.h"
+#include "astra/Filters.h"
+#include "astra/GeometryUtil2D.h"
+#include "astra/GeometryUtil3D.h"
+#include "astra/ParallelProjectionGeometry2D.h"
+#include "astra/ParallelProjectionGeometry3D.h"
+#include "astra/ParallelVecProjectionGeometry2D.h"
+#include "astra/ParallelVecProjectionGeometry3D.h"
+#include "astra/VolumeGeometry2D.h"
+#include "astra/VolumeGeometry3D.h"
+#include "astra/cuda/2d/fan_bp.h"
+#include "astra/cuda/2d/fan_fp.h"
+#include "astra/cuda/2d/par_bp.h"
+#include "astra/cuda/2d/par_fp.h"
+#include "astra/cuda/3d/cone_bp.h"
+#include "astra/cuda/3d/cone_fp.h"
+#include "astra/cuda/3d/dims3d.h"
+#include "astra/cuda/3d/fdk.h"
+#include "astra/cuda/3d/par3d_bp.h"
+#include "astra/cuda/3d/par3d_fp.h"
+
+using namespace astra;
+
+namespace {
+
+void copy_cone(const SConeProjection &p, double *o)
+{
+    const double v[12] = {p.fSrcX, p.fSrcY, p.fSrcZ, p.fDetSX, p.fDetSY, p.fDetSZ,
+                          p.fDetUX, p.fDetUY, p.fDetUZ, p.fDetVX, p.fDetVY, p.fDetVZ};
+    memcpy(o, v, sizeof(v));
+}
+void copy_par(const SPar3DProjection &p, double *o)
+{
+    const double v[12] = {p.fRayX, p.fRayY, p.fRayZ, p.fDetSX, p.fDetSY, p.fDetSZ,
+                          p.fDetUX, p.fDetUY, p.fDetUZ, p.fDetVX, p.fDetVY, p.fDetVZ};
+    memcpy(o, v, sizeof(v));
+}
+SConeProjection to_cone(const double *o)
+{
+    SConeProjection p;
+    p.fSrcX = o[0]; p.fSrcY = o[1]; p.fSrcZ = o[2];
+    p.fDetSX = o[3]; p.fDetSY = o[4]; p.fDetSZ = o[5];
+    p.fDetUX = o[6]; p.fDetUY = o[7]; p.fDetUZ = o[8];
+    p.fDetVX = o[9]; p.fDetVY = o[10]; p.fDetVZ = o[11];
+    return p;
+}
+SPar3DProjection to_par(const double *o)
+{
+    SPar3DProjection p;
+    p.fRayX = o[0]; p.fRayY = o[1]; p.fRayZ = o[2];
+    p.fDetSX = o[3]; p.fDetSY = o[4]; p.fDetSZ = o[5];
+    p.fDetUX = o[6]; p.fDetUY = o[7]; p.fDetUZ = o[8];
+    p.fDetVX = o[9]; p.fDetVY = o[10]; p.fDetVZ = o[11];
+    return p;
+}
+SDimensions3D dims3(int nx, int ny, int nz, int na, int nu, int nv)
+{
+    SDimensions3D d;
+    d.iVolX = nx; d.iVolY = ny; d.iVolZ = nz;
+    d.iProjAngles = na; d.iProjU = nu; d.iProjV = nv;
+    return d;
+}
+cudaPitchedPtr pitched(const float *p, int x, int y)
+{
+    return make_cudaPitchedPtr((void *)p, sizeof(float) * x, x, y);
+}
+
+}  // namespace
+
+extern "C" {
+
+// type: 0 parallel3d, 1 cone, 2 parallel3d_vec, 3 cone_vec.
+// window: min_x, max_x, min_y, max_y, min_z, max_z.  vecs: (na, 12) centre-based rows.
+int ref_geom3d(int type, int cols, int rows, int slices, const float *window, int na, int det_rows,
+               int det_cols, float sx, float sy, const float *angles, float sod, float odd,
+               const double *vecs, double *out_views, float *out_volscale)
+{
+    CVolumeGeometry3D vg(cols, rows, slices, window[0], window[2], window[4], window[1], window[3], window[5]);
+    std::unique_ptr<CProjectionGeometry3D> pg;
+    if (type == 0 || type == 1) {
+        std::vector<float32> a(angles, angles + na);
+        if (type == 0)
+            pg.reset(new CParallelProjectionGeometry3D(na, det_rows, det_cols, sx, sy, std::move(a)));
+        else
+            pg.reset(new CConeProjectionGeometry3D(na, det_rows, det_cols, sx, sy, std::move(a), sod, odd));
+    } else if (type == 2) {
+        std::vector<SPar3DProjection> v(na);
+        for (int i = 0; i < na; ++i) {
+            const double *d = vecs + 12 * i;
+            SPar3DProjection &p = v[i];
+            p.fRayX = d[0]; p.fRayY = d[1]; p.fRayZ = d[2];
+            p.fDetUX = d[6]; p.fDetUY = d[7]; p.fDetUZ = d[8];
+            p.fDetVX = d[9]; p.fDetVY = d[10]; p.fDetVZ = d[11];
+            p.fDetSX = d[3] - 0.5 * det_rows * p.fDetVX - 0.5 * det_cols * p.fDetUX;
+            p.fDetSY = d[4] - 0.5 * det_rows * p.fDetVY - 0.5 * det_cols * p.fDetUY;
+            p.fDetSZ = d[5] - 0.5 * det_rows * p.fDetVZ - 0.5 * det_cols * p.fDetUZ;
+        }
+        pg.reset(new CParallelVecProjectionGeometry3D(na, det_rows, det_cols, std::move(v)));
+    } else {
+        std::vector<SConeProjection> v(na);
+        for (int i = 0; i < na; ++i) {
+            const double *d = vecs + 12 * i;
+            SConeProjection &p = v[i];
+            p.fSrcX = d[0]; p.fSrcY = d[1]; p.fSrcZ = d[2];
+            p.fDetUX = d[6]; p.fDetUY = d[7]; p.fDetUZ = d[8];
+            p.fDetVX = d[9]; p.fDetVY = d[10]; p.fDetVZ = d[11];
+            p.fDetSX = d[3] - 0.5 * det_rows * p.fDetVX - 0.5 * det_cols * p.fDetUX;
+            p.fDetSY = d[4] - 0.5 * det_rows * p.fDetVY - 0.5 * det_cols * p.fDetUY;
+            p.fDetSZ = d[5] - 0.5 * det_rows * p.fDetVZ - 0.5 * det_cols * p.fDetUZ;
+        }
+        pg.reset(new CConeVecProjectionGeometry3D(na, det_rows, det_cols, std::move(v)));
+    }
+    Geometry3DParameters g = convertAstraGeometry(&vg, pg.get());
+    if (!g.isValid()) return 1;
+    for (int i = 0; i < na; ++i) {
+        if (g.isCone()) copy_cone(g.getCone()[i], out_views + 12 * i);
+        else copy_par(g.getParallel()[i], out_views + 12 * i);
+    }
+    out_volscale[0] = g.getVolScale().fX;
+    out_volscale[1] = g.getVolScale().fY;
+    out_volscale[2] = g.getVolScale().fZ;
+    return 0;
+}
+
+// type: 0 parallel, 1 fanflat, 2 parallel_vec, 3 fanflat_vec.  window: min_x, max_x, min_y, max_y.
+int ref_geom2d(int type, int cols, int rows, const float *window, int na, int ndet, float width,
+               const float *angles, float sod, float odd, const double *vecs, float *out_views,
+               float *out_scale)
+{
+    CVolumeGeometry2D vg(cols, rows, window[0], window[2], window[1], window[3]);
+    std::unique_ptr<CProjectionGeometry2D> pg;
+    if (type == 0 || type == 1) {
+        std::vector<float32> a(angles, angles + na);
+        if (type == 0) pg.reset(new CParallelProjectionGeometry2D(na, ndet, width, std::move(a)));
+        else pg.reset(new CFanFlatProjectionGeometry2D(na, ndet, width, std::move(a), sod, odd));
+    } else if (type == 2) {
+        std::vector<SParProjection> v(na);
+        for (int i = 0; i < na; ++i) {
+            const double *d = vecs + 6 * i;
+            SParProjection &p = v[i];
+            p.fRayX = d[0]; p.fRayY = d[1]; p.fDetUX = d[4]; p.fDetUY = d[5];
+            p.fDetSX = d[2] - 0.5 * ndet * p.fDetUX;
+            p.fDetSY = d[3] - 0.5 * ndet * p.fDetUY;
+        }
+        pg.reset(new CParallelVecProjectionGeometry2D(na, ndet, std::move(v)));
+    } else {
+        std::vector<SFanProjection> v(na);
+        for (int i = 0; i < na; ++i) {
+            const double *d = vecs + 6 * i;
+            SFanProjection &p = v[i];
+            p.fSrcX = d[0]; p.fSrcY = d[1]; p.fDetUX = d[4]; p.fDetUY = d[5];
+            p.fDetSX = d[2] - 0.5 * ndet * p.fDetUX;
+            p.fDetSY = d[3] - 0.5 * ndet * p.fDetUY;
+        }
+        pg.reset(new CFanFlatVecProjectionGeometry2D(na, ndet, std::move(v)));
+    }
+    Geometry2DParameters g = convertAstraGeometry(&vg, pg.get());
+    if (!g.isValid()) return 1;
+    for (int i = 0; i < na; ++i) {
+        float *o = out_views + 6 * i;
+        if (g.isParallel()) {
+            const SParProjection &p = g.getParallel()[i];
+            o[0] = p.fRayX; o[1] = p.fRayY; o[2] = p.fDetSX; o[3] = p.fDetSY; o[4] = p.fDetUX; o[5] = p.fDetUY;
+        } else {
+            const SFanProjection &p = g.getFan()[i];
+            o[0] = p.fSrcX; o[1] = p.fSrcY; o[2] = p.fDetSX; o[3] = p.fDetSY; o[4] = p.fDetUX; o[5] = p.fDetUY;
+        }
+    }
+    *out_scale = g.getOutputScale();
+    return 0;
+}
+
+// kind: 1 par3d, 2 cone (same codes as libb2tomo).  Device pointers; the
+// reference accumulates into d_proj (callers zero it for SET semantics).
+int ref_cuda_fp3d(int kind, const double *views, int nx, int ny, int nz, int na, int nu, int nv,
+                  const float *vs, float out_scale, int rays, const float *d_vol, float *d_proj)
+{
+    astraCUDA3d::SProjectorParams3D params;
+    params.volScale.fX = vs[0];
+    params.volScale.fY = vs[1];
+    params.volScale.fZ = vs[2];
+    params.iRaysPerDetDim = rays;
+    params.fOutputScale = out_scale;
+    SDimensions3D d = dims3(nx, ny, nz, na, nu, nv);
+    bool ok;
+    if (kind == 2) {
+        std::vector<SConeProjection> p(na);
+        for (int i = 0; i < na; ++i) p[i] = to_cone(views + 12 * i);
+        ok = astraCUDA3d::ConeFP(pitched(d_vol, nx, ny), pitched(d_proj, nu, na), d, &p[0], params);
+    } else {
+        std::vector<SPar3DProjection> p(na);
+        for (int i = 0; i < na; ++i) p[i] = to_par(views + 12 * i);
+        ok = astraCUDA3d::Par3DFP(pitched(d_vol, nx, ny), pitched(d_proj, nu, na), d, &p[0], params);
+    }
+    return ok ? 0 : 1;
+}
+
+// kernel: 0 default, 2 fdk_weighting, 3 2d_weighting.  Accumulates into d_vol.
+int ref_cuda_bp3d(int kind, int kernel, const double *views, int nx, int ny, int nz, int na, int nu, int nv,
+                  const float *vs, float out_scale, int rays, const float *d_proj, float *d_vol)
+{
+    astraCUDA3d::SProjectorParams3D params;
+    params.volScale.fX = vs[0];
+    params.volScale.fY = vs[1];
+    params.volScale.fZ = vs[2];
+    params.iRaysPerVoxelDim = rays;
+    params.fOutputScale = out_scale;
+    params.projKernel = (astraCUDA3d::Cuda3DProjectionKernel)kernel;
+    SDimensions3D d = dims3(nx, ny, nz, na, nu, nv);
+    bool ok;
+    if (kind == 2) {
+        std::vector<SConeProjection> p(na);
+        for (int i = 0; i < na; ++i) p[i] = to_cone(views + 12 * i);
+        ok = astraCUDA3d::ConeBP(pitched(d_vol, nx, ny), pitched(d_proj, nu, na), d, &p[0], params);
+    } else {
+        std::vector<SPar3DProjection> p(na);
+        for (int i = 0; i < na; ++i) p[i] = to_par(views + 12 * i);
+        ok = astraCUDA3d::Par3DBP(pitched(d_vol, nx, ny), pitched(d_proj, nu, na), d, &p[0], params);
+    }
+    return ok ? 0 : 1;
+}
+
+// FDK with the Ram-Lak filter; d_proj is weighted and filtered in place and
+// the result accumulated into d_vol.
+int ref_cuda_fdk(const double *views, int nx, int ny, int nz, int na, int nu, int nv, const float *vs,
+                 int short_scan, float out_scale, float *d_proj, float *d_vol)
+{
+    astraCUDA3d::SProjectorParams3D params;
+    params.volScale.fX = vs[0];
+    params.volScale.fY = vs[1];
+    params.volScale.fZ = vs[2];
+    params.fOutputScale = out_scale;
+    params.projKernel = astraCUDA3d::ker3d_fdk_weighting;
+    SDimensions3D d = dims3(nx, ny, nz, na, nu, nv);
+    std::vector<SConeProjection> p(na);
+    for (int i = 0; i < na; ++i) p[i] = to_cone(views + 12 * i);
+    SFilterConfig cfg;
+    cfg.m_eType = FILTER_RAMLAK;
+    bool ok = astraCUDA3d::FDK(pitched(d_vol, nx, ny), pitched(d_proj, nu, na), &p[0], d, params,
+                               short_scan != 0, cfg);
+    return ok ? 0 : 1;
+}
+
+// 2D: kind 3 parallel, 4 fan.  views: (na, 6) floats.  Accumulates.
+int ref_cuda_fp2d(int kind, const float *views, int W, int H, int na, int ndet, float out_scale, int rays,
+                  float *d_vol, float *d_sino)
+{
+    SDimensions d;
+    d.iVolWidth = W; d.iVolHeight = H; d.iProjAngles = na; d.iProjDets = ndet;
+    astraCUDA::SProjectorParams2D params;
+    params.iRaysPerDet = rays;
+    params.fOutputScale = out_scale;
+    bool ok;
+    if (kind == 3) {
+        std::vector<SParProjection> p(na);
+        for (int i = 0; i < na; ++i) {
+            const float *o = views + 6 * i;
+            p[i].fRayX = o[0]; p[i].fRayY = o[1]; p[i].fDetSX = o[2]; p[i].fDetSY = o[3];
+            p[i].fDetUX = o[4]; p[i].fDetUY = o[5];
+        }
+        ok = astraCUDA::FP(d_vol, W, d_sino, ndet, d, params, &p[0]);
+    } else {
+        std::vector<SFanProjection> p(na);
+        for (int i = 0; i < na; ++i) {
+            const float *o = views + 6 * i;
+            p[i].fSrcX = o[0]; p[i].fSrcY = o[1]; p[i].fDetSX = o[2]; p[i].fDetSY = o[3];
+            p[i].fDetUX = o[4]; p[i].fDetUY = o[5];
+        }
+        ok = astraCUDA::FanFP(d_vol, W, d_sino, ndet, d, params, &p[0]);
+    }
+    return ok ? 0 : 1;
+}
+
+int ref_cuda_bp2d(int kind, const float *views, int W, int H, int na, int ndet, float out_scale, int rays,
+                  int fbp, float *d_sino, float *d_vol)
+{
+    SDimensions d;
+    d.iVolWidth = W; d.iVolHeight = H; d.iProjAngles = na; d.iProjDets = ndet;
+    astraCUDA::SProjectorParams2D params;
+    params.iRaysPerPixelDim = rays;
+    params.fOutputScale = out_scale;
+    bool ok;
+    if (kind == 3) {
+        std::vector<SParProjection> p(na);
+        for (int i = 0; i < na; ++i) {
+            const float *o = views + 6 * i;
+            p[i].fRayX = o[0]; p[i].fRayY = o[1]; p[i].fDetSX = o[2]; p[i].fDetSY = o[3];
+            p[i].fDetUX = o[4]; p[i].fDetUY = o[5];
+        }
+        ok = astraCUDA::BP(d_vol, W, d_sino, ndet, d, params, &p[0]);
+    } else {
+        std::vector<SFanProjection> p(na);
+        for (int i = 0; i < na; ++i) {
+            const float *o = views + 6 * i;
+            p[i].fSrcX = o[0]; p[i].fSrcY = o[1]; p[i].fDetSX = o[2]; p[i].fDetSY = o[3];
+            p[i].fDetUX = o[4]; p[i].fDetUY = o[5];
+        }
+        if (fbp) ok = astraCUDA::FanBP_FBPWeighted(d_vol, W, d_sino, ndet, d, params, &p[0]);
+        else ok = astraCUDA::FanBP(d_vol, W, d_sino, ndet, d, params, &p[0]);
+    }
+    return ok ? 0 : 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,250 @@
+"""GPU parity of the 3D projectors (b2t_fp3d / b2t_bp3d) against the FP64 oracle.
+
+Tolerances: FP32 storage within 1e-5 relative L2 of the FP64 oracle of the
+same ray/voxel model; FP16 / BF16 storage within 1e-3 / 8e-3 of the oracle
+evaluated on the rounded input (the output rounding of the storage type).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+TOL_F32 = 1e-5
+
+
+def _cone_geoms(astra):
+    ang = np.linspace(0, 2 * np.pi, 24, endpoint=False).astype(np.float32)
+    return [
+        ("cone", astra.create_vol_geom(36, 40, 32),
+         astra.create_proj_geom('cone', 1.0, 1.0, 40, 48, ang, 150.0, 80.0)),
+        ("cone_aniso_window", astra.create_vol_geom(30, 34, 26, -16.0, 18.0, -14.0, 16.0, -12.0, 14.0),
+         astra.create_proj_geom('cone', 1.3, 0.8, 36, 44, ang + 0.3, 120.0, 60.0)),
+        ("parallel3d", astra.create_vol_geom(36, 40, 32),
+         astra.create_proj_geom('parallel3d', 1.0, 1.0, 40, 48, ang[:12] / 2)),
+        ("parallel3d_wide", astra.create_vol_geom(28, 30, 20),
+         astra.create_proj_geom('parallel3d', 0.7, 1.3, 30, 50, ang[:15])),
+    ]
+
+
+def _vec_geoms(astra):
+    rng = np.random.default_rng(5)
+    n = 9
+    vecs = []
+    for i in range(n):
+        # source mostly along z for a third of the views (z-major marching)
+        t = 2 * np.pi * i / n
+        if i % 3 == 0:
+            src = np.array([5 * np.cos(t), 5 * np.sin(t), -140.0])
+            det = np.array([0.0, 0.0, 70.0])
+            u = np.array([np.cos(t), np.sin(t), 0.0])
+            v = np.array([-np.sin(t), np.cos(t), 0.0])
+        else:
+            src = np.array([-140 * np.sin(t), 140 * np.cos(t), 3.0])
+            det = np.array([70 * np.sin(t), -70 * np.cos(t), -2.0])
+            u = np.array([np.cos(t), np.sin(t), 0.02])
+            v = np.array([0.01, 0.0, 1.0])
+        u += rng.normal(0, 0.01, 3)
+        vecs.append(np.concatenate([src, det, u, v]))
+    V = np.array(vecs)
+    P = V.copy()
+    P[:, 0:3] = P[:, 3:6] - P[:, 0:3]  # parallel: ray direction = detector - source
+    P[:, 0:3] /= np.linalg.norm(P[:, 0:3], axis=1, keepdims=True)
+    return [
+        ("cone_vec", astra.create_vol_geom(34, 30, 28), astra.create_proj_geom('cone_vec', 38, 42, V)),
+        ("parallel3d_vec", astra.create_vol_geom(34, 30, 28),
+         astra.create_proj_geom('parallel3d_vec', 38, 42, P)),
+    ]
+
+
+def _all_geoms(astra):
+    return _cone_geoms(astra) + _vec_geoms(astra)
+
+
+def _phantom(shape, seed=0):
+    rng = np.random.default_rng(seed)
+    v = rng.random(shape, dtype=np.float32)
+    # smooth-ish content plus an edge so interpolation matters
+    v[:, :, : shape[2] // 3] += 1.0
+    return v.astype(np.float32)
+
+
+def _proj(astra, vg, pg, opts=None):
+    from importlib import import_module
+    P = import_module("astra-toolbox_b200.projector")
+    return P.Projector3D(pg, vg, opts or {})
+
+
+def _oracle_kind(pr):
+    return 2 if pr.geom.kind == 2 else 1
+
+
+@pytest.mark.parametrize("idx", range(6))
+def test_fp3d_vs_oracle(astra, orc, idx):
+    name, vg, pg = _all_geoms(astra)[idx]
+    pr = _proj(astra, vg, pg)
+    vol = _phantom(pr.vol_shape, idx)
+    tv = torch.from_numpy(vol).cuda()
+    tp = torch.full(pr.proj_shape, 7.0, device='cuda')
+    pr.fp(tv, tp)
+    got = tp.cpu().numpy()
+    nv, na, nu = pr.proj_shape
+    ref = orc.fp3d(_oracle_kind(pr), pr.geom.views_array(), vol, nu, nv, pr.geom.vol_scale)
+    assert rel_l2(got, ref) < TOL_F32, name
+
+
+@pytest.mark.parametrize("idx", range(6))
+def test_bp3d_vs_oracle(astra, orc, idx):
+    name, vg, pg = _all_geoms(astra)[idx]
+    pr = _proj(astra, vg, pg)
+    rng = np.random.default_rng(idx + 10)
+    proj = rng.random(pr.proj_shape, dtype=np.float32)
+    tp = torch.from_numpy(proj).cuda()
+    tv = torch.full(pr.vol_shape, -3.0, device='cuda')
+    pr.bp(tp, tv)
+    got = tv.cpu().numpy()
+    ref = orc.bp3d(_oracle_kind(pr), pr.geom.views_array(), proj, pr.vol_shape, pr.geom.vol_scale)
+    assert rel_l2(got, ref) < TOL_F32, name
+
+
+def test_fp_bp_add_mode(astra):
+    name, vg, pg = _cone_geoms(astra)[0]
+    pr = _proj(astra, vg, pg)
+    vol = torch.from_numpy(_phantom(pr.vol_shape)).cuda()
+    p1 = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(vol, p1)
+    p2 = torch.ones(pr.proj_shape, device='cuda')
+    pr.fp(vol, p2, mode=0)
+    assert torch.allclose(p2, p1 + 1.0, rtol=1e-6, atol=1e-5)
+    v1 = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(p1, v1)
+    v2 = torch.full(pr.vol_shape, 2.0, device='cuda')
+    pr.bp(p1, v2, mode=0)
+    assert torch.allclose(v2, v1 + 2.0, rtol=1e-6, atol=1e-4)
+
+
+@pytest.mark.parametrize("kind", ["cone", "parallel3d"])
+def test_supersampling(astra, orc, kind):
+    geoms = {g[0]: g for g in _cone_geoms(astra)}
+    _, vg, pg = geoms[kind]
+    pr = _proj(astra, vg, pg, {'DetectorSuperSampling': 2, 'VoxelSuperSampling': 2})
+    vol = _phantom(pr.vol_shape, 3)
+    nv, na, nu = pr.proj_shape
+    tp = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(torch.from_numpy(vol).cuda(), tp)
+    ref = orc.fp3d(_oracle_kind(pr), pr.geom.views_array(), vol, nu, nv, pr.geom.vol_scale, rays=2)
+    assert rel_l2(tp.cpu().numpy(), ref) < TOL_F32
+    proj = np.random.default_rng(4).random(pr.proj_shape, dtype=np.float32)
+    tv = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(torch.from_numpy(proj).cuda(), tv)
+    refb = orc.bp3d(_oracle_kind(pr), pr.geom.views_array(), proj, pr.vol_shape, pr.geom.vol_scale, rays=2)
+    assert rel_l2(tv.cpu().numpy(), refb) < TOL_F32
+
+
+@pytest.mark.parametrize("kernel,okernel", [("2d_weighting", 3), ("fdk_weighting", 2)])
+def test_bp_weight_kernels(astra, orc, kernel, okernel):
+    _, vg, pg = _cone_geoms(astra)[0]
+    pr = _proj(astra, vg, pg, {'ProjectionKernel': kernel})
+    proj = np.random.default_rng(8).random(pr.proj_shape, dtype=np.float32)
+    tv = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(torch.from_numpy(proj).cuda(), tv)
+    ref = orc.bp3d(2, pr.geom.views_array(), proj, pr.vol_shape, pr.geom.vol_scale, kernel=okernel)
+    assert rel_l2(tv.cpu().numpy(), ref) < TOL_F32
+
+
+@pytest.mark.parametrize("idx", [0, 2, 4, 5])
+def test_matched_bp_is_exact_transpose(astra, orc, idx):
+    name, vg, pg = _all_geoms(astra)[idx]
+    pr = _proj(astra, vg, pg, {'ProjectionKernel': 'matched_bp'})
+    rng = np.random.default_rng(idx)
+    proj = rng.standard_normal(pr.proj_shape).astype(np.float32)
+    tv = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(torch.from_numpy(proj).cuda(), tv)
+    ref = orc.fp3d_transpose(_oracle_kind(pr), pr.geom.views_array(), proj, pr.vol_shape, pr.geom.vol_scale)
+    assert rel_l2(tv.cpu().numpy(), ref) < TOL_F32, name
+    # dot-product test <A x, y> = <x, A^T y> in FP64 accumulation
+    x = rng.standard_normal(pr.vol_shape).astype(np.float32)
+    ax = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(torch.from_numpy(x).cuda(), ax)
+    lhs = float(np.dot(ax.cpu().numpy().ravel().astype(np.float64), proj.ravel().astype(np.float64)))
+    rhs = float(np.dot(x.ravel().astype(np.float64), tv.cpu().numpy().ravel().astype(np.float64)))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5, (lhs, rhs)
+
+
+@pytest.mark.parametrize("dtype,tol", [("float16", 1e-3), ("bfloat16", 8e-3)])
+def test_half_storage(astra, orc, dtype, tol):
+    _, vg, pg = _cone_geoms(astra)[0]
+    pr = _proj(astra, vg, pg)
+    tdt = getattr(torch, dtype)
+    vol = torch.from_numpy(_phantom(pr.vol_shape, 9)).cuda().to(tdt)
+    tp = torch.zeros(pr.proj_shape, device='cuda', dtype=tdt)
+    pr.fp(vol, tp)
+    nv, na, nu = pr.proj_shape
+    ref = orc.fp3d(2, pr.geom.views_array(), vol.float().cpu().numpy(), nu, nv, pr.geom.vol_scale)
+    assert rel_l2(tp.float().cpu().numpy(), ref) < tol
+    tv = torch.zeros(pr.vol_shape, device='cuda', dtype=tdt)
+    pr.bp(tp, tv)
+    refb = orc.bp3d(2, pr.geom.views_array(), tp.float().cpu().numpy(), pr.vol_shape, pr.geom.vol_scale)
+    assert rel_l2(tv.float().cpu().numpy(), refb) < tol
+
+
+def test_edge_single_view_single_slice(astra, orc):
+    vg = astra.create_vol_geom(17, 23, 1)
+    pg = astra.create_proj_geom('cone', 1.0, 1.0, 1, 31, np.array([0.7], dtype=np.float32), 90.0, 40.0)
+    pr = _proj(astra, vg, pg)
+    vol = _phantom(pr.vol_shape, 2)
+    tp = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(torch.from_numpy(vol).cuda(), tp)
+    ref = orc.fp3d(2, pr.geom.views_array(), vol, 31, 1, pr.geom.vol_scale)
+    assert rel_l2(tp.cpu().numpy(), ref) < TOL_F32
+    tv = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(tp, tv)
+    refb = orc.bp3d(2, pr.geom.views_array(), tp.cpu().numpy(), pr.vol_shape, pr.geom.vol_scale)
+    assert rel_l2(tv.cpu().numpy(), refb) < TOL_F32
+
+
+def test_edge_detector_misses_volume(astra):
+    # detector shifted far away: every ray misses, every voxel projects off the detector
+    V = np.array([[0, -100, 0, 0, 50, 500, 1, 0, 0, 0, 0, 1]], dtype=np.float64)
+    vg = astra.create_vol_geom(16, 16, 16)
+    pg = astra.create_proj_geom('cone_vec', 8, 8, V)
+    pr = _proj(astra, vg, pg)
+    tp = torch.full(pr.proj_shape, 5.0, device='cuda')
+    pr.fp(torch.ones(pr.vol_shape, device='cuda'), tp)
+    assert float(tp.abs().max()) == 0.0
+    tv = torch.full(pr.vol_shape, 5.0, device='cuda')
+    pr.bp(torch.ones(pr.proj_shape, device='cuda'), tv)
+    assert float(tv.abs().max()) == 0.0
+
+
+def test_many_views_multiple_launches(astra, orc):
+    # more views than one parameter block holds (448 FP / 640 BP per launch)
+    ang = np.linspace(0, np.pi, 700, endpoint=False).astype(np.float32)
+    vg = astra.create_vol_geom(12, 14, 10)
+    pg = astra.create_proj_geom('cone', 1.0, 1.0, 12, 16, ang, 60.0, 30.0)
+    pr = _proj(astra, vg, pg)
+    vol = _phantom(pr.vol_shape, 1)
+    tp = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(torch.from_numpy(vol).cuda(), tp)
+    ref = orc.fp3d(2, pr.geom.views_array(), vol, 16, 12, pr.geom.vol_scale)
+    assert rel_l2(tp.cpu().numpy(), ref) < TOL_F32
+    proj = tp.cpu().numpy()
+    tv = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(tp, tv)
+    refb = orc.bp3d(2, pr.geom.views_array(), proj, pr.vol_shape, pr.geom.vol_scale)
+    assert rel_l2(tv.cpu().numpy(), refb) < TOL_F32
+
+
+def test_errors_are_raised_not_fallen_back(astra):
+    _, vg, pg = _cone_geoms(astra)[0]
+    pr = _proj(astra, vg, pg)
+    with pytest.raises(astra.AstraError):
+        pr.fp(torch.zeros(3, 3, 3, device='cuda'), torch.zeros(pr.proj_shape, device='cuda'))
+    with pytest.raises(astra.AstraError):
+        _proj(astra, vg, pg, {'DetectorSuperSampling': 0}).fp(
+            torch.zeros(pr.vol_shape, device='cuda'), torch.zeros(pr.proj_shape, device='cuda'))
