@@ -102,6 +102,10 @@ SIGNATURES = {
     "b2t_normalize_views2d": (_I32, [_P, _I32, _U32, _P, _P]),
     "b2t_fp3d": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
     "b2t_bp3d": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
+    "b2t_fp2d": (_I32, [_P, _U32, _P, _SZ, _P, _SZ, _I32, _P]),
+    "b2t_bp2d": (_I32, [_P, _U32, _I32, _P, _SZ, _P, _SZ, _I32, _P]),
+    "b2t_fdk": (_I32, [_P, _I32, _I32, _F, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
+    "b2t_fdk_weight_filter": (_I32, [_P, _I32, _I32, _P, _SZ, _I32, _P]),
     "b2t_vec_op": (_I32, [_I32, _P, _P, _P, _F, _SZ, _P]),
     "b2t_dot_f64": (_I32, [_P, _P, _SZ, _I32, _P, _P]),
 }

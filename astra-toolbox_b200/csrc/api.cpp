@@ -8,6 +8,8 @@
 
 #include "arith.h"
 #include "b2t_internal.h"
+#include "fdk.h"
+#include "proj2d.h"
 #include "proj3d.h"
 
 namespace b2t {
@@ -69,6 +71,36 @@ b2t_status b2t_bp3d(const b2t_geom3d *geom, const b2t_params3d *params, const vo
     clear_error();
     return bp3d_impl(geom, params, proj, proj_pitch, vol, vol_pitch, dtype, mode,
                      static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_fp2d(const b2t_geom2d *geom, uint32_t det_supersample, const float *vol, size_t vol_pitch, float *sino,
+                    size_t sino_pitch, int32_t mode, void *stream)
+{
+    clear_error();
+    return fp2d_impl(geom, det_supersample, vol, vol_pitch, sino, sino_pitch, mode, static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_bp2d(const b2t_geom2d *geom, uint32_t pixel_supersample, int32_t fbp_weight, const float *sino,
+                    size_t sino_pitch, float *vol, size_t vol_pitch, int32_t mode, void *stream)
+{
+    clear_error();
+    return bp2d_impl(geom, pixel_supersample, fbp_weight, sino, sino_pitch, vol, vol_pitch, mode,
+                     static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_fdk(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, float output_scale, const void *proj,
+                   size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, void *stream)
+{
+    clear_error();
+    return fdk_impl(geom, filter, short_scan, output_scale, proj, proj_pitch, vol, vol_pitch, dtype, mode,
+                    static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_fdk_weight_filter(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, void *proj,
+                                 size_t proj_pitch, int32_t dtype, void *stream)
+{
+    clear_error();
+    return fdk_weight_filter_impl(geom, filter, short_scan, proj, proj_pitch, dtype, static_cast<cudaStream_t>(stream));
 }
 
 b2t_status b2t_vec_op(int32_t op, float *out, const float *a, const float *b, float s, size_t n, void *stream)

@@ -1,0 +1,317 @@
+// FDK reconstruction: pre-weighting, Parker short-scan weighting, Ram-Lak
+// row filter and the FDK-weighted cone backprojection.
+//
+// Reference: FDK (cuda/3d/fdk.cu:415-478) runs devFDK_preweight
+// (fdk.cu:70-113), optionally devFDK_ParkerWeight (fdk.cu:115-163), then
+// FDK_Filter (fdk.cu:266-412: per detector row, memset + pitched copy + cuFFT
+// R2C + spectrum multiply + C2R + rescale + copy back), then ConeBP with
+// ker3d_fdk_weighting.
+//
+// Here the weights and the filter are one pass: each CTA loads a few
+// projection rows into shared memory with the weights applied, evaluates the
+// Ram-Lak filter as the Toeplitz product it equals (y_i = sum_j 2 h(|i-j|) x_j
+// with h(0) = 1/4, h(odd k) = -1/(pi k)^2, h(even k != 0) = 0; the reference's
+// zero padding to nextpow2(2 nU) makes its FFT convolution identical to this),
+// and writes the result straight into the zero-padded buffer the
+// backprojector reads, so the filtered projections never make an extra HBM
+// round trip.  The filter uses only the odd taps and a sliding register window
+// of 8 outputs per thread.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "b2t_internal.h"
+#include "fdk.h"
+#include "proj3d.h"
+
+namespace b2t {
+
+namespace {
+
+template <typename T> __device__ __forceinline__ float ldf(const T *p);
+template <> __device__ __forceinline__ float ldf<float>(const float *p) { return __ldg(p); }
+template <> __device__ __forceinline__ float ldf<__half>(const __half *p) { return __half2float(__ldg(p)); }
+template <> __device__ __forceinline__ float ldf<__nv_bfloat16>(const __nv_bfloat16 *p)
+{
+    return __bfloat162float(__ldg(p));
+}
+template <typename T> __device__ __forceinline__ T stf(float v);
+template <> __device__ __forceinline__ float stf<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half stf<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 stf<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+constexpr int FILT_THREADS = 256;
+constexpr int FILT_OUT = 8;  // consecutive outputs per thread
+
+// Parker weight of view a at detector column offset fU (devFDK_ParkerWeight).
+__device__ __forceinline__ float parker_weight(float beta, float fU, const FDKWeights &P)
+{
+    const float gamma = atanf(fU / P.central_ray);
+    const float cfa = P.central_fan;
+    float w;
+    if (beta <= 0.0f) {
+        w = 0.0f;
+    } else if (beta <= 2.0f * (cfa + gamma)) {
+        w = sinf((float)(M_PI / 4.0) * beta / (cfa + gamma));
+        w *= w;
+    } else if (beta <= (float)M_PI + 2.0f * gamma) {
+        w = 1.0f;
+    } else if (beta <= (float)M_PI + 2.0f * cfa) {
+        w = sinf((float)(M_PI / 4.0) * ((float)M_PI + 2.0f * cfa - beta) / (cfa - gamma));
+        w *= w;
+    } else {
+        w = 0.0f;
+    }
+    return w * P.parker_scale;
+}
+
+// One CTA filters `rows` consecutive rows m = v * na + a of proj (pitch in
+// elements).  Shared memory: rows x (3 nu + 32) floats (each row zero-padded
+// by nu + 16 on both sides, which covers every window read, including the
+// look-ahead loads of the last tap) followed by the odd taps.
+template <typename T>
+__global__ void __launch_bounds__(FILT_THREADS) fdk_weight_filter_kernel(
+    const T *src, long long src_pitch, int nu, int na, int nv, int rows, FDKWeights P,
+    const float *__restrict__ rel_angles, int do_filter, T *dst, long long dst_row_stride,
+    long long dst_v_stride)
+{
+    extern __shared__ float sm[];
+    const int PADW = nu + 16;
+    const int W3 = nu + 2 * PADW;
+    float *taps = sm + (size_t)rows * W3;
+    const int nodd = (nu + 1) / 2;
+    const long long m0 = (long long)blockIdx.x * rows;
+    const long long mtot = (long long)na * nv;
+    int nr = (int)min((long long)rows, mtot - m0);
+    if (nr <= 0) return;
+
+    for (int j = threadIdx.x; j < nodd; j += FILT_THREADS) {
+        const double k = 2.0 * j + 1.0;
+        taps[j] = (float)(-2.0 / (M_PI * M_PI * k * k));
+    }
+    // load rows with weights applied, zero padding on both sides
+    for (int r = 0; r < nr; ++r) {
+        const long long m = m0 + r;
+        const int v = (int)(m / na);
+        const int a = (int)(m - (long long)v * na);
+        const float fV = ((float)v - 0.5f * (float)nv + 0.5f) * P.det_vsize + P.zshift;
+        const float beta = P.short_scan ? rel_angles[a] : 0.0f;
+        const T *row = src + m * src_pitch;
+        float *xs = sm + (size_t)r * W3;
+        for (int j = threadIdx.x; j < W3; j += FILT_THREADS) {
+            const int u = j - PADW;
+            float val = 0.0f;
+            if (u >= 0 && u < nu) {
+                const float fU = ((float)u - 0.5f * (float)nu + 0.5f) * P.det_usize;
+                const float rl = sqrtf(P.central_ray * P.central_ray + fU * fU + fV * fV);
+                float w = P.W / rl;
+                if (P.short_scan) w *= parker_weight(beta, fU, P);
+                val = ldf(row + u) * w;
+            }
+            xs[j] = val;
+        }
+    }
+    __syncthreads();
+
+    const int groups = (nu + FILT_OUT - 1) / FILT_OUT;
+    for (int item = threadIdx.x; item < nr * groups; item += FILT_THREADS) {
+        const int r = item / groups;
+        const int i0 = (item - r * groups) * FILT_OUT;
+        const float *xs = sm + (size_t)r * W3 + PADW;  // xs[i] = x_i, i in [-nu-16, 2nu+16)
+        float acc[FILT_OUT];
+        if (do_filter) {
+            float Lw[FILT_OUT + 1], Rw[FILT_OUT + 1];
+            // window for k = 1: L[t] = x[i0 + t - 1], R[t] = x[i0 + t + 1]
+#pragma unroll
+            for (int t = 0; t < FILT_OUT; ++t) {
+                acc[t] = 0.5f * xs[i0 + t];
+                Lw[t] = xs[i0 + t - 1];
+                Rw[t] = xs[i0 + t + 1];
+            }
+            for (int j = 0; j < nodd; ++j) {
+                const float c = taps[j];
+#pragma unroll
+                for (int t = 0; t < FILT_OUT; ++t) acc[t] = fmaf(c, Lw[t] + Rw[t], acc[t]);
+                // advance k by 2: L shifts right by 2 (new x[i0-k-2], x[i0-k-1]),
+                // R shifts left by 2 (new x[i0+8+k], x[i0+9+k])
+                const int k = 2 * j + 1;
+#pragma unroll
+                for (int t = FILT_OUT - 1; t >= 2; --t) Lw[t] = Lw[t - 2];
+                Lw[1] = xs[i0 - k - 1];
+                Lw[0] = xs[i0 - k - 2];
+#pragma unroll
+                for (int t = 0; t < FILT_OUT - 2; ++t) Rw[t] = Rw[t + 2];
+                Rw[FILT_OUT - 2] = xs[i0 + FILT_OUT + k];
+                Rw[FILT_OUT - 1] = xs[i0 + FILT_OUT + k + 1];
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < FILT_OUT; ++t) acc[t] = xs[i0 + t];
+        }
+        const long long m = m0 + r;
+        const int v = (int)(m / na);
+        const int a = (int)(m - (long long)v * na);
+        T *out = dst + (long long)v * dst_v_stride + (long long)a * dst_row_stride;
+#pragma unroll
+        for (int t = 0; t < FILT_OUT; ++t)
+            if (i0 + t < nu) out[i0 + t] = stf<T>(acc[t]);
+    }
+}
+
+}  // namespace
+
+// Circular-orbit parameters from view 0 (FDK, fdk.cu:425-445) and the Parker
+// set-up (FDK_PreWeight, fdk.cu:195-251), with the reference's float / double
+// mix so the weights are the ones the reference applies.
+b2t_status fdk_setup(const b2t_geom3d *g, int short_scan, FDKWeights &P, std::vector<float> &rel)
+{
+    const b2t_dims3d &d = g->dims;
+    const b2t_view3d &p0 = g->views[0];
+    float fDetCX = (float)(p0.det_s[0] + 0.5 * d.det_u * p0.det_u[0]);
+    float fDetCY = (float)(p0.det_s[1] + 0.5 * d.det_u * p0.det_u[1]);
+    float fDetCZ = (float)(p0.det_s[2] + 0.5 * d.det_v * p0.det_v[2]);
+    float fSrcOrigin = (float)std::sqrt(p0.src[0] * p0.src[0] + p0.src[1] * p0.src[1]);
+    float fDetOrigin = std::sqrt(fDetCX * fDetCX + fDetCY * fDetCY);
+    float fDetUSize = (float)std::sqrt(p0.det_u[0] * p0.det_u[0] + p0.det_u[1] * p0.det_u[1]);
+    float fDetVSize = (float)std::abs(p0.det_v[2]);
+    float fZShift = (float)(fDetCZ - p0.src[2]);
+    P.central_ray = fSrcOrigin + fDetOrigin;
+    P.det_usize = fDetUSize;
+    P.det_vsize = fDetVSize;
+    P.zshift = fZShift;
+    const float fW2 = P.central_ray / (fDetUSize * fSrcOrigin);
+    P.W = (float)(P.central_ray * fW2 * (M_PI / 2.0f) / (float)d.angles);
+    P.short_scan = 0;
+    P.parker_scale = 1.0f;
+    P.central_fan = 0.0f;
+    rel.clear();
+    if (short_scan && d.angles > 1) {
+        std::vector<float> angles(d.angles);
+        for (uint32_t i = 0; i < d.angles; ++i)
+            angles[i] = (float)(-std::atan2(g->views[i].src[0], g->views[i].src[1]) + M_PI);
+        float fdA = angles[1] - angles[0];
+        while (fdA < -M_PI) fdA += 2 * M_PI;
+        while (fdA >= M_PI) fdA -= 2 * M_PI;
+        float base = (fdA >= 0.0f) ? angles[0] : angles[d.angles - 1];
+        rel.resize(d.angles);
+        for (uint32_t i = 0; i < d.angles; ++i) {
+            float f = angles[i] - base;
+            while (f >= 2 * M_PI) f -= 2 * M_PI;
+            while (f < 0) f += 2 * M_PI;
+            rel[i] = f;
+        }
+        float range = std::fabs(rel[d.angles - 1] - rel[0]);
+        range /= (float)(d.angles - 1);
+        range *= (float)d.angles;
+        P.parker_scale = (float)(range / M_PI);
+        P.central_fan = std::fabs(std::atan(fDetUSize * (d.det_u * 0.5f) / (fSrcOrigin + fDetOrigin)));
+        P.short_scan = 1;
+    }
+    return B2T_OK;
+}
+
+template <typename T>
+static b2t_status launch_filter(const void *src, size_t src_pitch, const b2t_dims3d &d, const FDKWeights &P,
+                                const float *rel_dev, int do_filter, void *dst, long long dst_row,
+                                long long dst_v, cudaStream_t s)
+{
+    const int nu = d.det_u;
+    const size_t row_bytes = sizeof(float) * (3 * (size_t)nu + 32);
+    const size_t tap_bytes = sizeof(float) * ((nu + 1) / 2 + 1);
+    const size_t budget = 200 * 1024;
+    if (row_bytes + tap_bytes > budget)
+        return fail(B2T_ERR_UNSUPPORTED, "FDK filter: detector rows of %d pixels exceed shared memory", nu);
+    int rows = (int)((budget - tap_bytes) / row_bytes);
+    if (rows > 8) rows = 8;
+    const size_t smem = rows * row_bytes + tap_bytes;
+    auto kern = fdk_weight_filter_kernel<T>;
+    B2T_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                 "FDK filter smem attribute");
+    const long long mtot = (long long)d.angles * d.det_v;
+    const long long blocks = (mtot + rows - 1) / rows;
+    if (blocks > 0x7fffffffLL) return fail(B2T_ERR_UNSUPPORTED, "FDK filter: too many rows");
+    kern<<<(unsigned)blocks, FILT_THREADS, smem, s>>>(static_cast<const T *>(src), (long long)src_pitch, nu,
+                                                      d.angles, d.det_v, rows, P, rel_dev, do_filter,
+                                                      static_cast<T *>(dst), dst_row, dst_v);
+    count_launches(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "FDK weight/filter launch");
+    return B2T_OK;
+}
+
+static b2t_status run_weight_filter(const b2t_geom3d *g, int filter, int short_scan, const void *src,
+                                    size_t src_pitch, void *dst, long long dst_row, long long dst_v, int32_t dtype,
+                                    cudaStream_t s)
+{
+    FDKWeights P;
+    std::vector<float> rel;
+    B2T_TRY(fdk_setup(g, short_scan, P, rel));
+    Scratch rs;
+    const float *rel_dev = nullptr;
+    if (!rel.empty()) {
+        B2T_TRY(rs.alloc(sizeof(float) * rel.size(), s, "FDK Parker angles"));
+        B2T_CUDA_TRY(cudaMemcpyAsync(rs.as<void>(), rel.data(), sizeof(float) * rel.size(), cudaMemcpyHostToDevice, s),
+                     "FDK Parker angles upload");
+        rel_dev = rs.as<float>();
+    }
+    const int do_filter = (filter == B2T_FILTER_RAMLAK) ? 1 : 0;
+    if (dtype == B2T_F32)
+        return launch_filter<float>(src, src_pitch, g->dims, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
+    if (dtype == B2T_F16)
+        return launch_filter<__half>(src, src_pitch, g->dims, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
+    return launch_filter<__nv_bfloat16>(src, src_pitch, g->dims, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
+}
+
+static b2t_status validate_fdk(const b2t_geom3d *g, int filter, int32_t dtype, const char *who)
+{
+    B2T_TRY(validate3d(g, who));
+    if (g->kind != B2T_GEOM_CONE) return fail(B2T_ERR_UNSUPPORTED, "%s: FDK needs a cone geometry", who);
+    if (filter != B2T_FILTER_NONE && filter != B2T_FILTER_RAMLAK)
+        return fail(B2T_ERR_UNSUPPORTED, "%s: only the none and ram-lak filters are implemented", who);
+    if (!dtype_valid(dtype)) return fail(B2T_ERR_INVALID_ARG, "%s: bad dtype %d", who, dtype);
+    return B2T_OK;
+}
+
+b2t_status fdk_weight_filter_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, void *proj,
+                                  size_t proj_pitch, int32_t dtype, cudaStream_t s)
+{
+    B2T_TRY(validate_fdk(g, filter, dtype, "b2t_fdk_weight_filter"));
+    if (!proj) return fail(B2T_ERR_INVALID_ARG, "b2t_fdk_weight_filter: null projections");
+    const b2t_dims3d &d = g->dims;
+    if (proj_pitch == 0) proj_pitch = d.det_u;
+    if (proj_pitch < d.det_u) return fail(B2T_ERR_INVALID_ARG, "b2t_fdk_weight_filter: pitch below row length");
+    // rows are loaded into shared memory before any is written: in place is safe
+    return run_weight_filter(g, filter, short_scan, proj, proj_pitch, proj, (long long)proj_pitch,
+                             (long long)proj_pitch * d.angles, dtype, s);
+}
+
+b2t_status fdk_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, float output_scale, const void *proj,
+                    size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s)
+{
+    B2T_TRY(validate_fdk(g, filter, dtype, "b2t_fdk"));
+    if (!proj || !vol) return fail(B2T_ERR_INVALID_ARG, "b2t_fdk: null data pointer");
+    if (mode != B2T_MODE_ADD && mode != B2T_MODE_SET) return fail(B2T_ERR_INVALID_ARG, "b2t_fdk: bad mode");
+    const b2t_dims3d &d = g->dims;
+    if (proj_pitch == 0) proj_pitch = d.det_u;
+    if (vol_pitch == 0) vol_pitch = d.vol_x;
+    if (proj_pitch < d.det_u || vol_pitch < d.vol_x) return fail(B2T_ERR_INVALID_ARG, "b2t_fdk: pitch below row length");
+    // filtered projections go straight into the zero-padded BP input
+    Scratch sp;
+    const size_t bytes = padded_proj_bytes(d, dtype);
+    B2T_TRY(sp.alloc(bytes, s, "b2t_fdk scratch (filtered projections)"));
+    B2T_CUDA_TRY(cudaMemsetAsync(sp.as<void>(), 0, bytes, s), "b2t_fdk memset");
+    const long long pu = d.det_u + 4;
+    const long long pv = pu * d.angles;
+    char *interior = sp.as<char>() + (2 * pv + 2) * dtype_size(dtype);
+    B2T_TRY(run_weight_filter(g, filter, short_scan, proj, proj_pitch, interior, pu, pv, dtype, s));
+    b2t_params3d p;
+    p.det_supersample = 1;
+    p.voxel_supersample = 1;
+    p.output_scale = output_scale;
+    p.kernel = B2T_KER_FDK_WEIGHTING;
+    return bp3d_from_padded(g, &p, sp.as<void>(), vol, vol_pitch, dtype, mode, s);
+}
+
+}  // namespace b2t

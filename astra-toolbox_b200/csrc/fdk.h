@@ -1,0 +1,28 @@
+// Internal declarations of the FDK module.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "b2tomo.h"
+
+namespace b2t {
+
+// Per-call FDK weighting parameters (circular orbit recovered from view 0).
+struct FDKWeights {
+    float central_ray;   // source-origin + origin-detector distance
+    float det_usize, det_vsize, zshift;
+    float W;             // (D^2 / (du * Rs)) * (pi / 2) / n_angles
+    int short_scan;
+    float parker_scale;  // scanned range / pi
+    float central_fan;   // half fan angle of the central row
+};
+
+b2t_status fdk_setup(const b2t_geom3d *g, int short_scan, FDKWeights &P, std::vector<float> &rel);
+b2t_status fdk_weight_filter_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, void *proj,
+                                  size_t proj_pitch, int32_t dtype, cudaStream_t s);
+b2t_status fdk_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, float output_scale, const void *proj,
+                    size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
+
+}  // namespace b2t

@@ -761,19 +761,34 @@ b2t_status bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *pro
     if (vol_pitch < d.vol_x || proj_pitch < d.det_u)
         return fail(B2T_ERR_INVALID_ARG, "b2t_bp3d: pitch below row length");
 
-    const size_t esz = dtype_size(dtype);
-    const size_t pu = d.det_u + 4;
     Scratch sp;
-    B2T_TRY(sp.alloc(pu * d.angles * (size_t)(d.det_v + 4) * esz, s, "b2t_bp3d scratch (padded projections)"));
+    B2T_TRY(sp.alloc(padded_proj_bytes(d, dtype), s, "b2t_bp3d scratch (padded projections)"));
     if (dtype == B2T_F32) B2T_TRY(pad_projections<float>(proj, proj_pitch, d, sp.as<void>(), s));
     else if (dtype == B2T_F16) B2T_TRY(pad_projections<__half>(proj, proj_pitch, d, sp.as<void>(), s));
     else B2T_TRY(pad_projections<__nv_bfloat16>(proj, proj_pitch, d, sp.as<void>(), s));
+    return bp3d_from_padded(g, p, sp.as<void>(), vol, vol_pitch, dtype, mode, s);
+}
 
+size_t padded_proj_bytes(const b2t_dims3d &d, int32_t dtype)
+{
+    return (size_t)(d.det_u + 4) * d.angles * (size_t)(d.det_v + 4) * dtype_size(dtype);
+}
+
+// BP from a zero-padded projection buffer [v+2][angle][u+2] (pitch det_u + 4,
+// border of 2 texels in u and v), already validated by the caller.
+b2t_status bp3d_from_padded(const b2t_geom3d *g, const b2t_params3d *p, const void *padded, void *vol,
+                            size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s)
+{
+    const b2t_dims3d &d = g->dims;
+    const int ker = p->kernel;
+    const size_t esz = dtype_size(dtype);
+    const size_t pu = d.det_u + 4;
+    if (vol_pitch == 0) vol_pitch = d.vol_x;
     BPLaunch *Lp = new BPLaunch;
     BPLaunch &L = *Lp;
     L.pu = (int)pu;
     L.pv = (long long)pu * d.angles;
-    L.proj = sp.as<char>() + (2 * L.pv + 2) * esz;
+    L.proj = static_cast<const char *>(padded) + (2 * L.pv + 2) * esz;
     L.vol = vol;
     L.vol_pitch = (long long)vol_pitch;
     L.nx = d.vol_x; L.ny = d.vol_y; L.nz = d.vol_z;

@@ -69,6 +69,9 @@ b2t_status fp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
                      void *proj, size_t proj_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *proj, size_t proj_pitch,
                      void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
+size_t padded_proj_bytes(const b2t_dims3d &d, int32_t dtype);
+b2t_status bp3d_from_padded(const b2t_geom3d *g, const b2t_params3d *p, const void *padded, void *vol,
+                            size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *proj,
                              size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype,
                              int32_t mode, cudaStream_t s);

@@ -97,6 +97,47 @@ class Projector3D:
         return vol
 
 
+class Projector2D:
+    """A 'cuda' projector: 2D geometry plus DetectorSuperSampling /
+    PixelSuperSampling (src/CudaProjector2D.cpp:84-100)."""
+
+    def __init__(self, proj_geom, vol_geom, options=None):
+        options = dict(options or {})
+        self.proj_geom = proj_geom
+        self.vol_geom = vol_geom
+        self.geom = Geometry2D(vol_geom, proj_geom)
+        self.det_ss = int(options.get('DetectorSuperSampling', 1))
+        self.pix_ss = int(options.get('PixelSuperSampling', 1))
+        self.gpu_index = int(options.get('GPUIndex', -1))
+        self.vol_shape = self.geom.vol_shape
+        self.proj_shape = self.geom.proj_shape
+
+    def device(self):
+        if self.gpu_index >= 0:
+            return torch.device('cuda', self.gpu_index)
+        return torch.device('cuda', torch.cuda.current_device())
+
+    def fp(self, vol, sino, mode=_lib.MODE_SET):
+        _check_tensor(vol, self.vol_shape, "volume")
+        _check_tensor(sino, self.proj_shape, "sinogram", vol.device)
+        if vol.dtype != torch.float32 or sino.dtype != torch.float32:
+            raise AstraError(1, "2D data must be float32")
+        with torch.cuda.device(vol.device):
+            _lib.call("b2t_fp2d", ctypes.byref(self.geom.c), self.det_ss, vol.data_ptr(), 0, sino.data_ptr(), 0,
+                      mode, stream_handle(vol.device))
+        return sino
+
+    def bp(self, sino, vol, mode=_lib.MODE_SET, fbp_weight=False):
+        _check_tensor(vol, self.vol_shape, "volume")
+        _check_tensor(sino, self.proj_shape, "sinogram", vol.device)
+        if vol.dtype != torch.float32 or sino.dtype != torch.float32:
+            raise AstraError(1, "2D data must be float32")
+        with torch.cuda.device(vol.device):
+            _lib.call("b2t_bp2d", ctypes.byref(self.geom.c), self.pix_ss, int(bool(fbp_weight)), sino.data_ptr(), 0,
+                      vol.data_ptr(), 0, mode, stream_handle(vol.device))
+        return vol
+
+
 def as_device_tensor(x, device, dtype=None):
     """(tensor on device, copy_back) for a numpy array or torch tensor."""
     if isinstance(x, np.ndarray):
@@ -136,3 +177,36 @@ def bp3d(projector, vol, proj, mode=_lib.MODE_SET):
         else:
             vol.copy_(tv.cpu())
     return vol
+
+
+_FILTERS = {'none': _lib.FILTER_NONE, 'ram-lak': _lib.FILTER_RAMLAK, 'ramlak': _lib.FILTER_RAMLAK}
+
+
+def filter_code(name):
+    """FilterType option -> libb2tomo filter code (Filters.cpp:508 names)."""
+    key = (name or 'ram-lak').lower()
+    if key not in _FILTERS:
+        raise AstraError(2, "FilterType %r is not implemented (ram-lak and none are)" % name)
+    return _FILTERS[key]
+
+
+def fdk(projector, proj, vol, short_scan=False, filter_type='ram-lak', output_scale=1.0, mode=_lib.MODE_SET):
+    """FDK of proj into vol (torch CUDA tensors); proj is not modified."""
+    _check_tensor(vol, projector.vol_shape, "volume")
+    _check_tensor(proj, projector.proj_shape, "projection data", vol.device)
+    if vol.dtype != proj.dtype:
+        raise AstraError(1, "volume and projection data must have the same dtype")
+    with torch.cuda.device(vol.device):
+        _lib.call("b2t_fdk", ctypes.byref(projector.geom.c), filter_code(filter_type), int(bool(short_scan)),
+                  float(output_scale), proj.data_ptr(), 0, vol.data_ptr(), 0, _DTYPES[vol.dtype], mode,
+                  stream_handle(vol.device))
+    return vol
+
+
+def fdk_weight_filter(projector, proj, short_scan=False, filter_type='ram-lak'):
+    """FDK pre-weighting and filtering of proj in place."""
+    _check_tensor(proj, projector.proj_shape, "projection data")
+    with torch.cuda.device(proj.device):
+        _lib.call("b2t_fdk_weight_filter", ctypes.byref(projector.geom.c), filter_code(filter_type),
+                  int(bool(short_scan)), proj.data_ptr(), 0, _DTYPES[proj.dtype], stream_handle(proj.device))
+    return proj

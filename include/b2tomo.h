@@ -235,6 +235,41 @@ b2t_status b2t_bp3d(const b2t_geom3d *geom, const b2t_params3d *params,
                     int32_t dtype, int32_t mode, void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* 2D projectors (f32 data)                                                */
+/* ---------------------------------------------------------------------- */
+
+/* sino (+)= A vol.  Replaces astraCUDA::FP (include/astra/cuda/2d/par_fp.h:33,
+ * cuda/2d/par_fp.cu:340) and astraCUDA::FanFP (fan_fp.h:33, fan_fp.cu:260);
+ * det_supersample = iRaysPerDet (DetectorSuperSampling). */
+b2t_status b2t_fp2d(const b2t_geom2d *geom, uint32_t det_supersample, const float *vol, size_t vol_pitch,
+                    float *sino, size_t sino_pitch, int32_t mode, void *stream);
+
+/* vol (+)= B sino.  Replaces astraCUDA::BP (par_bp.h:35, par_bp.cu:224),
+ * FanBP and FanBP_FBPWeighted (fan_bp.h:33-48, fan_bp.cu:380-448);
+ * fbp_weight != 0 selects the fan FBP weight 1/Den^2. */
+b2t_status b2t_bp2d(const b2t_geom2d *geom, uint32_t pixel_supersample, int32_t fbp_weight, const float *sino,
+                    size_t sino_pitch, float *vol, size_t vol_pitch, int32_t mode, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* FDK                                                                     */
+/* ---------------------------------------------------------------------- */
+
+/* FDK reconstruction of a cone geometry with a circular orbit: cosine /
+ * magnification pre-weight, Parker weight if short_scan, Ram-Lak (or no)
+ * filter along u, then the FDK-weighted cone BP; vol (+)= result * scale.
+ * Replaces astraCUDA3d::FDK (include/astra/cuda/3d/mem3d.h:113,
+ * cuda/3d/fdk.cu:415-478).  Unlike the reference, proj is left unmodified:
+ * the filtered projections go to a stream-ordered scratch buffer. */
+b2t_status b2t_fdk(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, float output_scale,
+                   const void *proj, size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype,
+                   int32_t mode, void *stream);
+
+/* Pre-weighting (+ Parker) and filtering of proj in place: FDK_PreWeight +
+ * FDK_Filter (cuda/3d/fdk.cu:168-412). */
+b2t_status b2t_fdk_weight_filter(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, void *proj,
+                                 size_t proj_pitch, int32_t dtype, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* element-wise operations and reductions                                  */
 /* ---------------------------------------------------------------------- */
 

@@ -1,5 +1,5 @@
 // ref_wrap.cu -- extern "C" entry points into the reference ASTRA Toolbox,
-// built from its own sources by oracle/build_ref.sh into oracle/_ref/.
+// built from its own sources by oracle/ref.mk into oracle/_ref/.
 //
 // TEST INFRASTRUCTURE ONLY.  These wrappers let the tests (and the reference
 // leg of bench.py) call the reference's geometry conversion, its CUDA
@@ -90,6 +90,24 @@ cudaPitchedPtr pitched(const float *p, int x, int y)
 {
     return make_cudaPitchedPtr((void *)p, sizeof(float) * x, x, y);
 }
+
+// The reference binds 2D data as pitched textures, which need the pitch
+// alignment cudaMallocPitch provides; stage tightly packed buffers through one.
+struct Pitched2D {
+    float *ptr = nullptr;
+    size_t pitch = 0;  // bytes
+    int w = 0, h = 0;
+    bool alloc(int width, int height)
+    {
+        w = width;
+        h = height;
+        return cudaMallocPitch((void **)&ptr, &pitch, sizeof(float) * width, height) == cudaSuccess;
+    }
+    void upload(const float *src) { cudaMemcpy2D(ptr, pitch, src, sizeof(float) * w, sizeof(float) * w, h, cudaMemcpyDeviceToDevice); }
+    void download(float *dst) { cudaMemcpy2D(dst, sizeof(float) * w, ptr, pitch, sizeof(float) * w, h, cudaMemcpyDeviceToDevice); }
+    unsigned elems() const { return (unsigned)(pitch / sizeof(float)); }
+    ~Pitched2D() { if (ptr) cudaFree(ptr); }
+};
 
 }  // namespace
 
@@ -262,8 +280,15 @@ int ref_cuda_fdk(const double *views, int nx, int ny, int nz, int na, int nu, in
     for (int i = 0; i < na; ++i) p[i] = to_cone(views + 12 * i);
     SFilterConfig cfg;
     cfg.m_eType = FILTER_RAMLAK;
-    bool ok = astraCUDA3d::FDK(pitched(d_vol, nx, ny), pitched(d_proj, nu, na), &p[0], d, params,
-                               short_scan != 0, cfg);
+    // The weighting kernels (devFDK_preweight, devFDK_ParkerWeight) do not
+    // bound-check u and rely on the row padding of pitched allocations, so
+    // the projections are staged through a cudaMallocPitch buffer as in ASTRA.
+    Pitched2D P;
+    if (!P.alloc(nu, na * nv)) return 2;
+    P.upload(d_proj);
+    cudaPitchedPtr pp = make_cudaPitchedPtr(P.ptr, P.pitch, nu, na);
+    bool ok = astraCUDA3d::FDK(pitched(d_vol, nx, ny), pp, &p[0], d, params, short_scan != 0, cfg);
+    P.download(d_proj);
     return ok ? 0 : 1;
 }
 
@@ -284,7 +309,12 @@ int ref_cuda_fp2d(int kind, const float *views, int W, int H, int na, int ndet, 
             p[i].fRayX = o[0]; p[i].fRayY = o[1]; p[i].fDetSX = o[2]; p[i].fDetSY = o[3];
             p[i].fDetUX = o[4]; p[i].fDetUY = o[5];
         }
-        ok = astraCUDA::FP(d_vol, W, d_sino, ndet, d, params, &p[0]);
+        Pitched2D V, S;
+        if (!V.alloc(W, H) || !S.alloc(ndet, na)) return 2;
+        V.upload(d_vol);
+        S.upload(d_sino);
+        ok = astraCUDA::FP(V.ptr, V.elems(), S.ptr, S.elems(), d, params, &p[0]);
+        S.download(d_sino);
     } else {
         std::vector<SFanProjection> p(na);
         for (int i = 0; i < na; ++i) {
@@ -292,7 +322,12 @@ int ref_cuda_fp2d(int kind, const float *views, int W, int H, int na, int ndet, 
             p[i].fSrcX = o[0]; p[i].fSrcY = o[1]; p[i].fDetSX = o[2]; p[i].fDetSY = o[3];
             p[i].fDetUX = o[4]; p[i].fDetUY = o[5];
         }
-        ok = astraCUDA::FanFP(d_vol, W, d_sino, ndet, d, params, &p[0]);
+        Pitched2D V, S;
+        if (!V.alloc(W, H) || !S.alloc(ndet, na)) return 2;
+        V.upload(d_vol);
+        S.upload(d_sino);
+        ok = astraCUDA::FanFP(V.ptr, V.elems(), S.ptr, S.elems(), d, params, &p[0]);
+        S.download(d_sino);
     }
     return ok ? 0 : 1;
 }
@@ -313,7 +348,12 @@ int ref_cuda_bp2d(int kind, const float *views, int W, int H, int na, int ndet, 
             p[i].fRayX = o[0]; p[i].fRayY = o[1]; p[i].fDetSX = o[2]; p[i].fDetSY = o[3];
             p[i].fDetUX = o[4]; p[i].fDetUY = o[5];
         }
-        ok = astraCUDA::BP(d_vol, W, d_sino, ndet, d, params, &p[0]);
+        Pitched2D V, S;
+        if (!V.alloc(W, H) || !S.alloc(ndet, na)) return 2;
+        V.upload(d_vol);
+        S.upload(d_sino);
+        ok = astraCUDA::BP(V.ptr, V.elems(), S.ptr, S.elems(), d, params, &p[0]);
+        V.download(d_vol);
     } else {
         std::vector<SFanProjection> p(na);
         for (int i = 0; i < na; ++i) {
@@ -321,8 +361,13 @@ int ref_cuda_bp2d(int kind, const float *views, int W, int H, int na, int ndet, 
             p[i].fSrcX = o[0]; p[i].fSrcY = o[1]; p[i].fDetSX = o[2]; p[i].fDetSY = o[3];
             p[i].fDetUX = o[4]; p[i].fDetUY = o[5];
         }
-        if (fbp) ok = astraCUDA::FanBP_FBPWeighted(d_vol, W, d_sino, ndet, d, params, &p[0]);
-        else ok = astraCUDA::FanBP(d_vol, W, d_sino, ndet, d, params, &p[0]);
+        Pitched2D V, S;
+        if (!V.alloc(W, H) || !S.alloc(ndet, na)) return 2;
+        V.upload(d_vol);
+        S.upload(d_sino);
+        if (fbp) ok = astraCUDA::FanBP_FBPWeighted(V.ptr, V.elems(), S.ptr, S.elems(), d, params, &p[0]);
+        else ok = astraCUDA::FanBP(V.ptr, V.elems(), S.ptr, S.elems(), d, params, &p[0]);
+        V.download(d_vol);
     }
     return ok ? 0 : 1;
 }

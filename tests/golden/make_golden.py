@@ -88,7 +88,11 @@ def cases():
         out.append(("bp3d_" + name, "bp3d", vg, pg, {}))
     out.append(("fp3d_cone_ss2", "fp3d", cone[1], cone[2], {'rays': 2}))
     out.append(("bp3d_cone_ss2", "bp3d", cone[1], cone[2], {'rays': 2}))
-    out.append(("bp3d_cone_2dw", "bp3d", cone[1], cone[2], {'kernel': 3}))
+    # 2d_weighting is meant for single-slice volumes: the reference launches it
+    # with one z voxel per thread on a grid of ceil(nz / 6) blocks
+    # (cuda/3d/cone_bp.cu:357-358), so on thicker volumes it fills only every
+    # sixth slice
+    out.append(("bp3d_cone_2dw", "bp3d", vol_geom3(36, 40, 1), cone[2], {'kernel': 3}))
     out.append(("bp3d_cone_fdkw", "bp3d", cone[1], cone[2], {'kernel': 2}))
     ang72 = np.linspace(0, 2 * np.pi, 72, endpoint=False).astype(np.float32)
     fdkg = {'type': 'cone', 'DetectorSpacingX': 1.0, 'DetectorSpacingY': 1.0, 'DetectorRowCount': 40,
