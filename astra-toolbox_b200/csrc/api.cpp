@@ -57,6 +57,14 @@ b2t_status b2t_set_device(int32_t device)
     return B2T_OK;
 }
 
+b2t_status b2t_device_errors(uint32_t *flags)
+{
+    clear_error();
+    if (!flags) return fail(B2T_ERR_INVALID_ARG, "b2t_device_errors: null pointer");
+    B2T_CUDA_TRY(cudaDeviceSynchronize(), "b2t_device_errors synchronize");
+    return device_errors_impl(flags);
+}
+
 b2t_status b2t_fp3d(const b2t_geom3d *geom, const b2t_params3d *params, const void *vol, size_t vol_pitch,
                     void *proj, size_t proj_pitch, int32_t dtype, int32_t mode, void *stream)
 {

@@ -302,7 +302,7 @@ b2t_status fdk_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, flo
     const size_t bytes = padded_proj_bytes(d, dtype);
     B2T_TRY(sp.alloc(bytes, s, "b2t_fdk scratch (filtered projections)"));
     B2T_CUDA_TRY(cudaMemsetAsync(sp.as<void>(), 0, bytes, s), "b2t_fdk memset");
-    const long long pu = d.det_u + 4;
+    const long long pu = (long long)padded_pu(d.det_u);
     const long long pv = pu * d.angles;
     char *interior = sp.as<char>() + (2 * pv + 2) * dtype_size(dtype);
     B2T_TRY(run_weight_filter(g, filter, short_scan, proj, proj_pitch, interior, pu, pv, dtype, s));

@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "b2t_internal.h"
@@ -129,12 +130,12 @@ __global__ void pad_volume_zxy(const T *__restrict__ src, size_t src_pitch, int 
     }
 }
 
-// dst[v+2][a][u+2] = src[v][a][u], zero border of width 2 in u and v.
+// dst[v+2][a][u+2] = src[v][a][u], zero border of width 2 in u and v (and
+// zero columns up to the row pitch pu).
 template <typename T>
-__global__ void pad_proj(const T *__restrict__ src, size_t src_pitch, int nu, int na, int nv,
+__global__ void pad_proj(const T *__restrict__ src, size_t src_pitch, int nu, int na, int nv, int pu,
                          T *__restrict__ dst)
 {
-    const int pu = nu + 4;
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     const int a = blockIdx.y;
     const int v = blockIdx.z;
@@ -426,8 +427,9 @@ template <typename T>
 b2t_status pad_projections(const void *proj, size_t pitch, const b2t_dims3d &d, void *pp,
                            cudaStream_t s)
 {
-    dim3 grid((d.det_u + 4 + 127) / 128, d.angles, d.det_v + 4);
-    pad_proj<T><<<grid, 128, 0, s>>>(static_cast<const T *>(proj), pitch, d.det_u, d.angles, d.det_v,
+    const int pu = (int)padded_pu(d.det_u);
+    dim3 grid((pu + 127) / 128, d.angles, d.det_v + 4);
+    pad_proj<T><<<grid, 128, 0, s>>>(static_cast<const T *>(proj), pitch, d.det_u, d.angles, d.det_v, pu,
                                      static_cast<T *>(pp));
     count_launches(1);
     B2T_CUDA_TRY(cudaGetLastError(), "pad_proj launch");
@@ -593,6 +595,14 @@ void bp_view_coeffs(int kind, int kernel, const b2t_view3d &w, const float *vs, 
         }
         o.den = make_float4(0.0f, 0.0f, 0.0f, (float)sc);
     }
+}
+
+// B2T_SIMPLE_BP=1 selects the direct-load backprojector instead of the
+// TMA-staged one (both implement the same model; tests compare them).
+bool force_simple_bp()
+{
+    const char *e = getenv("B2T_SIMPLE_BP");
+    return e && e[0] == '1';
 }
 
 b2t_status validate3d(const b2t_geom3d *g, const char *who)
@@ -771,7 +781,7 @@ b2t_status bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *pro
 
 size_t padded_proj_bytes(const b2t_dims3d &d, int32_t dtype)
 {
-    return (size_t)(d.det_u + 4) * d.angles * (size_t)(d.det_v + 4) * dtype_size(dtype);
+    return padded_pu(d.det_u) * d.angles * (size_t)(d.det_v + 4) * dtype_size(dtype);
 }
 
 // BP from a zero-padded projection buffer [v+2][angle][u+2] (pitch det_u + 4,
@@ -782,8 +792,15 @@ b2t_status bp3d_from_padded(const b2t_geom3d *g, const b2t_params3d *p, const vo
     const b2t_dims3d &d = g->dims;
     const int ker = p->kernel;
     const size_t esz = dtype_size(dtype);
-    const size_t pu = d.det_u + 4;
+    const size_t pu = padded_pu(d.det_u);
     if (vol_pitch == 0) vol_pitch = d.vol_x;
+    const float *vs0 = g->vol_scale;
+    if (p->voxel_supersample == 1 && !force_simple_bp()) {
+        const float outs = (g->kind == B2T_GEOM_CONE && ker == B2T_KER_FDK_WEIGHTING)
+                               ? p->output_scale / vs0[0]
+                               : p->output_scale * (vs0[0] * vs0[1] * vs0[2]);
+        return bp3d_tma(g, ker, outs, padded, vol, vol_pitch, dtype, mode, s);
+    }
     BPLaunch *Lp = new BPLaunch;
     BPLaunch &L = *Lp;
     L.pu = (int)pu;

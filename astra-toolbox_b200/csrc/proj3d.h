@@ -2,6 +2,7 @@
 // and host entry points behind b2t_fp3d / b2t_bp3d).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "b2tomo.h"
@@ -58,12 +59,42 @@ struct BPLaunch {
     BPView views[BP_MAX_VIEWS];
 };
 
+// TMA-staged backprojection (bp3d_tma.cu): voxel block, tile box, stages.
+constexpr int BPT_Z = 16;          // voxels per thread along z
+constexpr int BPT_BU = 80;         // tile width in texels (u), multiple of 8
+constexpr int BPT_BV = 64;         // tile height in texels (v)
+constexpr int BPT_STAGES = 3;
+constexpr int BPT_MAX_VIEWS = 640;
+
+struct alignas(64) BPTmaLaunch {
+    CUtensorMap tmap;       // padded projections: dims (pu, angles, det_v + 4)
+    const void *proj;       // padded projections at texel (u=0, angle 0, v=0)
+    long long pv;
+    int pu;
+    void *vol;
+    long long vol_pitch;
+    int nx, ny, nz, nu, nv, na;
+    int a0, nviews, accumulate;
+    float out_scale;
+    BPView views[BPT_MAX_VIEWS];
+};
+
+// Row pitch (elements) of the zero-padded projection buffer: det_u plus a
+// 2-texel border on each side, rounded up to 8 so rows are 16-byte aligned
+// for TMA in every storage type.
+inline size_t padded_pu(uint32_t det_u) { return ((size_t)det_u + 4 + 7) & ~(size_t)7; }
+
+b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *padded, void *vol, size_t vol_pitch,
+                    int32_t dtype, int32_t mode, cudaStream_t s);
+b2t_status device_errors_impl(uint32_t *flags);
+
 int dominant_axis(int kind, const b2t_view3d &w, const b2t_dims3d &d);
 void fp_view_coeffs(int kind, const b2t_view3d &w, const b2t_dims3d &d, int dir, FPView &o);
 void fp_scale(int kind, int dir, const float *vs, bool force_noncube, float out_scale, float &f1,
               float &f2, float &mul);
 void bp_view_coeffs(int kind, int kernel, const b2t_view3d &w, const float *vs, BPView &o);
 b2t_status validate3d(const b2t_geom3d *g, const char *who);
+bool force_simple_bp();
 
 b2t_status fp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch,
                      void *proj, size_t proj_pitch, int32_t dtype, int32_t mode, cudaStream_t s);

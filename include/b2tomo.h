@@ -58,6 +58,11 @@ uint64_t b2t_kernel_launches(void);
 /* Select the CUDA device for this host thread (astraCUDA::setGPUIndex,
  * cuda/2d/astra.cu:60-75). */
 b2t_status b2t_set_device(int32_t device);
+/* Read and clear the device-side error bits of the current device (bit 0:
+ * a bounded wait inside a kernel gave up; the kernel returned early and its
+ * output is incomplete).  Synchronises the device.  The reference has no
+ * device-side waits and no counterpart. */
+b2t_status b2t_device_errors(uint32_t *flags);
 
 /* ---------------------------------------------------------------------- */
 /* enumerations                                                            */
