@@ -8,15 +8,23 @@ Surface mirrored from the reference (python/astra/__init__.py):
 create_vol_geom, create_proj_geom, projector3d / projector ('cuda3d', 'cuda'),
 data3d / data2d, algorithm (FP3D_CUDA, BP3D_CUDA, FDK_CUDA, SIRT3D_CUDA,
 CGLS3D_CUDA, FP_CUDA, BP_CUDA, SIRT_CUDA, CGLS_CUDA, FBP_CUDA), experimental
-(direct_FP3D / direct_BP3D), create_sino3d_gpu / create_backprojection3d_gpu.
+(direct_FP3D / direct_BP3D), create_sino3d_gpu / create_backprojection3d_gpu,
+create_sino / create_backprojection / create_reconstruction, astra_dict.
 Every computation runs in libb2tomo.so (sm_100a); there is no CPU path.
 """
 from . import _lib
 from ._lib import AstraError
 from .geometry import create_proj_geom, create_vol_geom
-from .projector import Projector3D
+from .projector import Projector2D, Projector3D
+from . import algorithm, data2d, data3d, experimental, projector, projector3d  # noqa: F401
+from .algorithm import astra_dict
+from .creators import (create_backprojection, create_backprojection3d_gpu, create_projector,  # noqa: F401
+                       create_reconstruction, create_sino, create_sino3d_gpu)
 
-__all__ = ["AstraError", "create_proj_geom", "create_vol_geom", "Projector3D"]
+__all__ = ["AstraError", "create_proj_geom", "create_vol_geom", "Projector2D", "Projector3D", "algorithm",
+           "data2d", "data3d", "experimental", "projector", "projector3d", "astra_dict", "create_projector",
+           "create_sino3d_gpu", "create_backprojection3d_gpu", "create_sino", "create_backprojection",
+           "create_reconstruction"]
 
 
 def load_library():

@@ -80,6 +80,15 @@ class VolGeom2D(ctypes.Structure):
                 ("max_x", ctypes.c_float), ("min_y", ctypes.c_float), ("max_y", ctypes.c_float)]
 
 
+ALGO_SIRT, ALGO_CGLS = 1, 2
+
+
+class AlgoOptions(ctypes.Structure):
+    _fields_ = [("relaxation", ctypes.c_float), ("use_min", ctypes.c_int32), ("min_value", ctypes.c_float),
+                ("use_max", ctypes.c_int32), ("max_value", ctypes.c_float), ("vol_mask", ctypes.c_void_p),
+                ("sino_mask", ctypes.c_void_p), ("min_mask", ctypes.c_void_p), ("max_mask", ctypes.c_void_p)]
+
+
 _P = ctypes.c_void_p
 _SZ = ctypes.c_size_t
 _I32 = ctypes.c_int32
@@ -107,6 +116,14 @@ SIGNATURES = {
     "b2t_bp2d": (_I32, [_P, _U32, _I32, _P, _SZ, _P, _SZ, _I32, _P]),
     "b2t_fdk": (_I32, [_P, _I32, _I32, _F, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
     "b2t_fdk_weight_filter": (_I32, [_P, _I32, _I32, _P, _SZ, _I32, _P]),
+    "b2t_filter_rows": (_I32, [_P, _SZ, _U32, _SZ, _I32, _P]),
+    "b2t_fbp2d": (_I32, [_P, _I32, _I32, _P, _SZ, _P, _SZ, _I32, _P]),
+    "b2t_algo_create3d": (_I32, [_I32, _P, _P, _P, _P]),
+    "b2t_algo_create2d": (_I32, [_I32, _P, _U32, _U32, _P, _P]),
+    "b2t_algo_run": (_I32, [_P, _P, _P, _I32, _I32, _P]),
+    "b2t_algo_residual_norm": (_I32, [_P, _P, _P, _P, _P]),
+    "b2t_algo_abort": (None, [_P]),
+    "b2t_algo_destroy": (None, [_P]),
     "b2t_vec_op": (_I32, [_I32, _P, _P, _P, _F, _SZ, _P]),
     "b2t_dot_f64": (_I32, [_P, _P, _SZ, _I32, _P, _P]),
 }

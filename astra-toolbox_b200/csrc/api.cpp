@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <string>
 
+#include "algorithms.h"
 #include "arith.h"
 #include "b2t_internal.h"
 #include "fdk.h"
@@ -110,6 +111,51 @@ b2t_status b2t_fdk_weight_filter(const b2t_geom3d *geom, int32_t filter, int32_t
     clear_error();
     return fdk_weight_filter_impl(geom, filter, short_scan, proj, proj_pitch, dtype, static_cast<cudaStream_t>(stream));
 }
+
+b2t_status b2t_filter_rows(float *data, size_t nrows, uint32_t n, size_t pitch, int32_t filter, void *stream)
+{
+    clear_error();
+    return filter_rows_impl(data, nrows, n, pitch, filter, static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_fbp2d(const b2t_geom2d *geom, int32_t filter, int32_t short_scan, const float *sino,
+                     size_t sino_pitch, float *vol, size_t vol_pitch, int32_t mode, void *stream)
+{
+    clear_error();
+    return fbp2d_impl(geom, filter, short_scan, sino, sino_pitch, vol, vol_pitch, mode,
+                      static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_algo_create3d(int32_t type, const b2t_geom3d *geom, const b2t_params3d *params,
+                             const b2t_algo_options *options, b2t_algo **out)
+{
+    clear_error();
+    return algo_create3d_impl(type, geom, params, options, out);
+}
+
+b2t_status b2t_algo_create2d(int32_t type, const b2t_geom2d *geom, uint32_t det_supersample,
+                             uint32_t pixel_supersample, const b2t_algo_options *options, b2t_algo **out)
+{
+    clear_error();
+    return algo_create2d_impl(type, geom, det_supersample, pixel_supersample, options, out);
+}
+
+b2t_status b2t_algo_run(b2t_algo *algo, const float *sino, float *vol, int32_t iterations, int32_t use_graph,
+                        void *stream)
+{
+    clear_error();
+    return algo_run_impl(algo, sino, vol, iterations, use_graph, static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_algo_residual_norm(b2t_algo *algo, const float *sino, const float *vol, double *norm, void *stream)
+{
+    clear_error();
+    return algo_residual_impl(algo, sino, vol, norm, static_cast<cudaStream_t>(stream));
+}
+
+void b2t_algo_abort(b2t_algo *algo) { algo_abort_impl(algo); }
+
+void b2t_algo_destroy(b2t_algo *algo) { algo_destroy_impl(algo); }
 
 b2t_status b2t_vec_op(int32_t op, float *out, const float *a, const float *b, float s, size_t n, void *stream)
 {

@@ -25,6 +25,7 @@
 
 #include "b2t_internal.h"
 #include "fdk.h"
+#include "proj2d.h"
 #include "proj3d.h"
 
 namespace b2t {
@@ -105,10 +106,13 @@ __global__ void __launch_bounds__(FILT_THREADS) fdk_weight_filter_kernel(
             const int u = j - PADW;
             float val = 0.0f;
             if (u >= 0 && u < nu) {
-                const float fU = ((float)u - 0.5f * (float)nu + 0.5f) * P.det_usize;
-                const float rl = sqrtf(P.central_ray * P.central_ray + fU * fU + fV * fV);
-                float w = P.W / rl;
-                if (P.short_scan) w *= parker_weight(beta, fU, P);
+                float w = 1.0f;
+                if (P.apply) {
+                    const float fU = ((float)u - 0.5f * (float)nu + 0.5f) * P.det_usize;
+                    const float rl = sqrtf(P.central_ray * P.central_ray + fU * fU + fV * fV);
+                    w = P.W / rl;
+                    if (P.short_scan) w *= parker_weight(beta, fU, P);
+                }
                 val = ldf(row + u) * w;
             }
             xs[j] = val;
@@ -163,9 +167,48 @@ __global__ void __launch_bounds__(FILT_THREADS) fdk_weight_filter_kernel(
 
 }  // namespace
 
-// Circular-orbit parameters from view 0 (FDK, fdk.cu:425-445) and the Parker
-// set-up (FDK_PreWeight, fdk.cu:195-251), with the reference's float / double
-// mix so the weights are the ones the reference applies.
+// Weights of FDK_PreWeight (fdk.cu:168-264) for a circular orbit given by its
+// source-origin and origin-detector distances, detector pixel sizes, z shift
+// and per-view angles; Parker set-up as there (relative angles, scanned range,
+// central fan angle), with the reference's float / double mix.
+void fdk_weights(float fSrcOrigin, float fDetOrigin, float fZShift, float fDetUSize, float fDetVSize,
+                 uint32_t n_angles, uint32_t det_u, const float *angles, int short_scan, FDKWeights &P,
+                 std::vector<float> &rel)
+{
+    P.apply = 1;
+    P.central_ray = fSrcOrigin + fDetOrigin;
+    P.det_usize = fDetUSize;
+    P.det_vsize = fDetVSize;
+    P.zshift = fZShift;
+    const float fW2 = P.central_ray / (fDetUSize * fSrcOrigin);
+    P.W = (float)(P.central_ray * fW2 * (M_PI / 2.0f) / (float)n_angles);
+    P.short_scan = 0;
+    P.parker_scale = 1.0f;
+    P.central_fan = 0.0f;
+    rel.clear();
+    if (short_scan && n_angles > 1) {
+        float fdA = angles[1] - angles[0];
+        while (fdA < -M_PI) fdA += 2 * M_PI;
+        while (fdA >= M_PI) fdA -= 2 * M_PI;
+        float base = (fdA >= 0.0f) ? angles[0] : angles[n_angles - 1];
+        rel.resize(n_angles);
+        for (uint32_t i = 0; i < n_angles; ++i) {
+            float f = angles[i] - base;
+            while (f >= 2 * M_PI) f -= 2 * M_PI;
+            while (f < 0) f += 2 * M_PI;
+            rel[i] = f;
+        }
+        float range = std::fabs(rel[n_angles - 1] - rel[0]);
+        range /= (float)(n_angles - 1);
+        range *= (float)n_angles;
+        P.parker_scale = (float)(range / M_PI);
+        P.central_fan = std::fabs(std::atan(fDetUSize * (det_u * 0.5f) / (fSrcOrigin + fDetOrigin)));
+        P.short_scan = 1;
+    }
+}
+
+// Circular-orbit parameters from view 0 and the per-view angles, exactly as
+// FDK() derives them (fdk.cu:425-445).
 b2t_status fdk_setup(const b2t_geom3d *g, int short_scan, FDKWeights &P, std::vector<float> &rel)
 {
     const b2t_dims3d &d = g->dims;
@@ -178,38 +221,11 @@ b2t_status fdk_setup(const b2t_geom3d *g, int short_scan, FDKWeights &P, std::ve
     float fDetUSize = (float)std::sqrt(p0.det_u[0] * p0.det_u[0] + p0.det_u[1] * p0.det_u[1]);
     float fDetVSize = (float)std::abs(p0.det_v[2]);
     float fZShift = (float)(fDetCZ - p0.src[2]);
-    P.central_ray = fSrcOrigin + fDetOrigin;
-    P.det_usize = fDetUSize;
-    P.det_vsize = fDetVSize;
-    P.zshift = fZShift;
-    const float fW2 = P.central_ray / (fDetUSize * fSrcOrigin);
-    P.W = (float)(P.central_ray * fW2 * (M_PI / 2.0f) / (float)d.angles);
-    P.short_scan = 0;
-    P.parker_scale = 1.0f;
-    P.central_fan = 0.0f;
-    rel.clear();
-    if (short_scan && d.angles > 1) {
-        std::vector<float> angles(d.angles);
-        for (uint32_t i = 0; i < d.angles; ++i)
-            angles[i] = (float)(-std::atan2(g->views[i].src[0], g->views[i].src[1]) + M_PI);
-        float fdA = angles[1] - angles[0];
-        while (fdA < -M_PI) fdA += 2 * M_PI;
-        while (fdA >= M_PI) fdA -= 2 * M_PI;
-        float base = (fdA >= 0.0f) ? angles[0] : angles[d.angles - 1];
-        rel.resize(d.angles);
-        for (uint32_t i = 0; i < d.angles; ++i) {
-            float f = angles[i] - base;
-            while (f >= 2 * M_PI) f -= 2 * M_PI;
-            while (f < 0) f += 2 * M_PI;
-            rel[i] = f;
-        }
-        float range = std::fabs(rel[d.angles - 1] - rel[0]);
-        range /= (float)(d.angles - 1);
-        range *= (float)d.angles;
-        P.parker_scale = (float)(range / M_PI);
-        P.central_fan = std::fabs(std::atan(fDetUSize * (d.det_u * 0.5f) / (fSrcOrigin + fDetOrigin)));
-        P.short_scan = 1;
-    }
+    std::vector<float> angles(d.angles);
+    for (uint32_t i = 0; i < d.angles; ++i)
+        angles[i] = (float)(-std::atan2(g->views[i].src[0], g->views[i].src[1]) + M_PI);
+    fdk_weights(fSrcOrigin, fDetOrigin, fZShift, fDetUSize, fDetVSize, d.angles, d.det_u, angles.data(), short_scan,
+                P, rel);
     return B2T_OK;
 }
 
@@ -241,6 +257,101 @@ static b2t_status launch_filter(const void *src, size_t src_pitch, const b2t_dim
     return B2T_OK;
 }
 
+static b2t_status run_filter(const b2t_dims3d &d, const FDKWeights &P, const std::vector<float> &rel, int filter,
+                             const void *src, size_t src_pitch, void *dst, long long dst_row, long long dst_v,
+                             int32_t dtype, cudaStream_t s)
+{
+    Scratch rs;
+    const float *rel_dev = nullptr;
+    if (!rel.empty()) {
+        B2T_TRY(rs.alloc(sizeof(float) * rel.size(), s, "Parker angles"));
+        B2T_CUDA_TRY(cudaMemcpyAsync(rs.as<void>(), rel.data(), sizeof(float) * rel.size(), cudaMemcpyHostToDevice, s),
+                     "Parker angles upload");
+        rel_dev = rs.as<float>();
+    }
+    const int do_filter = (filter == B2T_FILTER_RAMLAK) ? 1 : 0;
+    if (dtype == B2T_F32) return launch_filter<float>(src, src_pitch, d, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
+    if (dtype == B2T_F16) return launch_filter<__half>(src, src_pitch, d, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
+    return launch_filter<__nv_bfloat16>(src, src_pitch, d, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
+}
+
+b2t_status filter_rows_impl(float *data, size_t nrows, uint32_t n, size_t pitch, int32_t filter, cudaStream_t s)
+{
+    if (!data) return fail(B2T_ERR_INVALID_ARG, "b2t_filter_rows: null data");
+    if (filter != B2T_FILTER_NONE && filter != B2T_FILTER_RAMLAK)
+        return fail(B2T_ERR_UNSUPPORTED, "b2t_filter_rows: only the none and ram-lak filters are implemented");
+    if (n == 0 || nrows == 0) return B2T_OK;
+    if (nrows > 0xffffffffu) return fail(B2T_ERR_INVALID_ARG, "b2t_filter_rows: too many rows");
+    if (pitch == 0) pitch = n;
+    if (pitch < n) return fail(B2T_ERR_INVALID_ARG, "b2t_filter_rows: pitch below row length");
+    b2t_dims3d d{};
+    d.det_u = n;
+    d.angles = (uint32_t)nrows;
+    d.det_v = 1;
+    FDKWeights P{};
+    P.apply = 0;
+    std::vector<float> rel;
+    return run_filter(d, P, rel, filter, data, pitch, data, (long long)pitch, (long long)pitch * nrows, B2T_F32, s);
+}
+
+// getFanParameters (src/GeometryUtil2D.cpp:134-178): circular fan parameters
+// of one view; false if the view is not a circular fan.
+static bool fan_parameters(const b2t_view2d &p, uint32_t ndet, float &angle, float &src_origin, float &origin_det,
+                           float &det_size)
+{
+    double dp = p.src[0] * p.det_u[0] + p.src[1] * p.det_u[1];
+    double rel = std::sqrt(((double)p.src[0] * p.src[0] + (double)p.src[1] * p.src[1]) *
+                           ((double)p.det_u[0] * p.det_u[0] + (double)p.det_u[1] * p.det_u[1]));
+    if (std::abs(dp) > rel * 0.0001) return false;
+    src_origin = (float)std::sqrt((double)p.src[0] * p.src[0] + (double)p.src[1] * p.src[1]);
+    det_size = (float)std::sqrt((double)p.det_u[0] * p.det_u[0] + (double)p.det_u[1] * p.det_u[1]);
+    double t = (-(double)p.det_s[0]) * p.det_u[0] + (-(double)p.det_s[1]) * p.det_u[1];
+    t /= ((double)p.det_u[0] * p.det_u[0] + (double)p.det_u[1] * p.det_u[1]);
+    origin_det = (float)std::sqrt((p.det_s[0] + t * p.det_u[0]) * (p.det_s[0] + t * p.det_u[0]) +
+                                  (p.det_s[1] + t * p.det_u[1]) * (p.det_s[1] + t * p.det_u[1]));
+    angle = (float)std::atan2((double)p.det_u[1], (double)p.det_u[0]);
+    (void)ndet;
+    return true;
+}
+
+// FBP_CUDA (cuda/2d/fbp.cu:77-190): parallel = Ram-Lak filter + BP scaled by
+// (pi/2)/n_angles; fan = FDK pre-weighting of a one-row cone (+ Parker) +
+// filter + fan BP with the FBP weighting.  sino is not modified.
+b2t_status fbp2d_impl(const b2t_geom2d *g, int32_t filter, int32_t short_scan, const float *sino, size_t sino_pitch,
+                      float *vol, size_t vol_pitch, int32_t mode, cudaStream_t s)
+{
+    B2T_TRY(validate2d(g, "b2t_fbp2d"));
+    if (!sino || !vol) return fail(B2T_ERR_INVALID_ARG, "b2t_fbp2d: null data pointer");
+    if (filter != B2T_FILTER_NONE && filter != B2T_FILTER_RAMLAK)
+        return fail(B2T_ERR_UNSUPPORTED, "b2t_fbp2d: only the none and ram-lak filters are implemented");
+    const b2t_dims2d &dm = g->dims;
+    if (sino_pitch == 0) sino_pitch = dm.dets;
+    if (sino_pitch < dm.dets) return fail(B2T_ERR_INVALID_ARG, "b2t_fbp2d: pitch below row length");
+    b2t_dims3d d{};
+    d.det_u = dm.dets;
+    d.angles = dm.angles;
+    d.det_v = 1;
+    FDKWeights P{};
+    P.apply = 0;
+    std::vector<float> rel;
+    b2t_geom2d q = *g;
+    if (g->kind == B2T_GEOM_FAN2D) {
+        std::vector<float> angles(dm.angles);
+        float fs = 0, fd = 0, du = 0;
+        for (uint32_t i = 0; i < dm.angles; ++i)
+            if (!fan_parameters(g->views[i], dm.dets, angles[i], fs, fd, du))
+                return fail(B2T_ERR_UNSUPPORTED, "b2t_fbp2d: view %u is not a circular fan beam", i);
+        fdk_weights(fs, fd, 0.0f, du, 1.0f, dm.angles, dm.dets, angles.data(), short_scan, P, rel);
+    } else {
+        q.output_scale = (float)(q.output_scale * ((M_PI / 2.0f) / (float)dm.angles));
+    }
+    Scratch tmp;
+    B2T_TRY(tmp.alloc(sizeof(float) * (size_t)dm.angles * dm.dets, s, "b2t_fbp2d scratch"));
+    B2T_TRY(run_filter(d, P, rel, filter, sino, sino_pitch, tmp.as<void>(), (long long)dm.dets,
+                       (long long)dm.dets * dm.angles, B2T_F32, s));
+    return bp2d_impl(&q, 1, g->kind == B2T_GEOM_FAN2D ? 1 : 0, tmp.as<float>(), dm.dets, vol, vol_pitch, mode, s);
+}
+
 static b2t_status run_weight_filter(const b2t_geom3d *g, int filter, int short_scan, const void *src,
                                     size_t src_pitch, void *dst, long long dst_row, long long dst_v, int32_t dtype,
                                     cudaStream_t s)
@@ -248,20 +359,7 @@ static b2t_status run_weight_filter(const b2t_geom3d *g, int filter, int short_s
     FDKWeights P;
     std::vector<float> rel;
     B2T_TRY(fdk_setup(g, short_scan, P, rel));
-    Scratch rs;
-    const float *rel_dev = nullptr;
-    if (!rel.empty()) {
-        B2T_TRY(rs.alloc(sizeof(float) * rel.size(), s, "FDK Parker angles"));
-        B2T_CUDA_TRY(cudaMemcpyAsync(rs.as<void>(), rel.data(), sizeof(float) * rel.size(), cudaMemcpyHostToDevice, s),
-                     "FDK Parker angles upload");
-        rel_dev = rs.as<float>();
-    }
-    const int do_filter = (filter == B2T_FILTER_RAMLAK) ? 1 : 0;
-    if (dtype == B2T_F32)
-        return launch_filter<float>(src, src_pitch, g->dims, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
-    if (dtype == B2T_F16)
-        return launch_filter<__half>(src, src_pitch, g->dims, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
-    return launch_filter<__nv_bfloat16>(src, src_pitch, g->dims, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
+    return run_filter(g->dims, P, rel, filter, src, src_pitch, dst, dst_row, dst_v, dtype, s);
 }
 
 static b2t_status validate_fdk(const b2t_geom3d *g, int filter, int32_t dtype, const char *who)

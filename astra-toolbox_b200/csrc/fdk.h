@@ -11,6 +11,7 @@ namespace b2t {
 
 // Per-call FDK weighting parameters (circular orbit recovered from view 0).
 struct FDKWeights {
+    int apply;           // 0: filter only (no pre-weighting)
     float central_ray;   // source-origin + origin-detector distance
     float det_usize, det_vsize, zshift;
     float W;             // (D^2 / (du * Rs)) * (pi / 2) / n_angles
@@ -19,7 +20,13 @@ struct FDKWeights {
     float central_fan;   // half fan angle of the central row
 };
 
+void fdk_weights(float fSrcOrigin, float fDetOrigin, float fZShift, float fDetUSize, float fDetVSize,
+                 uint32_t n_angles, uint32_t det_u, const float *angles, int short_scan, FDKWeights &P,
+                 std::vector<float> &rel);
 b2t_status fdk_setup(const b2t_geom3d *g, int short_scan, FDKWeights &P, std::vector<float> &rel);
+b2t_status filter_rows_impl(float *data, size_t nrows, uint32_t n, size_t pitch, int32_t filter, cudaStream_t s);
+b2t_status fbp2d_impl(const b2t_geom2d *g, int32_t filter, int32_t short_scan, const float *sino, size_t sino_pitch,
+                      float *vol, size_t vol_pitch, int32_t mode, cudaStream_t s);
 b2t_status fdk_weight_filter_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, void *proj,
                                   size_t proj_pitch, int32_t dtype, cudaStream_t s);
 b2t_status fdk_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, float output_scale, const void *proj,

@@ -1,0 +1,134 @@
+"""Data objects and the id registry behind data2d / data3d / projector /
+algorithm (the reference's CData3DManager / CAstraIndexManager,
+python/astra/data3d_c.pyx, data2d_c.pyx).
+
+A data object holds a float32 torch tensor on the GPU (the reference keeps
+float32 host memory and copies it to the GPU per call; here the data stay
+resident).  Linked numpy arrays are mirrored on the device and written back
+after every operation that changes them; linked torch CUDA tensors are used in
+place (zero copy).
+"""
+import itertools
+
+import numpy as np
+import torch
+
+from ._lib import AstraError
+from . import geometry as G
+
+_ids = itertools.count(1)
+_objects = {}
+
+
+def new_id():
+    return next(_ids)
+
+
+def register(obj):
+    i = new_id()
+    _objects[i] = obj
+    return i
+
+
+def lookup(i, cls=None):
+    obj = _objects.get(int(i))
+    if obj is None or (cls is not None and not isinstance(obj, cls)):
+        raise AstraError(1, "Unknown object id %r" % (i,))
+    return obj
+
+
+def remove(i):
+    _objects.pop(int(i), None)
+
+
+def ids_of(cls):
+    return [i for i, o in _objects.items() if isinstance(o, cls)]
+
+
+def _device():
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+class DataObject:
+    """'-vol' or '-sino' / '-proj3d' data with its geometry."""
+
+    def __init__(self, kind, geometry, dims3):
+        self.kind = kind  # 'vol' or 'sino'
+        self.geometry = geometry
+        self.is3d = dims3
+        if kind == 'vol':
+            self.shape = tuple(G.vol_shape(geometry))
+        else:
+            self.shape = tuple(G.proj_shape(geometry))
+        self.tensor = None
+        self.host = None       # linked numpy array (written back after changes)
+
+    def fill(self, data):
+        dev = _device()
+        if data is None:
+            self.tensor = torch.zeros(self.shape, dtype=torch.float32, device=dev)
+        elif np.isscalar(data):
+            self.tensor = torch.full(self.shape, float(data), dtype=torch.float32, device=dev)
+        else:
+            arr = data.detach().cpu().numpy() if isinstance(data, torch.Tensor) else np.asarray(data)
+            if tuple(arr.shape) != self.shape:
+                raise AstraError(1, "The dimensions of the data %s do not match those specified in the geometry %s"
+                                 % (tuple(arr.shape), self.shape))
+            self.tensor = torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32)).to(dev)
+
+    def link(self, data):
+        if isinstance(data, torch.Tensor):
+            if tuple(data.shape) != self.shape:
+                raise AstraError(1, "The dimensions of the data do not match those specified in the geometry")
+            if data.dtype != torch.float32:
+                raise AstraError(1, "Linked data must be float32")
+            if not data.is_contiguous():
+                raise AstraError(1, "Linked data must be contiguous")
+            if data.is_cuda:
+                self.tensor = data
+                return
+            self.host = data.numpy()
+        else:
+            if not isinstance(data, np.ndarray) or data.dtype != np.float32:
+                raise AstraError(1, "Linked data must be a float32 numpy array or torch tensor")
+            if not data.flags['C_CONTIGUOUS']:
+                raise AstraError(1, "Linked data must be C-contiguous")
+            if not data.flags['WRITEABLE']:
+                raise AstraError(1, "Linked data must be writeable")
+            if tuple(data.shape) != self.shape:
+                raise AstraError(1, "The dimensions of the data do not match those specified in the geometry")
+            self.host = data
+        self.tensor = torch.from_numpy(self.host).to(_device())
+
+    def changed(self):
+        """Write device data back to a linked host array."""
+        if self.host is not None:
+            self.host[...] = self.tensor.cpu().numpy()
+
+    def get(self):
+        return self.tensor.cpu().numpy()
+
+    def store(self, data):
+        if np.isscalar(data):
+            self.tensor.fill_(float(data))
+        else:
+            arr = data.detach().cpu().numpy() if isinstance(data, torch.Tensor) else np.asarray(data)
+            if tuple(arr.shape) != self.shape:
+                raise AstraError(1, "The dimensions of the data do not match those specified in the geometry")
+            self.tensor.copy_(torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32)))
+        self.changed()
+
+
+def create(datatype, geometry, data=None, link=False, dims3=True):
+    if datatype == '-vol':
+        kind = 'vol'
+    elif datatype in ('-sino', '-proj3d', '-sinocone'):
+        kind = 'sino'
+    else:
+        raise ValueError("Invalid datatype. Please specify '-vol' or '-proj3d'")
+    obj = DataObject(kind, geometry, dims3)
+    if link:
+        obj.link(data)
+    else:
+        obj.fill(data)
+    return register(obj)

@@ -50,6 +50,7 @@ class Projector3D:
 
     def __init__(self, proj_geom, vol_geom, options=None):
         options = dict(options or {})
+        self.options = options
         self.proj_geom = proj_geom
         self.vol_geom = vol_geom
         self.geom = Geometry3D(vol_geom, proj_geom)
@@ -103,6 +104,7 @@ class Projector2D:
 
     def __init__(self, proj_geom, vol_geom, options=None):
         options = dict(options or {})
+        self.options = options
         self.proj_geom = proj_geom
         self.vol_geom = vol_geom
         self.geom = Geometry2D(vol_geom, proj_geom)
@@ -201,6 +203,62 @@ def fdk(projector, proj, vol, short_scan=False, filter_type='ram-lak', output_sc
                   float(output_scale), proj.data_ptr(), 0, vol.data_ptr(), 0, _DTYPES[vol.dtype], mode,
                   stream_handle(vol.device))
     return vol
+
+
+def fbp2d(projector, sino, vol, short_scan=False, filter_type='ram-lak', mode=_lib.MODE_SET):
+    """2D FBP of sino into vol (torch CUDA float32); sino is not modified."""
+    _check_tensor(vol, projector.vol_shape, "volume")
+    _check_tensor(sino, projector.proj_shape, "sinogram", vol.device)
+    with torch.cuda.device(vol.device):
+        _lib.call("b2t_fbp2d", ctypes.byref(projector.geom.c), filter_code(filter_type), int(bool(short_scan)),
+                  sino.data_ptr(), 0, vol.data_ptr(), 0, mode, stream_handle(vol.device))
+    return vol
+
+
+# ---------------------------------------------------------------------------
+# astra.projector: registry of 2D 'cuda' projectors (python/astra/projector.py)
+# ---------------------------------------------------------------------------
+
+def create(cfg):
+    """Create a projector from a configuration dict; 'cuda' (2D) or 'cuda3d'."""
+    from . import data as _d
+    t = cfg.get('type')
+    opts = dict(cfg.get('options', cfg.get('option', {})) or {})
+    if t == 'cuda':
+        return _d.register(Projector2D(cfg['ProjectionGeometry'], cfg['VolumeGeometry'], opts))
+    if t == 'cuda3d':
+        return _d.register(Projector3D(cfg['ProjectionGeometry'], cfg['VolumeGeometry'], opts))
+    raise AstraError(2, "Projector type %r is not available (cuda and cuda3d are)" % (t,))
+
+
+def delete(ids):
+    from . import data as _d
+    for i in (ids if isinstance(ids, (list, tuple)) else [ids]):
+        _d.remove(i)
+
+
+def clear():
+    from . import data as _d
+    for i in _d.ids_of(Projector2D) + _d.ids_of(Projector3D):
+        _d.remove(i)
+
+
+def lookup_projector(i):
+    from . import data as _d
+    pr = _d.lookup(i)
+    if not isinstance(pr, (Projector2D, Projector3D)):
+        raise AstraError(1, "Not a projector id: %r" % (i,))
+    return pr
+
+
+def projection_geometry(i):
+    from . import data as _d
+    return _d.lookup(i).proj_geom
+
+
+def volume_geometry(i):
+    from . import data as _d
+    return _d.lookup(i).vol_geom
 
 
 def fdk_weight_filter(projector, proj, short_scan=False, filter_type='ram-lak'):

@@ -274,6 +274,18 @@ b2t_status b2t_fdk(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, f
 b2t_status b2t_fdk_weight_filter(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, void *proj,
                                  size_t proj_pitch, int32_t dtype, void *stream);
 
+/* Ram-Lak filtering of nrows rows of n f32 samples in place (row pitch in
+ * elements): the zero-padded FFT convolution of runCudaFFT / applyFilter /
+ * runCudaIFFT (cuda/2d/fft.cu:52-336) evaluated as its exact Toeplitz form. */
+b2t_status b2t_filter_rows(float *data, size_t nrows, uint32_t n, size_t pitch, int32_t filter, void *stream);
+
+/* 2D filtered backprojection, vol (+)= FBP(sino); sino is not modified.
+ * Replaces astraCUDA::FBP (cuda/2d/fbp.cu:77-190): parallel = filter + BP
+ * scaled by (pi/2)/n_angles; fan = FDK pre-weighting of a one-row cone (+
+ * Parker if short_scan) + filter + FBP-weighted fan BP. */
+b2t_status b2t_fbp2d(const b2t_geom2d *geom, int32_t filter, int32_t short_scan, const float *sino,
+                     size_t sino_pitch, float *vol, size_t vol_pitch, int32_t mode, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* element-wise operations and reductions                                  */
 /* ---------------------------------------------------------------------- */
@@ -290,6 +302,52 @@ b2t_status b2t_vec_op(int32_t op, float *out, const float *a, const float *b, fl
  * allocates and frees in stream order. */
 b2t_status b2t_dot_f64(const void *a, const void *b, size_t n, int32_t dtype, double *result,
                        void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* SIRT / CGLS reconstruction                                              */
+/* ---------------------------------------------------------------------- */
+
+enum { B2T_ALGO_SIRT = 1, B2T_ALGO_CGLS = 2 };
+
+/* Options of SIRT3D_CUDA / CGLS3D_CUDA / SIRT_CUDA / CGLS_CUDA
+ * (src/ReconstructionAlgorithm3D.cpp:95-120, CudaSirtAlgorithm3D.cpp:141).
+ * Mask and bound arrays are device pointers (NULL = unused) that must stay
+ * valid while the algorithm is used. */
+typedef struct b2t_algo_options {
+    float relaxation;          /* SIRT "Relaxation" (default 1)                 */
+    int32_t use_min;           /* MinConstraint                                 */
+    float min_value;
+    int32_t use_max;           /* MaxConstraint                                 */
+    float max_value;
+    const float *vol_mask;     /* ReconstructionMaskId                          */
+    const float *sino_mask;    /* SinogramMaskId (SIRT)                         */
+    const float *min_mask;     /* per-pixel lower bound (2D SIRT MinMaskId)     */
+    const float *max_mask;     /* per-pixel upper bound (2D SIRT MaxMaskId)     */
+} b2t_algo_options;
+
+typedef struct b2t_algo b2t_algo;  /* opaque: operator, weights, work buffers */
+
+/* SIRT3D_CUDA / CGLS3D_CUDA (src/CudaSirtAlgorithm3D.cpp,
+ * src/CudaCglsAlgorithm3D.cpp).  Allocates the work buffers (cudaMalloc). */
+b2t_status b2t_algo_create3d(int32_t type, const b2t_geom3d *geom, const b2t_params3d *params,
+                             const b2t_algo_options *options, b2t_algo **out);
+/* SIRT_CUDA / CGLS_CUDA (src/CudaSirtAlgorithm.cpp, src/CudaCglsAlgorithm.cpp). */
+b2t_status b2t_algo_create2d(int32_t type, const b2t_geom2d *geom, uint32_t det_supersample,
+                             uint32_t pixel_supersample, const b2t_algo_options *options, b2t_algo **out);
+/* run(iterations) (CudaSirtAlgorithm3D.cpp:301-381, CudaCglsAlgorithm3D.cpp:264-355):
+ * iterates on device f32 data; vol is updated in place, sino is read.  CGLS
+ * restarts at every call, as the reference does.  use_graph != 0 replays a
+ * CUDA graph of the iteration (captured on first use). */
+b2t_status b2t_algo_run(b2t_algo *algo, const float *sino, float *vol, int32_t iterations, int32_t use_graph,
+                        void *stream);
+/* getResidualNorm (CudaSirtAlgorithm3D.cpp:383-418): ||sino - A vol||_2,
+ * accumulated in FP64; synchronises the stream. */
+b2t_status b2t_algo_residual_norm(b2t_algo *algo, const float *sino, const float *vol, double *norm,
+                                  void *stream);
+/* Ask a running b2t_algo_run (on another thread) to stop between iterations
+ * (astra::shouldAbort, src/Globals.cpp:49-58). */
+void b2t_algo_abort(b2t_algo *algo);
+void b2t_algo_destroy(b2t_algo *algo);
 
 #ifdef __cplusplus
 }
