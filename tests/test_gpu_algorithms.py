@@ -165,7 +165,7 @@ def test_fbp2d_parallel_vs_oracle(astra, orc):
 def test_direct_fp3d_matches_create_sino3d_gpu(astra):
     # tests/python/integration/test_dlpack3d.py:123-133 pattern
     vg, pg = _cone_setup(astra)
-    vol = np.random.default_rng(5).random((20, 28, 24)).astype(np.float32)
+    vol = np.random.default_rng(5).random((20, 24, 28)).astype(np.float32)
     sid, sino = astra.create_sino3d_gpu(vol, pg, vg)
     pid = astra.create_projector('cuda3d', pg, vg)
     tv = torch.from_numpy(vol).cuda()
@@ -188,7 +188,7 @@ def test_direct_fp3d_matches_create_sino3d_gpu(astra):
 
 def test_linked_arrays_are_updated(astra):
     vg, pg = _cone_setup(astra)
-    vol = np.random.default_rng(6).random((20, 28, 24)).astype(np.float32)
+    vol = np.random.default_rng(6).random((20, 24, 28)).astype(np.float32)
     sino = np.zeros((26, 30, 34), dtype=np.float32)
     vid = astra.data3d.link('-vol', vg, vol)
     sid = astra.data3d.link('-sino', pg, sino)
