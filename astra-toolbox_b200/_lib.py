@@ -126,6 +126,7 @@ SIGNATURES = {
     "b2t_algo_destroy": (None, [_P]),
     "b2t_vec_op": (_I32, [_I32, _P, _P, _P, _F, _SZ, _P]),
     "b2t_dot_f64": (_I32, [_P, _P, _SZ, _I32, _P, _P]),
+    "b2t_dot_f64_noalloc": (_I32, [_P, _P, _SZ, _I32, _P, _P]),
 }
 
 _lib = None

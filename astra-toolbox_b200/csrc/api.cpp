@@ -169,4 +169,10 @@ b2t_status b2t_dot_f64(const void *a, const void *b, size_t n, int32_t dtype, do
     return dot_impl(a, b, n, dtype, result, static_cast<cudaStream_t>(stream));
 }
 
+b2t_status b2t_dot_f64_noalloc(const void *a, const void *b, size_t n, int32_t dtype, double *result, void *stream)
+{
+    clear_error();
+    return dot_noalloc_impl(a, b, n, dtype, result, static_cast<cudaStream_t>(stream));
+}
+
 }  // extern "C"

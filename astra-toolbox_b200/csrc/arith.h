@@ -16,5 +16,6 @@ b2t_status dot_launch(const void *a, const void *b, size_t n, int32_t dtype, dou
 b2t_status vec_op_impl(int32_t op, float *out, const float *a, const float *b, float sc, size_t n,
                        cudaStream_t s);
 b2t_status dot_impl(const void *a, const void *b, size_t n, int32_t dtype, double *result, cudaStream_t s);
+b2t_status dot_noalloc_impl(const void *a, const void *b, size_t n, int32_t dtype, double *result, cudaStream_t s);
 
 }  // namespace b2t

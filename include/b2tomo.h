@@ -303,6 +303,19 @@ b2t_status b2t_vec_op(int32_t op, float *out, const float *a, const float *b, fl
 b2t_status b2t_dot_f64(const void *a, const void *b, size_t n, int32_t dtype, double *result,
                        void *stream);
 
+/* The same FP64 inner product, allocating nothing.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory when they call
+ * it (a real-time loop that must not wait on the allocator, a host that
+ * hands out all device memory from its own fixed pool): the partial sums live
+ * in a fixed 32 KB array built into the library, present on every GPU that
+ * loads it until the process exits.  Limit: n <= 4096 * 2^20 elements; larger
+ * n returns B2T_ERR_INVALID_ARG before any device work.  All calls on one
+ * device share the array, so calls that overlap on the GPU race: serialise
+ * them.  The first call on each device looks up the array's device address
+ * with that device current. */
+b2t_status b2t_dot_f64_noalloc(const void *a, const void *b, size_t n, int32_t dtype, double *result,
+                               void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* SIRT / CGLS reconstruction                                              */
 /* ---------------------------------------------------------------------- */
