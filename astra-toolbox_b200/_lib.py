@@ -80,6 +80,10 @@ class VolGeom2D(ctypes.Structure):
                 ("max_x", ctypes.c_float), ("min_y", ctypes.c_float), ("max_y", ctypes.c_float)]
 
 
+class Problem2D(ctypes.Structure):
+    _fields_ = [("geom", Geom2D), ("det_supersample", ctypes.c_uint32), ("pixel_supersample", ctypes.c_uint32)]
+
+
 ALGO_SIRT, ALGO_CGLS = 1, 2
 
 
@@ -127,6 +131,13 @@ SIGNATURES = {
     "b2t_vec_op": (_I32, [_I32, _P, _P, _P, _F, _SZ, _P]),
     "b2t_dot_f64": (_I32, [_P, _P, _SZ, _I32, _P, _P]),
     "b2t_dot_f64_noalloc": (_I32, [_P, _P, _SZ, _I32, _P, _P]),
+    "b2t_onchip_peak": (_I32, [_I32, _P]),
+    "b2t_batch2d_create": (_I32, [_P, _I32, _P]),
+    "b2t_batch2d_layout": (_I32, [_P, _P, _P, _P, _P]),
+    "b2t_batch2d_fp": (_I32, [_P, _P, _P, _I32, _P]),
+    "b2t_batch2d_bp": (_I32, [_P, _P, _P, _I32, _P]),
+    "b2t_algo_create_batch2d": (_I32, [_I32, _P, _P, _P]),
+    "b2t_batch2d_destroy": (None, [_P]),
 }
 
 _lib = None

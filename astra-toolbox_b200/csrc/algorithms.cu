@@ -21,6 +21,7 @@
 #include <memory>
 
 #include "algorithms.h"
+#include "batch2d.h"
 #include "arith.h"
 #include "b2t_internal.h"
 #include "proj2d.h"
@@ -156,6 +157,25 @@ struct Op2D : Operator {
         b2t_geom2d q = g;
         q.output_scale *= scale;
         return bp2d_impl(&q, pix_ss, 0, proj, 0, vol, 0, mode, s);
+    }
+};
+
+// All problems of a batch (batch2d.cu) as one block-diagonal operator on the
+// packed buffers: SIRT's element-wise steps then run once for the batch.
+struct OpBatch2D : Operator {
+    Batch2D *b;
+    explicit OpBatch2D(Batch2D *batch) : b(batch)
+    {
+        nvol = batch->vol_total;
+        nproj = batch->sino_total;
+    }
+    b2t_status fp(const float *vol, float *proj, float scale, int mode, cudaStream_t s) override
+    {
+        return batch2d_fp_impl(b, vol, proj, scale, mode, s);
+    }
+    b2t_status bp(const float *proj, float *vol, float scale, int mode, cudaStream_t s) override
+    {
+        return batch2d_bp_impl(b, proj, vol, scale, mode, s);
     }
 };
 
@@ -350,6 +370,17 @@ b2t_status algo_create2d_impl(int32_t type, const b2t_geom2d *geom, uint32_t det
 {
     B2T_TRY(validate2d(geom, "b2t_algo_create2d"));
     return algo_create(type, new Op2D(geom, det_ss ? det_ss : 1, pix_ss ? pix_ss : 1), opt, out);
+}
+
+b2t_status algo_create_batch2d_impl(int32_t type, Batch2D *batch, const b2t_algo_options *opt, b2t_algo **out)
+{
+    if (!batch) return fail(B2T_ERR_INVALID_ARG, "b2t_algo_create_batch2d: null batch");
+    if (type != B2T_ALGO_SIRT)
+        return fail(B2T_ERR_UNSUPPORTED, "b2t_algo_create_batch2d: only SIRT runs on a batch (CGLS needs per-problem "
+                                         "step sizes)");
+    if (opt && (opt->vol_mask || opt->sino_mask || opt->min_mask || opt->max_mask))
+        return fail(B2T_ERR_UNSUPPORTED, "b2t_algo_create_batch2d: masks are not supported on a batch");
+    return algo_create(type, new OpBatch2D(batch), opt, out);
 }
 
 b2t_status algo_run_impl(b2t_algo *h, const float *sino, float *vol, int32_t iters, int32_t use_graph, cudaStream_t s)

@@ -14,6 +14,8 @@ b2t_status algo_create3d_impl(int32_t type, const b2t_geom3d *geom, const b2t_pa
                               const b2t_algo_options *opt, b2t_algo **out);
 b2t_status algo_create2d_impl(int32_t type, const b2t_geom2d *geom, uint32_t det_ss, uint32_t pix_ss,
                               const b2t_algo_options *opt, b2t_algo **out);
+struct Batch2D;
+b2t_status algo_create_batch2d_impl(int32_t type, Batch2D *batch, const b2t_algo_options *opt, b2t_algo **out);
 b2t_status algo_run_impl(b2t_algo *a, const float *sino, float *vol, int32_t iters, int32_t use_graph, cudaStream_t s);
 b2t_status algo_residual_impl(b2t_algo *a, const float *sino, const float *vol, double *norm, cudaStream_t s);
 void algo_abort_impl(b2t_algo *a);

@@ -8,6 +8,7 @@
 
 #include "algorithms.h"
 #include "arith.h"
+#include "batch2d.h"
 #include "b2t_internal.h"
 #include "fdk.h"
 #include "proj2d.h"
@@ -173,6 +174,59 @@ b2t_status b2t_dot_f64_noalloc(const void *a, const void *b, size_t n, int32_t d
 {
     clear_error();
     return dot_noalloc_impl(a, b, n, dtype, result, static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_batch2d_create(const b2t_problem2d *problems, int32_t n, b2t_batch2d **out)
+{
+    clear_error();
+    return batch2d_create_impl(problems, n, reinterpret_cast<Batch2D **>(out));
+}
+
+b2t_status b2t_batch2d_layout(const b2t_batch2d *batch, uint64_t *vol_offsets, uint64_t *sino_offsets,
+                              uint64_t *vol_total, uint64_t *sino_total)
+{
+    clear_error();
+    const Batch2D *b = reinterpret_cast<const Batch2D *>(batch);
+    if (!b) return fail(B2T_ERR_INVALID_ARG, "b2t_batch2d_layout: null batch");
+    for (size_t i = 0; i < b->probs.size(); ++i) {
+        if (vol_offsets) vol_offsets[i] = (uint64_t)b->probs[i].vol_off;
+        if (sino_offsets) sino_offsets[i] = (uint64_t)b->probs[i].sino_off;
+    }
+    if (vol_total) *vol_total = b->vol_total;
+    if (sino_total) *sino_total = b->sino_total;
+    return B2T_OK;
+}
+
+b2t_status b2t_batch2d_fp(b2t_batch2d *batch, const float *vols, float *sinos, int32_t mode, void *stream)
+{
+    clear_error();
+    return batch2d_fp_impl(reinterpret_cast<Batch2D *>(batch), vols, sinos, 1.0f, mode,
+                           static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_batch2d_bp(b2t_batch2d *batch, const float *sinos, float *vols, int32_t mode, void *stream)
+{
+    clear_error();
+    return batch2d_bp_impl(reinterpret_cast<Batch2D *>(batch), sinos, vols, 1.0f, mode,
+                           static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_algo_create_batch2d(int32_t type, b2t_batch2d *batch, const b2t_algo_options *options,
+                                   b2t_algo **out)
+{
+    clear_error();
+    return algo_create_batch2d_impl(type, reinterpret_cast<Batch2D *>(batch), options, out);
+}
+
+void b2t_batch2d_destroy(b2t_batch2d *batch)
+{
+    delete reinterpret_cast<Batch2D *>(batch);
+}
+
+b2t_status b2t_onchip_peak(int32_t which, double *gbs)
+{
+    clear_error();
+    return onchip_peak_impl(which, gbs);
 }
 
 }  // extern "C"

@@ -20,6 +20,9 @@ void count_launches(int n);
 // Map a CUDA error to B2T_ERR_CUDA (or B2T_ERR_NO_MEMORY) with context.
 b2t_status cuda_fail(cudaError_t e, const char *where);
 
+// Measured on-chip load bandwidth (onchip_peak.cu).
+b2t_status onchip_peak_impl(int32_t which, double *gbs);
+
 #define B2T_CUDA_TRY(expr, where)                                  \
     do {                                                           \
         cudaError_t _e = (expr);                                   \
@@ -57,6 +60,7 @@ public:
         cudaError_t e = cudaMallocAsync(&ptr_, bytes, s);
         if (e != cudaSuccess) {
             ptr_ = nullptr;
+            (void)cudaGetLastError();  // allocation failures are not sticky: clear them
             return cuda_fail(e, what);
         }
         bytes_ = bytes;

@@ -31,6 +31,7 @@
 
 #include "b2t_internal.h"
 #include "proj3d.h"
+#include "ramp_tc.h"
 #include "tma.h"
 
 namespace b2t {
@@ -93,13 +94,17 @@ __global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant_
     extern __shared__ __align__(128) unsigned char smraw[];
     T *tiles = reinterpret_cast<T *>(smraw);
     uint64_t *full = reinterpret_cast<uint64_t *>(smraw + (size_t)BPT_STAGES * BPT_BV * BPT_BU * sizeof(T));
-    StageInfo *info = reinterpret_cast<StageInfo *>(full + BPT_STAGES);
+    uint64_t *empty = full + BPT_STAGES;
+    StageInfo *info = reinterpret_cast<StageInfo *>(empty + BPT_STAGES);
 
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int tid = ty * 32 + tx;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
     const int warp = tid >> 5;
-    const int x = blockIdx.x * 32 + tx;
-    const int y = blockIdx.y * 8 + ty;
+    const int lane = tid & 31;
+    // a warp covers 8 x 4 voxels, so its detector footprint in a tile row
+    // stays under 32 texels (no shared-memory bank conflicts between lanes
+    // of one row); the 8 warps tile the 32 x 8 block
+    const int x = blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7);
+    const int y = blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3);
     const int z0 = blockIdx.z * BPT_Z;
     const bool active = (x < L.nx) && (y < L.ny);
     const float cx = 0.5f - 0.5f * (float)L.nx, cy = 0.5f - 0.5f * (float)L.ny, cz = 0.5f - 0.5f * (float)L.nz;
@@ -110,7 +115,10 @@ __global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant_
     const float bz0 = fz0, bz1 = (float)(min(L.nz, z0 + BPT_Z) - 1) + cz;
 
     if (tid == 0) {
-        for (int s = 0; s < BPT_STAGES; ++s) mbar_init(&full[s], 1);
+        for (int s = 0; s < BPT_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 8);  // one arrival per warp when it is done with the stage
+        }
         mbar_fence_init();
         tma_prefetch_map(&L.tmap);
     }
@@ -120,7 +128,6 @@ __global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant_
     auto produce = [&](int i) {
         const int stage = i % BPT_STAGES;
         const BPView &W = L.views[i];
-        const int lane = tid & 31;
         float U = 0.0f, V = 0.0f;
         if (lane < 8) {
             project<KIND>(W, (lane & 1) ? bx1 : bx0, (lane & 2) ? by1 : by0, (lane & 4) ? bz1 : bz0, U, V);
@@ -172,9 +179,11 @@ __global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant_
     for (int i = 0; i < L.nviews; ++i) {
         const int stage = i % BPT_STAGES;
         const uint32_t parity = (uint32_t)((i / BPT_STAGES) & 1);
-        const bool ok = mbar_wait_bounded(&full[stage], parity, 2000000000LL);
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicOr(&g_b2t_device_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
+        // every wait is bounded: a thread that gives up records the error
+        // and leaves; the others then give up on the barriers it no longer
+        // arrives on, so the kernel always ends
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[stage], parity, 2000000000LL))) {
+            if (lane == 0) atomicOr(&g_b2t_device_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
             return;
         }
         const StageInfo si = info[stage];
@@ -287,8 +296,18 @@ __global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant_
                 }
             }
         }
-        __syncthreads();  // every thread is done with this stage
-        if (warp == 0 && i + BPT_STAGES < L.nviews) produce(i + BPT_STAGES);
+        // release the stage: one arrival per warp once all its lanes are done
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stage]);
+        // warp 0 refills it for view i + STAGES once every warp has released
+        // it; the other warps run ahead on the stages already loaded
+        if (warp == 0 && i + BPT_STAGES < L.nviews) {
+            if (!__all_sync(0xffffffffu, mbar_wait_bounded(&empty[stage], parity, 2000000000LL))) {
+                if (lane == 0) atomicOr(&g_b2t_device_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
+                return;
+            }
+            produce(i + BPT_STAGES);
+        }
     }
 
     if (active) {
@@ -309,7 +328,7 @@ __global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant_
 template <typename T, int KIND, int KER, bool CIRC>
 b2t_status launch_one(const BPTmaLaunch &L, const b2t_dims3d &d, cudaStream_t s)
 {
-    const size_t smem = (size_t)BPT_STAGES * BPT_BV * BPT_BU * sizeof(T) + BPT_STAGES * (sizeof(uint64_t) + 16) + 64;
+    const size_t smem = (size_t)BPT_STAGES * BPT_BV * BPT_BU * sizeof(T) + BPT_STAGES * (2 * sizeof(uint64_t) + 16) + 64;
     auto kern = bp3d_tma_kernel<T, KIND, KER, CIRC>;
     B2T_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                  "bp3d_tma smem attribute");
@@ -383,7 +402,8 @@ b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *p
 }
 
 b2t_status encode_tensor_map(CUtensorMap *map, CUtensorMapDataType dtype, uint32_t rank, const void *base,
-                             const uint64_t *dims, const uint64_t *strides_bytes, const uint32_t *box)
+                             const uint64_t *dims, const uint64_t *strides_bytes, const uint32_t *box,
+                             CUtensorMapSwizzle swizzle)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
@@ -404,7 +424,7 @@ b2t_status encode_tensor_map(CUtensorMap *map, CUtensorMapDataType dtype, uint32
         if (k + 1 < rank) gstr[k] = strides_bytes[k];
     }
     CUresult r = encode(map, dtype, rank, const_cast<void *>(base), gdim, gstr, bdim, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(B2T_ERR_CUDA, "cuTensorMapEncodeTiled failed (CUresult %d)", (int)r);
     return B2T_OK;
@@ -416,7 +436,9 @@ b2t_status device_errors_impl(uint32_t *flags)
     B2T_CUDA_TRY(cudaMemcpyFromSymbol(&v, g_b2t_device_errors, sizeof(v)), "read device error word");
     const unsigned int zero = 0;
     B2T_CUDA_TRY(cudaMemcpyToSymbol(g_b2t_device_errors, &zero, sizeof(zero)), "clear device error word");
-    *flags = v;
+    uint32_t w = 0;
+    B2T_TRY(ramp_tc_errors(&w));
+    *flags = v | w;
     return B2T_OK;
 }
 

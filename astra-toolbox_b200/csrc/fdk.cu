@@ -20,6 +20,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -27,6 +28,7 @@
 #include "fdk.h"
 #include "proj2d.h"
 #include "proj3d.h"
+#include "ramp_tc.h"
 
 namespace b2t {
 
@@ -69,6 +71,102 @@ __device__ __forceinline__ float parker_weight(float beta, float fU, const FDKWe
     return w * P.parker_scale;
 }
 
+// FDK weight of detector column u in a row with vertical offset fV (view at
+// relative angle beta): devFDK_preweight times, for short scans, the Parker
+// weight.  1 when the weights are off (plain filtering).
+__device__ __forceinline__ float fdk_weight(const FDKWeights &P, int u, int nu, float fV, float beta)
+{
+    if (!P.apply) return 1.0f;
+    const float fU = ((float)u - 0.5f * (float)nu + 0.5f) * P.det_usize;
+    const float rl = sqrtf(P.central_ray * P.central_ray + fU * fU + fV * fV);
+    float w = P.W / rl;
+    if (P.short_scan) w *= parker_weight(beta, fU, P);
+    return w;
+}
+
+__device__ __forceinline__ void split3(float x, __nv_bfloat16 &t0, __nv_bfloat16 &t1, __nv_bfloat16 &t2)
+{
+    t0 = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(t0);
+    t1 = __float2bfloat16_rn(r1);
+    t2 = __float2bfloat16_rn(r1 - __bfloat162float(t1));
+}
+
+// Weighted rows for the tensor-core filter (ramp_tc.h).  One CTA stages
+// SPLIT_ROWS rows in shared memory (FDK weights applied, zero beyond the row)
+// and then
+//   - writes the exact near part of the filter to dst:
+//       near_n = x_n / 2 + sum_{odd d <= RAMP_TC_BAND} c(d) (x_{n-d} + x_{n+d})
+//     in FP32 (round to nearest); the tensor cores later add the far taps;
+//   - writes the three BF16 terms of x[m][2j] and x[m][2j+1] into the even and
+//     odd planes of the split operand (zero past the row and in the pitch).
+// Every row is read completely before any of it is written, so src may equal
+// dst (in-place filtering).
+constexpr int SPLIT_ROWS = 4;
+constexpr int SPLIT_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(SPLIT_THREADS) fdk_split_kernel(
+    const T *src, long long src_pitch, int nu, int na, int nv, FDKWeights P, const float *__restrict__ rel_angles,
+    __nv_bfloat16 *out, int khp, long long M, T *dst, long long dst_row, long long dst_v)
+{
+    extern __shared__ float xs[];  // SPLIT_ROWS rows of (nu + 2 * RAMP_TC_BAND + 2) floats
+    __shared__ float taps[(RAMP_TC_BAND + 1) / 2];
+    const int W = nu + 2 * RAMP_TC_BAND + 2;
+    const int PADL = RAMP_TC_BAND + 1;
+    const long long m0 = (long long)blockIdx.x * SPLIT_ROWS;
+    const int nr = (int)min((long long)SPLIT_ROWS, M - m0);
+    for (int t = threadIdx.x; t < (RAMP_TC_BAND + 1) / 2; t += SPLIT_THREADS) {
+        const double d = 2.0 * t + 1.0;
+        taps[t] = (float)(-2.0 / (M_PI * M_PI * d * d));
+    }
+    for (int r = 0; r < nr; ++r) {
+        const long long m = m0 + r;
+        const int v = (int)(m / na);
+        const int a = (int)(m - (long long)v * na);
+        const float fV = ((float)v - 0.5f * (float)nv + 0.5f) * P.det_vsize + P.zshift;
+        const float beta = P.short_scan ? rel_angles[a] : 0.0f;
+        const T *row = src + m * src_pitch;
+        float *x = xs + r * W;
+        for (int j = threadIdx.x; j < W; j += SPLIT_THREADS) {
+            const int u = j - PADL;
+            x[j] = (u >= 0 && u < nu) ? ldf(row + u) * fdk_weight(P, u, nu, fV, beta) : 0.0f;
+        }
+    }
+    __syncthreads();
+    const long long term = M * khp;
+    for (int r = 0; r < nr; ++r) {
+        const long long m = m0 + r;
+        const float *x = xs + r * W + PADL;  // x[-PADL .. nu + PADL)
+        const int v = (int)(m / na);
+        T *orow = dst + (long long)v * dst_v + (m - (long long)v * na) * dst_row;
+        for (int n = threadIdx.x; n < nu; n += SPLIT_THREADS) {
+            float acc = 0.5f * x[n];
+#pragma unroll 8
+            for (int t = 0; t < (RAMP_TC_BAND + 1) / 2; ++t) {
+                const int d = 2 * t + 1;
+                acc = fmaf(taps[t], x[n - d] + x[n + d], acc);
+            }
+            orow[n] = stf<T>(acc);
+        }
+        __nv_bfloat16 *e = out + m * khp;
+        for (int j = threadIdx.x; j < khp; j += SPLIT_THREADS) {
+            const int u0 = 2 * j, u1 = 2 * j + 1;
+            const float x0 = (u0 < nu) ? x[u0] : 0.0f;
+            const float x1 = (u1 < nu) ? x[u1] : 0.0f;
+            __nv_bfloat16 t0, t1, t2;
+            split3(x0, t0, t1, t2);
+            e[j] = t0;
+            e[j + term] = t1;
+            e[j + 2 * term] = t2;
+            split3(x1, t0, t1, t2);
+            e[j + 3 * term] = t0;
+            e[j + 4 * term] = t1;
+            e[j + 5 * term] = t2;
+        }
+    }
+}
+
 // One CTA filters `rows` consecutive rows m = v * na + a of proj (pitch in
 // elements).  Shared memory: rows x (3 nu + 32) floats (each row zero-padded
 // by nu + 16 on both sides, which covers every window read, including the
@@ -106,14 +204,7 @@ __global__ void __launch_bounds__(FILT_THREADS) fdk_weight_filter_kernel(
             const int u = j - PADW;
             float val = 0.0f;
             if (u >= 0 && u < nu) {
-                float w = 1.0f;
-                if (P.apply) {
-                    const float fU = ((float)u - 0.5f * (float)nu + 0.5f) * P.det_usize;
-                    const float rl = sqrtf(P.central_ray * P.central_ray + fU * fU + fV * fV);
-                    w = P.W / rl;
-                    if (P.short_scan) w *= parker_weight(beta, fU, P);
-                }
-                val = ldf(row + u) * w;
+                val = ldf(row + u) * fdk_weight(P, u, nu, fV, beta);
             }
             xs[j] = val;
         }
@@ -257,6 +348,22 @@ static b2t_status launch_filter(const void *src, size_t src_pitch, const b2t_dim
     return B2T_OK;
 }
 
+template <typename T>
+static b2t_status launch_split(const void *src, size_t src_pitch, const b2t_dims3d &d, const FDKWeights &P,
+                               const float *rel_dev, __nv_bfloat16 *a, int khp, long long M, void *dst,
+                               long long dst_row, long long dst_v, int blocks, size_t smem, cudaStream_t s)
+{
+    auto kern = fdk_split_kernel<T>;
+    B2T_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                 "ramp filter split smem attribute");
+    kern<<<blocks, SPLIT_THREADS, smem, s>>>(static_cast<const T *>(src), (long long)src_pitch, (int)d.det_u,
+                                             (int)d.angles, (int)d.det_v, P, rel_dev, a, khp, M,
+                                             static_cast<T *>(dst), dst_row, dst_v);
+    count_launches(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "ramp filter split launch");
+    return B2T_OK;
+}
+
 static b2t_status run_filter(const b2t_dims3d &d, const FDKWeights &P, const std::vector<float> &rel, int filter,
                              const void *src, size_t src_pitch, void *dst, long long dst_row, long long dst_v,
                              int32_t dtype, cudaStream_t s)
@@ -270,6 +377,35 @@ static b2t_status run_filter(const b2t_dims3d &d, const FDKWeights &P, const std
         rel_dev = rs.as<float>();
     }
     const int do_filter = (filter == B2T_FILTER_RAMLAK) ? 1 : 0;
+    // Ram-Lak on the tensor cores (ramp_tc.cu) when the shape allows it and
+    // its scratch fits; otherwise the SIMT Toeplitz kernel below
+    RampTCPlan plan;
+    const long long M = (long long)d.angles * d.det_v;
+    if (do_filter && ramp_tc_enabled() && ramp_tc_plan(d.det_u, M, plan)) {
+        Scratch sa, sb;
+        b2t_status st = sa.alloc(plan.a_elems * sizeof(__nv_bfloat16), s, "ramp filter split rows");
+        if (st == B2T_OK) st = sb.alloc(plan.b_elems * sizeof(__nv_bfloat16), s, "ramp filter taps");
+        if (st == B2T_OK) {
+            __nv_bfloat16 *a = sa.as<__nv_bfloat16>();
+            const long long blocks = (M + SPLIT_ROWS - 1) / SPLIT_ROWS;
+            const size_t smem = sizeof(float) * SPLIT_ROWS * ((size_t)d.det_u + 2 * RAMP_TC_BAND + 2);
+            if (blocks > 0x7fffffffLL || smem > 200 * 1024)
+                return fail(B2T_ERR_UNSUPPORTED, "ramp filter: %lld rows of %u columns are too many", M, d.det_u);
+            if (dtype == B2T_F32)
+                st = launch_split<float>(src, src_pitch, d, P, rel_dev, a, plan.khp, M, dst, dst_row, dst_v,
+                                         (int)blocks, smem, s);
+            else if (dtype == B2T_F16)
+                st = launch_split<__half>(src, src_pitch, d, P, rel_dev, a, plan.khp, M, dst, dst_row, dst_v,
+                                          (int)blocks, smem, s);
+            else
+                st = launch_split<__nv_bfloat16>(src, src_pitch, d, P, rel_dev, a, plan.khp, M, dst, dst_row,
+                                                 dst_v, (int)blocks, smem, s);
+            if (st != B2T_OK) return st;
+            return ramp_tc_filter(plan, a, sb.as<__nv_bfloat16>(), dst, dst_row, dst_v, (int)d.angles, dtype, s);
+        }
+        if (st != B2T_ERR_NO_MEMORY) return st;
+        clear_error();  // not enough memory for the split operands: SIMT filter
+    }
     if (dtype == B2T_F32) return launch_filter<float>(src, src_pitch, d, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
     if (dtype == B2T_F16) return launch_filter<__half>(src, src_pitch, d, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
     return launch_filter<__nv_bfloat16>(src, src_pitch, d, P, rel_dev, do_filter, dst, dst_row, dst_v, s);

@@ -1,0 +1,375 @@
+// Ray-driven 3D forward projection from a "bilinear cell" copy of the volume.
+//
+// Same model as fp3d_kernel (the reference's cone_FP_t / par3D_FP_t,
+// cuda/3d/cone_fp.cu:154-231, cuda/3d/par3d_fp.cu:152-230): per ray, the
+// slices of the view's dominant axis are sampled bilinearly at unit steps.
+//
+// The direct-load kernel issues four scalar loads per sample and is bound by
+// the L1/TEX pipeline (about seven sectors per warp load).  Here the volume is
+// first rewritten, once per call and per marching direction present, into a
+// grid of cells: the cell at texel (k1, k2) of slice s holds everything the
+// bilinear sample with base texel (k1, k2) needs, so a sample is one aligned
+// vector load:
+//   FP32 storage:      float4 (c0, c1, c2, c3) with
+//                      c0 = v00, c1 = v10 - v00, c2 = v01 - v00,
+//                      c3 = v11 - v10 - v01 + v00,
+//                      value = c0 + f1 c1 + f2 (c2 + f1 c3)  (three FMAs);
+//   FP16/BF16 storage: the four corner values (8 bytes), interpolated in FP32
+//                      (no re-rounding of the stored data).
+// Cells cover padded texel indices -2..n+1 in both plane axes (the texture
+// border is zero), so every ray's clipped slice range stays inside the grid
+// exactly as in fp3d_kernel.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <vector>
+
+#include "b2t_internal.h"
+#include "proj3d.h"
+
+namespace b2t {
+
+namespace {
+
+template <typename T> __device__ __forceinline__ float vload(const T *p);
+template <> __device__ __forceinline__ float vload<float>(const float *p) { return __ldg(p); }
+template <> __device__ __forceinline__ float vload<__half>(const __half *p) { return __half2float(__ldg(p)); }
+template <> __device__ __forceinline__ float vload<__nv_bfloat16>(const __nv_bfloat16 *p)
+{
+    return __bfloat162float(__ldg(p));
+}
+template <typename T> __device__ __forceinline__ T vstore(float v);
+template <> __device__ __forceinline__ float vstore<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half vstore<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 vstore<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+// Cell storage per type: 16 bytes (float coefficients) or 8 bytes (corners).
+template <typename T> struct CellT;
+template <> struct CellT<float> { using type = float4; };
+template <> struct CellT<__half> { using type = uint2; };
+template <> struct CellT<__nv_bfloat16> { using type = uint2; };
+
+__device__ __forceinline__ float4 make_cell(float v00, float v10, float v01, float v11, float *)
+{
+    return make_float4(v00, v10 - v00, v01 - v00, (v11 - v10) - (v01 - v00));
+}
+
+template <typename H> __device__ __forceinline__ uint2 pack_corners(float v00, float v10, float v01, float v11);
+template <> __device__ __forceinline__ uint2 pack_corners<__half>(float v00, float v10, float v01, float v11)
+{
+    __half2 a = __floats2half2_rn(v00, v10), b = __floats2half2_rn(v01, v11);
+    return make_uint2(*reinterpret_cast<unsigned *>(&a), *reinterpret_cast<unsigned *>(&b));
+}
+template <> __device__ __forceinline__ uint2 pack_corners<__nv_bfloat16>(float v00, float v10, float v01, float v11)
+{
+    __nv_bfloat162 a = __floats2bfloat162_rn(v00, v10), b = __floats2bfloat162_rn(v01, v11);
+    return make_uint2(*reinterpret_cast<unsigned *>(&a), *reinterpret_cast<unsigned *>(&b));
+}
+
+// Interpolate a cell at weights (f1, f2).
+__device__ __forceinline__ float interp(const float4 &c, float f1, float f2)
+{
+    return fmaf(f2, fmaf(f1, c.w, c.z), fmaf(f1, c.y, c.x));
+}
+template <typename H> __device__ __forceinline__ float interp_corners(uint2 c, float f1, float f2);
+template <> __device__ __forceinline__ float interp_corners<__half>(uint2 c, float f1, float f2)
+{
+    const float2 a = __half22float2(*reinterpret_cast<__half2 *>(&c.x));
+    const float2 b = __half22float2(*reinterpret_cast<__half2 *>(&c.y));
+    const float r0 = fmaf(f1, a.y - a.x, a.x), r1 = fmaf(f1, b.y - b.x, b.x);
+    return fmaf(f2, r1 - r0, r0);
+}
+template <> __device__ __forceinline__ float interp_corners<__nv_bfloat16>(uint2 c, float f1, float f2)
+{
+    const float2 a = __bfloat1622float2(*reinterpret_cast<__nv_bfloat162 *>(&c.x));
+    const float2 b = __bfloat1622float2(*reinterpret_cast<__nv_bfloat162 *>(&c.y));
+    const float r0 = fmaf(f1, a.y - a.x, a.x), r1 = fmaf(f1, b.y - b.x, b.x);
+    return fmaf(f2, r1 - r0, r0);
+}
+
+// Builds the cells of direction `dir`: cell index (j2 * n0 + s) * m1 + j1 for
+// dir 0 / 1, (s * m2 + j2) * m1 + j1 for dir 2, m = n + 4, j = k + 2.
+template <typename T>
+__global__ void build_cells(const T *__restrict__ vol, size_t pitch, int nx, int ny, int nz, int dir,
+                            typename CellT<T>::type *__restrict__ cells)
+{
+    const int j1 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j2 = blockIdx.y;
+    const int s = blockIdx.z;
+    int n1, n2;
+    if (dir == 0) { n1 = ny; n2 = nz; }
+    else if (dir == 1) { n1 = nx; n2 = nz; }
+    else { n1 = nx; n2 = ny; }
+    const int m1 = n1 + 4, m2 = n2 + 4;
+    if (j1 >= m1) return;
+    const int k1 = j1 - 2, k2 = j2 - 2;
+    float v[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int a1 = k1 + (c & 1), a2 = k2 + (c >> 1);
+        float val = 0.0f;
+        if (a1 >= 0 && a1 < n1 && a2 >= 0 && a2 < n2) {
+            int x, y, z;
+            if (dir == 0) { x = s; y = a1; z = a2; }
+            else if (dir == 1) { x = a1; y = s; z = a2; }
+            else { x = a1; y = a2; z = s; }
+            val = vload(vol + ((size_t)z * ny + y) * pitch + x);
+        }
+        v[c] = val;
+    }
+    size_t idx;
+    if (dir == 2) idx = ((size_t)s * m2 + j2) * m1 + j1;
+    else {
+        const int n0 = (dir == 0) ? nx : ny;
+        idx = ((size_t)j2 * n0 + s) * m1 + j1;
+    }
+    if constexpr (sizeof(typename CellT<T>::type) == 16) {
+        cells[idx] = make_cell(v[0], v[1], v[2], v[3], nullptr);
+    } else {
+        cells[idx] = pack_corners<T>(v[0], v[1], v[2], v[3]);
+    }
+}
+
+__device__ __forceinline__ void split_texel_c(float qm, int &k, float &f)
+{
+    const float M = 12582912.0f;
+    float t = __fadd_rn(qm, M);
+    float r = __fadd_rn(t, -M);
+    k = __float_as_int(t) - 0x4B400000;
+    f = __fadd_rn(__fadd_rn(qm, -r), 0.5f);
+}
+
+__device__ __forceinline__ void clip_slices_c(float A, float B, float lo, float hi, float &smin, float &smax)
+{
+    if (fabsf(A) < 1e-12f) {
+        if (!(B >= lo && B <= hi)) {
+            smin = 1.0f;
+            smax = 0.0f;
+        }
+        return;
+    }
+    float s1 = (lo - B) / A, s2 = (hi - B) / A;
+    smin = fmaxf(smin, fminf(s1, s2));
+    smax = fminf(smax, fmaxf(s1, s2));
+}
+
+__device__ __forceinline__ bool texel_ok_c(float A, float B, int s, int n)
+{
+    int k;
+    float f;
+    split_texel_c(fmaf(A, (float)s, B), k, f);
+    return k >= -2 && k <= n;
+}
+
+template <typename T>
+__device__ __forceinline__ float cell_value(const typename CellT<T>::type *p, float f1, float f2)
+{
+    if constexpr (sizeof(typename CellT<T>::type) == 16) {
+        return interp(__ldg(p), f1, f2);
+    } else {
+        return interp_corners<T>(__ldg(p), f1, f2);
+    }
+}
+
+// L.vol points at the cell of padded texel (k1 = 0, k2 = 0) of slice 0, i.e.
+// the cell array base + 2 * st2 + 2 (strides in cells).
+//
+// A CTA traces one 32 x VROWS tile of detector pixels for VPC consecutive
+// views (threadIdx.z selects the view).  Neighbouring views sample nearly the
+// same cells at the same slice (the orbit turns by a fraction of a degree
+// per view), and the warps of one CTA share an SM, so the views of a CTA
+// reuse each other's cells in L1 instead of fetching them again from L2.
+template <typename T, int VPC, int VROWS>
+__global__ void __launch_bounds__(32 * VROWS * VPC, 2048 / (32 * VROWS * VPC)) fp3d_cell_kernel(const __grid_constant__ FPLaunch L)
+{
+    using C = typename CellT<T>::type;
+    const int vi = blockIdx.x * VPC + threadIdx.z;
+    if (vi >= L.nviews) return;
+    const FPView &V = L.views[vi];
+    const int u = blockIdx.y * 32 + threadIdx.x;
+    const int v = blockIdx.z * VROWS + threadIdx.y;
+    if (u >= L.nu || v >= L.nv) return;
+    const C *__restrict__ cells = static_cast<const C *>(L.vol);
+    const long long st0 = L.st0, st2 = L.st2;
+    const int R = L.rays;
+    const float n0 = (float)L.n0;
+    float acc = 0.0f;
+    for (int iu = 0; iu < R; ++iu) {
+        for (int iv = 0; iv < R; ++iv) {
+            float uu = (float)u + 0.5f - 0.5f * (float)L.nu;
+            float vv = (float)v + 0.5f - 0.5f * (float)L.nv;
+            if (R > 1) {
+                uu += -0.5f + (0.5f + (float)iu) / (float)R;
+                vv += -0.5f + (0.5f + (float)iv) / (float)R;
+            }
+            const float den = fmaf(vv, V.e[2], fmaf(uu, V.e[1], V.e[0]));
+            const float inv = 1.0f / den;
+            const float A1 = fmaf(vv, V.m1[2], fmaf(uu, V.m1[1], V.m1[0])) * inv;
+            const float A2 = fmaf(vv, V.m2[2], fmaf(uu, V.m2[1], V.m2[0])) * inv;
+            const float B1 = fmaf(vv, V.n1[2], fmaf(uu, V.n1[1], V.n1[0])) * inv;
+            const float B2 = fmaf(vv, V.n2[2], fmaf(uu, V.n2[1], V.n2[0])) * inv;
+            float smin = 0.0f, smax = n0 - 1.0f;
+            clip_slices_c(A1, B1, -1.6f, (float)L.n1 - 0.4f, smin, smax);
+            clip_slices_c(A2, B2, -1.6f, (float)L.n2 - 0.4f, smin, smax);
+            int s_lo = max(0, (int)ceilf(fmaxf(smin, -1.0f)));
+            int s_hi = min(L.n0 - 1, (int)floorf(fminf(smax, n0)));
+            for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
+                if (texel_ok_c(A1, B1, s_lo, L.n1) && texel_ok_c(A2, B2, s_lo, L.n2)) break;
+                ++s_lo;
+            }
+            for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
+                if (texel_ok_c(A1, B1, s_hi, L.n1) && texel_ok_c(A2, B2, s_hi, L.n2)) break;
+                --s_hi;
+            }
+            if (!(texel_ok_c(A1, B1, s_lo, L.n1) && texel_ok_c(A2, B2, s_lo, L.n2) &&
+                  texel_ok_c(A1, B1, s_hi, L.n1) && texel_ok_c(A2, B2, s_hi, L.n2)))
+                s_hi = s_lo - 1;
+            // two independent accumulators keep two loads in flight per thread
+            float sum0 = 0.0f, sum1 = 0.0f;
+            int s = s_lo;
+            for (; s + 1 <= s_hi; s += 2) {
+                int k1a, k2a, k1b, k2b;
+                float f1a, f2a, f1b, f2b;
+                split_texel_c(fmaf(A1, (float)s, B1), k1a, f1a);
+                split_texel_c(fmaf(A2, (float)s, B2), k2a, f2a);
+                split_texel_c(fmaf(A1, (float)(s + 1), B1), k1b, f1b);
+                split_texel_c(fmaf(A2, (float)(s + 1), B2), k2b, f2b);
+                const C *pa = cells + (long long)s * st0 + (long long)k2a * st2 + k1a;
+                const C *pb = cells + (long long)(s + 1) * st0 + (long long)k2b * st2 + k1b;
+                sum0 += cell_value<T>(pa, f1a, f2a);
+                sum1 += cell_value<T>(pb, f1b, f2b);
+            }
+            if (s <= s_hi) {
+                int k1, k2;
+                float f1, f2;
+                split_texel_c(fmaf(A1, (float)s, B1), k1, f1);
+                split_texel_c(fmaf(A2, (float)s, B2), k2, f2);
+                sum0 += cell_value<T>(cells + (long long)s * st0 + (long long)k2 * st2 + k1, f1, f2);
+            }
+            const float sc = sqrtf(fmaf(A1 * A1, L.f1, fmaf(A2 * A2, L.f2, 1.0f))) * L.mul;
+            acc = fmaf(sum0 + sum1, sc, acc);
+        }
+    }
+    if (R > 1) acc /= (float)(R * R);
+    T *out = static_cast<T *>(L.proj) + ((size_t)v * L.na + V.a) * L.proj_pitch + u;
+    float r = acc;
+    if (L.accumulate) r += (float)(*out);
+    *out = vstore<T>(r);
+}
+
+// Views per CTA of the cell kernel: B2T_FP_VPC (1, 2, 4 or 8) or 4.
+static int cells_vpc()
+{
+    const char *e = std::getenv("B2T_FP_VPC");
+    const int v = e ? std::atoi(e) : 4;
+    return (v == 1 || v == 2 || v == 8) ? v : 4;
+}
+
+template <typename T, int VPC, int VROWS>
+static b2t_status launch_cells_shape(const FPLaunch &P, int nviews, const b2t_dims3d &d, cudaStream_t s)
+{
+    dim3 grid((unsigned)((nviews + VPC - 1) / VPC), (d.det_u + 31) / 32, (d.det_v + VROWS - 1) / VROWS);
+    fp3d_cell_kernel<T, VPC, VROWS><<<grid, dim3(32, VROWS, VPC), 0, s>>>(P);
+    count_launches(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "fp3d_cell_kernel launch");
+    return B2T_OK;
+}
+
+template <typename T>
+static b2t_status launch_cells(const FPLaunch &P, int nviews, const b2t_dims3d &d, cudaStream_t s)
+{
+    switch (cells_vpc()) {
+    case 1: return launch_cells_shape<T, 1, 8>(P, nviews, d, s);
+    case 2: return launch_cells_shape<T, 2, 4>(P, nviews, d, s);
+    case 8: return launch_cells_shape<T, 8, 2>(P, nviews, d, s);
+    default: return launch_cells_shape<T, 4, 4>(P, nviews, d, s);
+    }
+}
+
+template <typename T>
+b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch, void *proj,
+                     size_t proj_pitch, int32_t mode, const std::vector<int> &dirs, cudaStream_t s)
+{
+    using C = typename CellT<T>::type;
+    const b2t_dims3d &d = g->dims;
+    bool need[3] = {false, false, false};
+    for (int dd : dirs) need[dd] = true;
+    const int nx = d.vol_x, ny = d.vol_y, nz = d.vol_z;
+    Scratch cs[3];
+    const C *base[3] = {nullptr, nullptr, nullptr};
+    long long st0[3], st2[3];
+    for (int dir = 0; dir < 3; ++dir) {
+        if (!need[dir]) continue;
+        int n0, n1, n2;
+        if (dir == 0) { n0 = nx; n1 = ny; n2 = nz; }
+        else if (dir == 1) { n0 = ny; n1 = nx; n2 = nz; }
+        else { n0 = nz; n1 = nx; n2 = ny; }
+        const long long m1 = n1 + 4, m2 = n2 + 4;
+        const size_t count = (size_t)m1 * m2 * n0;
+        B2T_TRY(cs[dir].alloc(count * sizeof(C), s, "b2t_fp3d scratch (cells)"));
+        dim3 grid((unsigned)((m1 + 127) / 128), (unsigned)m2, (unsigned)n0);
+        build_cells<T><<<grid, 128, 0, s>>>(static_cast<const T *>(vol), vol_pitch, nx, ny, nz, dir, cs[dir].as<C>());
+        count_launches(1);
+        B2T_CUDA_TRY(cudaGetLastError(), "build_cells launch");
+        if (dir == 2) {
+            st0[dir] = m1 * m2;
+            st2[dir] = m1;
+        } else {
+            st0[dir] = m1;
+            st2[dir] = m1 * n0;
+        }
+        base[dir] = cs[dir].as<C>() + 2 * st2[dir] + 2;
+    }
+    FPLaunch *Lp = new FPLaunch;
+    FPLaunch &P = *Lp;
+    const bool force_noncube = p->det_supersample > 1;
+    b2t_status st = B2T_OK;
+    for (int dir = 0; dir < 3 && st == B2T_OK; ++dir) {
+        if (!need[dir]) continue;
+        P.proj = proj;
+        P.proj_pitch = (long long)proj_pitch;
+        P.nu = d.det_u;
+        P.nv = d.det_v;
+        P.na = d.angles;
+        P.rays = p->det_supersample;
+        P.accumulate = (mode == B2T_MODE_ADD) ? 1 : 0;
+        fp_scale(g->kind, dir, g->vol_scale, force_noncube, p->output_scale, P.f1, P.f2, P.mul);
+        if (dir == 0) { P.n0 = nx; P.n1 = ny; P.n2 = nz; }
+        else if (dir == 1) { P.n0 = ny; P.n1 = nx; P.n2 = nz; }
+        else { P.n0 = nz; P.n1 = nx; P.n2 = ny; }
+        P.st0 = st0[dir];
+        P.st2 = st2[dir];
+        P.vol = base[dir];
+        std::vector<int> views;
+        for (uint32_t a = 0; a < d.angles; ++a)
+            if (dirs[a] == dir) views.push_back((int)a);
+        for (size_t c0 = 0; c0 < views.size() && st == B2T_OK; c0 += FP_MAX_VIEWS) {
+            const size_t cn = std::min(views.size() - c0, (size_t)FP_MAX_VIEWS);
+            P.nviews = (int)cn;
+            for (size_t i = 0; i < cn; ++i) {
+                const int a = views[c0 + i];
+                fp_view_coeffs(g->kind, g->views[a], d, dir, P.views[i]);
+                P.views[i].a = a;
+            }
+            st = launch_cells<T>(P, (int)cn, d, s);
+            if (st != B2T_OK) break;
+        }
+    }
+    delete Lp;
+    return st;
+}
+
+}  // namespace
+
+b2t_status fp3d_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch, void *proj,
+                      size_t proj_pitch, int32_t dtype, int32_t mode, const std::vector<int> &dirs, cudaStream_t s)
+{
+    if (dtype == B2T_F32) return run_cells<float>(g, p, vol, vol_pitch, proj, proj_pitch, mode, dirs, s);
+    if (dtype == B2T_F16) return run_cells<__half>(g, p, vol, vol_pitch, proj, proj_pitch, mode, dirs, s);
+    return run_cells<__nv_bfloat16>(g, p, vol, vol_pitch, proj, proj_pitch, mode, dirs, s);
+}
+
+}  // namespace b2t

@@ -11,7 +11,8 @@
 //
 // One launch covers every view of a chunk: FP threads own one ray (all
 // slices accumulated in registers), BP threads own one pixel (all views of
-// the chunk accumulated in registers).
+// the chunk accumulated in registers).  The per-ray and per-pixel bodies live
+// in proj2d_dev.cuh, shared with the batched kernels.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -20,22 +21,11 @@
 
 #include "b2t_internal.h"
 #include "proj2d.h"
+#include "proj2d_dev.cuh"
 
 namespace b2t {
 
 namespace {
-
-// linear interpolation of a 1D line at continuous index q (texel i at q = i),
-// zero outside [0, n)
-__device__ __forceinline__ float lerp_line(const float *__restrict__ p, long long stride, int n, float q)
-{
-    const float fl = floorf(q);
-    const int k = (int)fl;
-    const float f = q - fl;
-    const float a = (k >= 0 && k < n) ? __ldg(p + (long long)k * stride) : 0.0f;
-    const float b = (k + 1 >= 0 && k + 1 < n) ? __ldg(p + (long long)(k + 1) * stride) : 0.0f;
-    return fmaf(f, b - a, a);
-}
 
 __global__ void __launch_bounds__(256) fp2d_par_kernel(const __grid_constant__ FP2DParLaunch L)
 {
@@ -43,21 +33,8 @@ __global__ void __launch_bounds__(256) fp2d_par_kernel(const __grid_constant__ F
     const int vi = blockIdx.y;
     if (det >= L.ndet) return;
     const ParFPView &V = L.views[vi];
-    const int R = L.rays;
-    float acc = 0.0f;
-    for (int r = 0; r < R; ++r) {
-        const float p0 = fmaf((float)det + (0.5f + (float)r) / (float)R - 0.5f, V.detstep, V.p0);
-        if (!V.vertical) {
-            // slices are columns; the sample moves along the rows
-            for (int sl = 0; sl < L.W; ++sl)
-                acc += lerp_line(L.vol + sl, L.vol_pitch, L.H, fmaf((float)sl, V.slicestep, p0) - 0.5f);
-        } else {
-            for (int sl = 0; sl < L.H; ++sl)
-                acc += lerp_line(L.vol + (long long)sl * L.vol_pitch, 1, L.W, fmaf((float)sl, V.slicestep, p0) - 0.5f);
-        }
-    }
+    const float acc = fp2d_par_ray(L.vol, L.vol_pitch, L.W, L.H, V, det, L.rays);
     float *out = L.sino + (long long)V.a * L.sino_pitch + det;
-    acc *= V.corr / (float)R;
     *out = L.accumulate ? *out + acc : acc;
 }
 
@@ -66,38 +43,7 @@ __global__ void __launch_bounds__(256) fp2d_fan_kernel(const __grid_constant__ F
     const int det = blockIdx.x * blockDim.x + threadIdx.x;
     const int vi = blockIdx.y;
     if (det >= L.ndet) return;
-    const b2t_view2d &V = L.views[vi];
-    // per-ray orientation choice, in float as the reference evaluates it
-    const float fdx = fabsf(fmaf((float)det, V.det_u[0], V.det_s[0]) + 0.5f - V.src[0]);
-    const float fdy = fabsf(fmaf((float)det, V.det_u[1], V.det_s[1]) + 0.5f - V.src[1]);
-    const bool horizontal = !(fdy > fdx);
-    const int R = L.rays;
-    float acc = 0.0f;
-    for (int r = 0; r < R; ++r) {
-        // ray set-up in FP64: the source sits far from the origin
-        const double fdet = det + (0.5 + r) / (double)R;
-        const double DX = V.det_s[0] + fdet * V.det_u[0];
-        const double DY = V.det_s[1] + fdet * V.det_u[1];
-        float sum = 0.0f, corr;
-        if (horizontal) {
-            const double alpha = (V.src[1] - DY) / (V.src[0] - DX);
-            const double beta = V.src[1] - alpha * V.src[0];
-            corr = (float)(sqrt(alpha * alpha + 1.0) * L.out_scale / R);
-            const float y0 = (float)(-alpha * (0.5 - 0.5 * L.W) - beta + 0.5 * L.H - 0.5);
-            const float dy = (float)-alpha;
-            for (int sl = 0; sl < L.W; ++sl)
-                sum += lerp_line(L.vol + sl, L.vol_pitch, L.H, fmaf((float)sl, dy, y0));
-        } else {
-            const double alpha = (V.src[0] - DX) / (V.src[1] - DY);
-            const double beta = V.src[0] - alpha * V.src[1];
-            corr = (float)(sqrt(alpha * alpha + 1.0) * L.out_scale / R);
-            const float x0 = (float)(-alpha * (0.5 - 0.5 * L.H) + beta + 0.5 * L.W - 0.5);
-            const float dx = (float)-alpha;
-            for (int sl = 0; sl < L.H; ++sl)
-                sum += lerp_line(L.vol + (long long)sl * L.vol_pitch, 1, L.W, fmaf((float)sl, dx, x0));
-        }
-        acc = fmaf(sum, corr, acc);
-    }
+    const float acc = fp2d_fan_ray(L.vol, L.vol_pitch, L.W, L.H, L.views[vi], det, L.rays, L.out_scale);
     float *out = L.sino + (long long)(L.a0 + vi) * L.sino_pitch + det;
     *out = L.accumulate ? *out + acc : acc;
 }
@@ -107,36 +53,8 @@ __global__ void __launch_bounds__(256) bp2d_kernel(const __grid_constant__ BP2DL
     const int X = blockIdx.x * 32 + threadIdx.x;
     const int Y = blockIdx.y * 8 + threadIdx.y;
     if (X >= L.W || Y >= L.H) return;
-    const int R = L.rays;
-    const float sub = 1.0f / (float)R;
-    float acc = 0.0f;
-    for (int i = 0; i < L.nviews; ++i) {
-        const BPView2D &C = L.views[i];
-        const float *row = L.sino + (long long)(L.a0 + i) * L.sino_pitch;
-        for (int ix = 0; ix < R; ++ix) {
-            for (int iy = 0; iy < R; ++iy) {
-                float x = (float)X - 0.5f * (float)L.W + 0.5f;
-                float y = (float)Y - 0.5f * (float)L.H + 0.5f;
-                if (R > 1) {
-                    x += -0.5f + 0.5f * sub + (float)ix * sub;
-                    y += -0.5f + 0.5f * sub + (float)iy * sub;
-                }
-                if (L.kind == B2T_GEOM_PAR2D) {
-                    // T = x c - y s + offset (par_bp.cu:78-81)
-                    const float T = fmaf(x, C.c[0], fmaf(-y, C.c[1], C.c[2]));
-                    acc = fmaf(lerp_line(row, 1, L.ndet, T - 0.5f), C.c[3], acc);
-                } else {
-                    // world y is flipped (fan_bp.cu:73)
-                    const float yw = -y;
-                    const float num = fmaf(x, C.c[1], fmaf(yw, C.c[2], C.c[0]));
-                    const float den = fmaf(x, C.c[4], fmaf(yw, C.c[5], C.c[3]));
-                    const float fr = 1.0f / den;
-                    const float w = L.fbp ? fr * fr : fr;
-                    acc = fmaf(lerp_line(row, 1, L.ndet, num * fr - 0.5f), w, acc);
-                }
-            }
-        }
-    }
+    const float acc = bp2d_pixel(L.sino, L.sino_pitch, L.a0, L.nviews, L.views, L.W, L.H, L.ndet, L.rays, L.kind,
+                                 L.fbp, X, Y);
     float *o = L.vol + (long long)Y * L.vol_pitch + X;
     const float r = acc * L.out_scale;
     *o = L.accumulate ? *o + r : r;

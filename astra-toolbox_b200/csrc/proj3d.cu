@@ -605,6 +605,14 @@ bool force_simple_bp()
     return e && e[0] == '1';
 }
 
+// B2T_SIMPLE_FP=1 selects the padded-copy forward projector instead of the
+// cell one (same model; tests compare them).
+bool force_simple_fp()
+{
+    const char *e = getenv("B2T_SIMPLE_FP");
+    return e && e[0] == '1';
+}
+
 b2t_status validate3d(const b2t_geom3d *g, const char *who)
 {
     if (!g || !g->views) return fail(B2T_ERR_INVALID_ARG, "%s: null geometry", who);
@@ -647,6 +655,13 @@ b2t_status fp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
     for (uint32_t a = 0; a < d.angles; ++a) {
         dirs[a] = dominant_axis(g->kind, g->views[a], d);
         need[dirs[a]] = true;
+    }
+    if (!force_simple_fp()) {
+        // cell path (fp3d_cells.cu); if its scratch does not fit, use the
+        // padded-copy path below, which needs a quarter of the memory
+        const b2t_status st = fp3d_cells(g, p, vol, vol_pitch, proj, proj_pitch, dtype, mode, dirs, s);
+        if (st != B2T_ERR_NO_MEMORY) return st;
+        clear_error();
     }
     const size_t esz = dtype_size(dtype);
     const size_t px = d.vol_x + 4, py = d.vol_y + 4, pz = d.vol_z + 4;

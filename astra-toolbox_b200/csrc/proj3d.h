@@ -5,6 +5,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "b2tomo.h"
 
 namespace b2t {
@@ -95,6 +97,9 @@ void fp_scale(int kind, int dir, const float *vs, bool force_noncube, float out_
 void bp_view_coeffs(int kind, int kernel, const b2t_view3d &w, const float *vs, BPView &o);
 b2t_status validate3d(const b2t_geom3d *g, const char *who);
 bool force_simple_bp();
+bool force_simple_fp();
+b2t_status fp3d_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch, void *proj,
+                      size_t proj_pitch, int32_t dtype, int32_t mode, const std::vector<int> &dirs, cudaStream_t s);
 
 b2t_status fp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch,
                      void *proj, size_t proj_pitch, int32_t dtype, int32_t mode, cudaStream_t s);

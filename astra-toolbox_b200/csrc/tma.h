@@ -14,9 +14,11 @@
 namespace b2t {
 
 // Host: encode a tiled tensor map.  rank <= 5; dims/strides/box in elements /
-// bytes as cuTensorMapEncodeTiled expects (strides of dims 1..rank-1).
+// bytes as cuTensorMapEncodeTiled expects (strides of dims 1..rank-1).  Out of
+// range elements read as zero.
 b2t_status encode_tensor_map(CUtensorMap *map, CUtensorMapDataType dtype, uint32_t rank, const void *base,
-                             const uint64_t *dims, const uint64_t *strides_bytes, const uint32_t *box);
+                             const uint64_t *dims, const uint64_t *strides_bytes, const uint32_t *box,
+                             CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE);
 
 // Device-side error bits: kernels OR them into their translation unit's
 // error word instead of trapping; b2t_device_errors() reads and clears them.

@@ -362,6 +362,56 @@ b2t_status b2t_algo_residual_norm(b2t_algo *algo, const float *sino, const float
 void b2t_algo_abort(b2t_algo *algo);
 void b2t_algo_destroy(b2t_algo *algo);
 
+/* ---------------------------------------------------------------------- */
+/* batched 2D problems                                                     */
+/* ---------------------------------------------------------------------- */
+
+/* One problem of a batch: its normalised geometry and supersampling. */
+typedef struct b2t_problem2d {
+    b2t_geom2d geom;              /* kind, dims, output scale, host views        */
+    uint32_t det_supersample;     /* FP rays per detector (DetectorSuperSampling) */
+    uint32_t pixel_supersample;   /* BP sub-pixels per axis (PixelSuperSampling)  */
+} b2t_problem2d;
+
+typedef struct b2t_batch2d b2t_batch2d;  /* opaque: device tables + work list */
+
+/* Plan a batch of n independent 2D problems (parallel and fan mixed, any
+ * sizes).  No counterpart in the reference, which projects such a set one
+ * problem at a time through FP / FanFP / BP / FanBP
+ * (include/astra/cuda/2d/par_fp.h:33, fan_fp.h, par_bp.h, fan_bp.h:33-44), at
+ * least one launch each.  Copies the geometry to the device (synchronous,
+ * allocates with cudaMalloc).  Problem i's volume (H x W, row-major) and
+ * sinogram (angles x dets) live in two packed buffers at the element offsets
+ * b2t_batch2d_layout reports. */
+b2t_status b2t_batch2d_create(const b2t_problem2d *problems, int32_t n, b2t_batch2d **out);
+/* Offsets (elements) of every problem in the packed buffers, and the buffer
+ * lengths.  vol_offsets / sino_offsets hold n entries each (may be NULL). */
+b2t_status b2t_batch2d_layout(const b2t_batch2d *batch, uint64_t *vol_offsets, uint64_t *sino_offsets,
+                              uint64_t *vol_total, uint64_t *sino_total);
+/* sinos (=|+=) A vols for every problem, in one persistent launch. */
+b2t_status b2t_batch2d_fp(b2t_batch2d *batch, const float *vols, float *sinos, int32_t mode, void *stream);
+/* vols (=|+=) A^T-style backprojection of sinos for every problem (the
+ * reference's unmatched BP), in one persistent launch. */
+b2t_status b2t_batch2d_bp(b2t_batch2d *batch, const float *sinos, float *vols, int32_t mode, void *stream);
+/* SIRT_CUDA on every problem of the batch at once (src/CudaSirtAlgorithm.cpp):
+ * run with b2t_algo_run / b2t_algo_residual_norm on the packed buffers.  Only
+ * B2T_ALGO_SIRT; options as for b2t_algo_create2d without masks.  The batch
+ * must outlive the algorithm. */
+b2t_status b2t_algo_create_batch2d(int32_t type, b2t_batch2d *batch, const b2t_algo_options *options,
+                                   b2t_algo **out);
+void b2t_batch2d_destroy(b2t_batch2d *batch);
+
+/* ---------------------------------------------------------------------- */
+/* measurement                                                             */
+/* ---------------------------------------------------------------------- */
+
+/* On-chip load bandwidth of the current GPU in GB/s (no counterpart in the
+ * reference): which = 0 streams 16-byte shared-memory loads, which = 1
+ * streams 16-byte global loads that hit L1.  The projectors' interpolation
+ * reads are bound by this roof rather than by HBM.  Synchronous; allocates
+ * nothing. */
+b2t_status b2t_onchip_peak(int32_t which, double *gbs);
+
 #ifdef __cplusplus
 }
 #endif
