@@ -112,6 +112,15 @@ class Batch2D:
              max_constraint=None):
         """SIRT_CUDA on every problem at once; vols is updated in place.
         Returns the batch's residual norm ||b - A x|| over all problems."""
+        return self._iterate(_lib.ALGO_SIRT, sinos, vols, iterations, use_graph, relaxation, min_constraint,
+                             max_constraint)
+
+    def cgls(self, sinos, vols, iterations, use_graph=True):
+        """CGLS_CUDA on every problem at once (per-problem step sizes); vols
+        is updated in place.  Returns the batch's residual norm."""
+        return self._iterate(_lib.ALGO_CGLS, sinos, vols, iterations, use_graph, 1.0, None, None)
+
+    def _iterate(self, kind, sinos, vols, iterations, use_graph, relaxation, min_constraint, max_constraint):
         self._check(sinos, self.sino_total, "packed sinograms")
         self._check(vols, self.vol_total, "packed volumes")
         opt = _lib.AlgoOptions(float(relaxation), int(min_constraint is not None),
@@ -119,7 +128,7 @@ class Batch2D:
                                float(max_constraint if max_constraint is not None else 0.0), None, None, None, None)
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            _lib.call("b2t_algo_create_batch2d", _lib.ALGO_SIRT, self.handle, ctypes.byref(opt), ctypes.byref(h))
+            _lib.call("b2t_algo_create_batch2d", kind, self.handle, ctypes.byref(opt), ctypes.byref(h))
             try:
                 _lib.call("b2t_algo_run", h, sinos.data_ptr(), vols.data_ptr(), int(iterations), int(bool(use_graph)),
                           stream_handle(self.device))

@@ -17,6 +17,7 @@
 //     run() and replayed (the graph is rebuilt if the data pointers change).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <memory>
 
@@ -97,6 +98,75 @@ __global__ void xpby_ratio_kernel(float *__restrict__ p, const float *__restrict
         p[i] = fmaf(p[i], beta, z[i]);
 }
 
+// Per-problem (segmented) forms for CGLS on a batch of problems: scalars are
+// stored slot-major, s[slot * nseg + problem].  Deterministic: each chunk
+// reduces in a fixed order, and each problem's chunks are summed in order.
+constexpr int SEG_THREADS = 256;
+
+__global__ void __launch_bounds__(SEG_THREADS) seg_dot_partial_kernel(const float *__restrict__ a,
+                                                                       const SegChunk *__restrict__ chunks,
+                                                                       double *__restrict__ partial)
+{
+    __shared__ double red[SEG_THREADS / 32];
+    const SegChunk c = chunks[blockIdx.x];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < c.len; i += SEG_THREADS) {
+        const double v = (double)a[c.begin + i];
+        acc = fma(v, v, acc);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < SEG_THREADS / 32; ++w) t += red[w];
+        partial[blockIdx.x] = t;
+    }
+}
+
+// one thread per problem: s[slot * nseg + p] = sum of its chunks' partials
+__global__ void seg_dot_final_kernel(const double *__restrict__ partial, const int *__restrict__ first, int nseg,
+                                     double *__restrict__ s, int slot)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nseg) return;
+    double t = 0.0;
+    for (int c = first[p]; c < first[p + 1]; ++c) t += partial[c];
+    s[slot * nseg + p] = t;
+}
+
+// step size of problem p; 0 when its denominator is 0 (a problem whose data
+// are all zero stays at its start instead of turning into NaN)
+__device__ __forceinline__ float seg_ratio(const double *s, int nseg, int num, int den, int p)
+{
+    const double d = s[den * nseg + p];
+    return d != 0.0 ? (float)(s[num * nseg + p] / d) : 0.0f;
+}
+
+// x += sign * ratio_p * y on every chunk (chunk = one CTA)
+__global__ void __launch_bounds__(SEG_THREADS) seg_axpy_ratio_kernel(float *__restrict__ x,
+                                                                      const float *__restrict__ y,
+                                                                      const SegChunk *__restrict__ chunks,
+                                                                      const double *__restrict__ s, int nseg, int num,
+                                                                      int den, float sign)
+{
+    const SegChunk c = chunks[blockIdx.x];
+    const float a = sign * seg_ratio(s, nseg, num, den, c.seg);
+    for (int i = threadIdx.x; i < c.len; i += SEG_THREADS) x[c.begin + i] = fmaf(a, y[c.begin + i], x[c.begin + i]);
+}
+
+// p = z + ratio_p * p on every chunk
+__global__ void __launch_bounds__(SEG_THREADS) seg_xpby_ratio_kernel(float *__restrict__ p,
+                                                                      const float *__restrict__ z,
+                                                                      const SegChunk *__restrict__ chunks,
+                                                                      const double *__restrict__ s, int nseg, int num,
+                                                                      int den)
+{
+    const SegChunk c = chunks[blockIdx.x];
+    const float beta = seg_ratio(s, nseg, num, den, c.seg);
+    for (int i = threadIdx.x; i < c.len; i += SEG_THREADS) p[c.begin + i] = fmaf(p[c.begin + i], beta, z[c.begin + i]);
+}
+
 // ---------------------------------------------------------------------------
 // operators
 // ---------------------------------------------------------------------------
@@ -107,6 +177,8 @@ struct Operator {
     virtual b2t_status fp(const float *vol, float *proj, float scale, int mode, cudaStream_t s) = 0;
     // vol (=|+=) scale * B proj
     virtual b2t_status bp(const float *proj, float *vol, float scale, int mode, cudaStream_t s) = 0;
+    // chunk tables when the operator is a batch of independent problems
+    virtual const SegTable *segments(bool vol) const { return nullptr; }
     size_t nvol = 0, nproj = 0;
 };
 
@@ -177,6 +249,7 @@ struct OpBatch2D : Operator {
     {
         return batch2d_bp_impl(b, proj, vol, scale, mode, s);
     }
+    const SegTable *segments(bool vol) const override { return vol ? &b->vol_segs : &b->sino_segs; }
 };
 
 struct DevBuf {
@@ -191,8 +264,13 @@ struct DevBuf {
         cudaError_t e = cudaMalloc(&p, bytes);
         if (e != cudaSuccess) {
             p = nullptr;
+            (void)cudaGetLastError();
             return cuda_fail(e, what);
         }
+        // zero: element-wise passes also run over the gaps between the
+        // problems of a packed batch, which no projector writes
+        e = cudaMemset(p, 0, bytes);
+        if (e != cudaSuccess) return cuda_fail(e, what);
         return B2T_OK;
     }
     template <class T> T *as() const { return static_cast<T *>(p); }
@@ -222,11 +300,53 @@ struct Algo {
 
     size_t nv() const { return op->nvol; }
     size_t np() const { return op->nproj; }
+    int nseg = 1;  // problems sharing the algorithm (a batch), one scalar set each
 
-    b2t_status dot_sq(const float *a, size_t n, int slot, cudaStream_t s)
+    enum class Space { vol, proj };
+
+    // |a|^2 into scalar slot `slot` (per problem on a batch)
+    b2t_status dot_sq(const float *a, Space sp, int slot, cudaStream_t s)
     {
-        const int nb = dot_num_blocks(n);
-        return dot_launch(a, a, n, B2T_F32, partial.as<double>(), nb, scalars.as<double>() + slot, s);
+        const bool is_vol = sp == Space::vol;
+        const SegTable *t = op->segments(is_vol);
+        if (!t) {
+            const size_t n = is_vol ? nv() : np();
+            const int nb = dot_num_blocks(n);
+            return dot_launch(a, a, n, B2T_F32, partial.as<double>(), nb, scalars.as<double>() + slot, s);
+        }
+        seg_dot_partial_kernel<<<t->nchunks, SEG_THREADS, 0, s>>>(a, t->chunks, partial.as<double>());
+        B2T_TRY(ew(cudaGetLastError(), "batch dot partials"));
+        seg_dot_final_kernel<<<(t->nseg + 127) / 128, 128, 0, s>>>(partial.as<double>(), t->first, t->nseg,
+                                                                   scalars.as<double>(), slot);
+        return ew(cudaGetLastError(), "batch dot final");
+    }
+
+    // x += sign * (s[num] / s[den]) * y over a volume or projection buffer
+    b2t_status axpy_ratio(float *x, const float *y, Space sp, int num, int den, float sign, cudaStream_t s)
+    {
+        const bool is_vol = sp == Space::vol;
+        const SegTable *t = op->segments(is_vol);
+        if (!t) {
+            const size_t n = is_vol ? nv() : np();
+            axpy_ratio_kernel<<<ew_blocks(n), EW_THREADS, 0, s>>>(x, y, n, scalars.as<double>(), num, den, sign);
+        } else {
+            seg_axpy_ratio_kernel<<<t->nchunks, SEG_THREADS, 0, s>>>(x, y, t->chunks, scalars.as<double>(), t->nseg,
+                                                                     num, den, sign);
+        }
+        return ew(cudaGetLastError(), "CGLS axpy");
+    }
+
+    // p = z + (s[num] / s[den]) * p over the volume
+    b2t_status xpby_ratio(float *p_, const float *z_, int num, int den, cudaStream_t s)
+    {
+        const SegTable *t = op->segments(true);
+        if (!t) {
+            xpby_ratio_kernel<<<ew_blocks(nv()), EW_THREADS, 0, s>>>(p_, z_, nv(), scalars.as<double>(), num, den);
+        } else {
+            seg_xpby_ratio_kernel<<<t->nchunks, SEG_THREADS, 0, s>>>(p_, z_, t->chunks, scalars.as<double>(), t->nseg,
+                                                                     num, den);
+        }
+        return ew(cudaGetLastError(), "CGLS p update");
     }
 
     b2t_status ew(cudaError_t e, const char *what)
@@ -296,24 +416,20 @@ struct Algo {
         B2T_TRY(ew(cudaGetLastError(), "CGLS residual"));
         B2T_TRY(op->bp(r.as<float>(), p.as<float>(), 1.0f, B2T_MODE_SET, s));
         if (opt.vol_mask) B2T_TRY(vec_op_impl(B2T_OP_MUL, p.as<float>(), opt.vol_mask, nullptr, 0.0f, nv(), s));
-        return dot_sq(p.as<float>(), nv(), 0, s);  // gamma in slot 0
+        return dot_sq(p.as<float>(), Space::vol, 0, s);  // gamma in slot 0
     }
 
     // one CGLS iteration; gamma in slot g, new gamma into slot 1 - g; ww in slot 2
     b2t_status cgls_iteration(float *vol, int g, cudaStream_t s)
     {
         B2T_TRY(op->fp(p.as<float>(), w.as<float>(), 1.0f, B2T_MODE_SET, s));
-        B2T_TRY(dot_sq(w.as<float>(), np(), 2, s));
-        double *sc = scalars.as<double>();
-        axpy_ratio_kernel<<<ew_blocks(nv()), EW_THREADS, 0, s>>>(vol, p.as<float>(), nv(), sc, g, 2, 1.0f);
-        B2T_TRY(ew(cudaGetLastError(), "CGLS x update"));
-        axpy_ratio_kernel<<<ew_blocks(np()), EW_THREADS, 0, s>>>(r.as<float>(), w.as<float>(), np(), sc, g, 2, -1.0f);
-        B2T_TRY(ew(cudaGetLastError(), "CGLS r update"));
+        B2T_TRY(dot_sq(w.as<float>(), Space::proj, 2, s));
+        B2T_TRY(axpy_ratio(vol, p.as<float>(), Space::vol, g, 2, 1.0f, s));
+        B2T_TRY(axpy_ratio(r.as<float>(), w.as<float>(), Space::proj, g, 2, -1.0f, s));
         B2T_TRY(op->bp(r.as<float>(), z.as<float>(), 1.0f, B2T_MODE_SET, s));
         if (opt.vol_mask) B2T_TRY(vec_op_impl(B2T_OP_MUL, z.as<float>(), opt.vol_mask, nullptr, 0.0f, nv(), s));
-        B2T_TRY(dot_sq(z.as<float>(), nv(), 1 - g, s));
-        xpby_ratio_kernel<<<ew_blocks(nv()), EW_THREADS, 0, s>>>(p.as<float>(), z.as<float>(), nv(), sc, 1 - g, g);
-        return ew(cudaGetLastError(), "CGLS p update");
+        B2T_TRY(dot_sq(z.as<float>(), Space::vol, 1 - g, s));
+        return xpby_ratio(p.as<float>(), z.as<float>(), 1 - g, g, s);
     }
 
     b2t_status iteration(const float *sino, float *vol, int parity, cudaStream_t s)
@@ -351,8 +467,14 @@ b2t_status algo_create(int32_t type, Operator *op_raw, const b2t_algo_options *o
         B2T_TRY(a->tmpProj.alloc(pb, "residual buffer"));
     }
     if (!a->tmpProj.p) B2T_TRY(a->tmpProj.alloc(pb, "residual buffer"));
-    B2T_TRY(a->partial.alloc(sizeof(double) * DOT_MAX_BLOCKS, "dot partials"));
-    B2T_TRY(a->scalars.alloc(sizeof(double) * 8, "CGLS scalars"));
+    const SegTable *tv = a->op->segments(true), *tp = a->op->segments(false);
+    size_t nparts = DOT_MAX_BLOCKS;
+    if (tv) {
+        a->nseg = tv->nseg;
+        nparts = std::max<size_t>(nparts, (size_t)std::max(tv->nchunks, tp->nchunks));
+    }
+    B2T_TRY(a->partial.alloc(sizeof(double) * nparts, "dot partials"));
+    B2T_TRY(a->scalars.alloc(sizeof(double) * 8 * a->nseg, "CGLS scalars"));
     *out = reinterpret_cast<b2t_algo *>(a.release());
     return B2T_OK;
 }
@@ -375,9 +497,6 @@ b2t_status algo_create2d_impl(int32_t type, const b2t_geom2d *geom, uint32_t det
 b2t_status algo_create_batch2d_impl(int32_t type, Batch2D *batch, const b2t_algo_options *opt, b2t_algo **out)
 {
     if (!batch) return fail(B2T_ERR_INVALID_ARG, "b2t_algo_create_batch2d: null batch");
-    if (type != B2T_ALGO_SIRT)
-        return fail(B2T_ERR_UNSUPPORTED, "b2t_algo_create_batch2d: only SIRT runs on a batch (CGLS needs per-problem "
-                                         "step sizes)");
     if (opt && (opt->vol_mask || opt->sino_mask || opt->min_mask || opt->max_mask))
         return fail(B2T_ERR_UNSUPPORTED, "b2t_algo_create_batch2d: masks are not supported on a batch");
     return algo_create(type, new OpBatch2D(batch), opt, out);
@@ -460,10 +579,12 @@ b2t_status algo_residual_impl(b2t_algo *h, const float *sino, const float *vol, 
     B2T_TRY(a->op->fp(xv, tp, 1.0f, B2T_MODE_SET, s));
     residual_weight_kernel<<<ew_blocks(a->np()), EW_THREADS, 0, s>>>(tp, sino, nullptr, a->np());
     B2T_TRY(a->ew(cudaGetLastError(), "residual"));
-    B2T_TRY(a->dot_sq(tp, a->np(), 4, s));
+    // one norm over the whole buffer (every problem of a batch), in the last
+    // scalar slot
+    double *slot = a->scalars.as<double>() + 7 * a->nseg;
+    B2T_TRY(dot_launch(tp, tp, a->np(), B2T_F32, a->partial.as<double>(), dot_num_blocks(a->np()), slot, s));
     double v = 0.0;
-    B2T_CUDA_TRY(cudaMemcpyAsync(&v, a->scalars.as<double>() + 4, sizeof(double), cudaMemcpyDeviceToHost, s),
-                 "residual readback");
+    B2T_CUDA_TRY(cudaMemcpyAsync(&v, slot, sizeof(double), cudaMemcpyDeviceToHost, s), "residual readback");
     B2T_CUDA_TRY(cudaStreamSynchronize(s), "residual synchronize");
     *norm = std::sqrt(v);
     return B2T_OK;

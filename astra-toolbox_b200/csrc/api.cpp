@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 #include "algorithms.h"
@@ -17,6 +18,47 @@
 namespace b2t {
 
 static thread_local std::string g_last_error;
+
+constexpr int MAX_POOL_DEVICES = 64;
+static std::mutex g_pool_mutex;
+static cudaMemPool_t g_pools[MAX_POOL_DEVICES] = {};
+
+cudaMemPool_t scratch_pool(cudaError_t &err)
+{
+    int dev = 0;
+    err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return nullptr;
+    if (dev < 0 || dev >= MAX_POOL_DEVICES) {
+        err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        err = cudaMemPoolCreate(&pool, &props);
+        if (err != cudaSuccess) return nullptr;
+        uint64_t keep = UINT64_MAX;  // never hand freed blocks back on synchronisation
+        err = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (err != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return nullptr;
+        }
+        g_pools[dev] = pool;
+    }
+    return g_pools[dev];
+}
+
+void trim_scratch_pools()
+{
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    for (int d = 0; d < MAX_POOL_DEVICES; ++d)
+        if (g_pools[d]) cudaMemPoolTrimTo(g_pools[d], 0);
+}
 static std::atomic<unsigned long long> g_launches{0};
 
 void count_launches(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
@@ -221,6 +263,22 @@ b2t_status b2t_algo_create_batch2d(int32_t type, b2t_batch2d *batch, const b2t_a
 void b2t_batch2d_destroy(b2t_batch2d *batch)
 {
     delete reinterpret_cast<Batch2D *>(batch);
+}
+
+b2t_status b2t_autotune_fp3d(const b2t_geom3d *geom, const b2t_params3d *params, const void *vol, size_t vol_pitch,
+                             void *proj, size_t proj_pitch, int32_t dtype, void *stream, int32_t *vpc)
+{
+    clear_error();
+    return fp3d_autotune_impl(geom, params, vol, vol_pitch, proj, proj_pitch, dtype, static_cast<cudaStream_t>(stream),
+                              vpc);
+}
+
+b2t_status b2t_release_cached_memory(void)
+{
+    clear_error();
+    B2T_CUDA_TRY(cudaDeviceSynchronize(), "b2t_release_cached_memory synchronize");
+    trim_scratch_pools();
+    return B2T_OK;
 }
 
 b2t_status b2t_onchip_peak(int32_t which, double *gbs)

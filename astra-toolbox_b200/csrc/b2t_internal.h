@@ -44,6 +44,12 @@ inline bool dtype_valid(int32_t dtype)
     return dtype == B2T_F32 || dtype == B2T_F16 || dtype == B2T_BF16;
 }
 
+// The library's stream-ordered memory pool of the current device (created on
+// first use).  Freed scratch stays cached in it between calls, so repeated
+// calls do not map and unmap device memory; b2t_release_cached_memory trims it.
+cudaMemPool_t scratch_pool(cudaError_t &err);
+void trim_scratch_pools();
+
 // Stream-ordered scratch allocation that is freed (stream-ordered) when the
 // object goes out of scope.
 class Scratch {
@@ -57,7 +63,9 @@ public:
         release();
         stream_ = s;
         if (bytes == 0) bytes = 16;
-        cudaError_t e = cudaMallocAsync(&ptr_, bytes, s);
+        cudaError_t e = cudaSuccess;
+        cudaMemPool_t pool = scratch_pool(e);
+        if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&ptr_, bytes, pool, s);
         if (e != cudaSuccess) {
             ptr_ = nullptr;
             (void)cudaGetLastError();  // allocation failures are not sticky: clear them

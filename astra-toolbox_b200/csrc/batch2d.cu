@@ -213,6 +213,22 @@ b2t_status batch2d_create_impl(const b2t_problem2d *problems, int32_t n, Batch2D
     b->n_fp_items = (int)fpi.size();
     b->n_bp_items = (int)bpi.size();
 
+    // chunk tables of the packed buffers (per-problem reductions)
+    std::vector<SegChunk> vch, sch;
+    std::vector<int> vfirst(n + 1), sfirst(n + 1);
+    for (int i = 0; i < n; ++i) {
+        const BatchProb &P = b->probs[i];
+        const long long nvol = (long long)P.W * P.H, nsino = (long long)P.nang * P.ndet;
+        vfirst[i] = (int)vch.size();
+        for (long long o = 0; o < nvol; o += SEG_CHUNK)
+            vch.push_back({P.vol_off + o, (int)std::min<long long>(SEG_CHUNK, nvol - o), i});
+        sfirst[i] = (int)sch.size();
+        for (long long o = 0; o < nsino; o += SEG_CHUNK)
+            sch.push_back({P.sino_off + o, (int)std::min<long long>(SEG_CHUNK, nsino - o), i});
+    }
+    vfirst[n] = (int)vch.size();
+    sfirst[n] = (int)sch.size();
+
     // one device allocation for every table
     auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t o_probs = 0;
@@ -222,7 +238,11 @@ b2t_status batch2d_create_impl(const b2t_problem2d *problems, int32_t n, Batch2D
     const size_t o_fpi = align(o_bp + sizeof(BPView2D) * view_off);
     const size_t o_bpi = align(o_fpi + sizeof(int4) * fpi.size());
     const size_t o_cnt = align(o_bpi + sizeof(int4) * bpi.size());
-    const size_t total = o_cnt + 256;
+    const size_t o_vch = align(o_cnt + 256);
+    const size_t o_sch = align(o_vch + sizeof(SegChunk) * vch.size());
+    const size_t o_vfi = align(o_sch + sizeof(SegChunk) * sch.size());
+    const size_t o_sfi = align(o_vfi + sizeof(int) * (n + 1));
+    const size_t total = o_sfi + sizeof(int) * (n + 1);
     cudaError_t e = cudaMalloc(&b->mem, total);
     if (e != cudaSuccess) {
         b->mem = nullptr;
@@ -237,6 +257,10 @@ b2t_status batch2d_create_impl(const b2t_problem2d *problems, int32_t n, Batch2D
     b->d_fp_items = reinterpret_cast<int4 *>(base + o_fpi);
     b->d_bp_items = reinterpret_cast<int4 *>(base + o_bpi);
     b->d_counters = reinterpret_cast<int *>(base + o_cnt);
+    b->vol_segs = SegTable{reinterpret_cast<SegChunk *>(base + o_vch), reinterpret_cast<int *>(base + o_vfi),
+                           (int)vch.size(), n};
+    b->sino_segs = SegTable{reinterpret_cast<SegChunk *>(base + o_sch), reinterpret_cast<int *>(base + o_sfi),
+                            (int)sch.size(), n};
     std::vector<int4> fp_items(fpi.size()), bp_items(bpi.size());
     for (size_t k = 0; k < fpi.size(); ++k) fp_items[k] = fpi[k].item;
     for (size_t k = 0; k < bpi.size(); ++k) bp_items[k] = bpi[k].item;
@@ -249,7 +273,11 @@ b2t_status batch2d_create_impl(const b2t_problem2d *problems, int32_t n, Batch2D
                {b->d_fan, fan.data(), sizeof(b2t_view2d) * view_off},
                {b->d_bp, bp.data(), sizeof(BPView2D) * view_off},
                {b->d_fp_items, fp_items.data(), sizeof(int4) * fp_items.size()},
-               {b->d_bp_items, bp_items.data(), sizeof(int4) * bp_items.size()}};
+               {b->d_bp_items, bp_items.data(), sizeof(int4) * bp_items.size()},
+               {base + o_vch, vch.data(), sizeof(SegChunk) * vch.size()},
+               {base + o_sch, sch.data(), sizeof(SegChunk) * sch.size()},
+               {base + o_vfi, vfirst.data(), sizeof(int) * (n + 1)},
+               {base + o_sfi, sfirst.data(), sizeof(int) * (n + 1)}};
     for (const Up &u : ups) {
         if (u.bytes == 0) continue;
         e = cudaMemcpy(u.dst, u.src, u.bytes, cudaMemcpyHostToDevice);

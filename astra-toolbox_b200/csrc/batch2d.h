@@ -18,6 +18,23 @@ struct BatchProb {
     long long vol_off, sino_off;  // element offsets in the packed buffers
 };
 
+// Chunks of the packed buffers, each inside one problem's segment, for the
+// per-problem reductions and updates of CGLS on a batch: chunk c covers
+// elements [begin, begin + len) of segment (problem) seg; the chunks of
+// segment p are first[p] .. first[p + 1] - 1, in order.
+struct SegChunk {
+    long long begin;
+    int len;
+    int seg;
+};
+struct SegTable {
+    const SegChunk *chunks = nullptr;  // device
+    const int *first = nullptr;        // device, nseg + 1 entries
+    int nchunks = 0;
+    int nseg = 0;
+};
+constexpr int SEG_CHUNK = 32768;
+
 // A batch: problems, their packed layout, per-view constants on the device
 // and the work items of the persistent kernels, ordered by decreasing cost.
 struct Batch2D {
@@ -35,6 +52,7 @@ struct Batch2D {
     int4 *d_fp_items = nullptr;    // (problem, view, first detector, 0)
     int4 *d_bp_items = nullptr;    // (problem, tile x, tile y, 0)
     int *d_counters = nullptr;     // work counters of the FP and BP launches
+    SegTable vol_segs, sino_segs;  // chunk tables of the packed buffers
     ~Batch2D();
 };
 

@@ -110,10 +110,20 @@ __global__ void __launch_bounds__(SPLIT_THREADS) fdk_split_kernel(
     const T *src, long long src_pitch, int nu, int na, int nv, FDKWeights P, const float *__restrict__ rel_angles,
     __nv_bfloat16 *out, int khp, long long M, T *dst, long long dst_row, long long dst_v)
 {
-    extern __shared__ float xs[];  // SPLIT_ROWS rows of (nu + 2 * RAMP_TC_BAND + 2) floats
+    extern __shared__ float xs[];  // SPLIT_ROWS rows of skewed(PADL + nu + PADR) floats
     __shared__ float taps[(RAMP_TC_BAND + 1) / 2];
-    const int W = nu + 2 * RAMP_TC_BAND + 2;
-    const int PADL = RAMP_TC_BAND + 1;
+    // the sliding window below reads x[n0 - BAND - 2 .. n0 + BAND + 9] for
+    // output groups n0 <= nu - 1 (its last shift fetches one tap ahead)
+    const int PADL = RAMP_TC_BAND + 3, PADR = RAMP_TC_BAND + 9;
+    const int W = PADL + nu + PADR;
+    // Skewed row layout: logical column i sits at k + k / 8 with k = i + PADL,
+    // so lanes whose windows start 8 columns apart hit banks 9 apart
+    // (conflict-free) instead of 8 apart (4 banks, 8-way conflicts).
+    const int WS = W + W / 8 + 1;
+    auto at = [PADL](const float *row, int i) -> float {
+        const int k = i + PADL;
+        return row[k + (k >> 3)];
+    };
     const long long m0 = (long long)blockIdx.x * SPLIT_ROWS;
     const int nr = (int)min((long long)SPLIT_ROWS, M - m0);
     for (int t = threadIdx.x; t < (RAMP_TC_BAND + 1) / 2; t += SPLIT_THREADS) {
@@ -127,33 +137,54 @@ __global__ void __launch_bounds__(SPLIT_THREADS) fdk_split_kernel(
         const float fV = ((float)v - 0.5f * (float)nv + 0.5f) * P.det_vsize + P.zshift;
         const float beta = P.short_scan ? rel_angles[a] : 0.0f;
         const T *row = src + m * src_pitch;
-        float *x = xs + r * W;
+        float *x = xs + r * WS;
         for (int j = threadIdx.x; j < W; j += SPLIT_THREADS) {
             const int u = j - PADL;
-            x[j] = (u >= 0 && u < nu) ? ldf(row + u) * fdk_weight(P, u, nu, fV, beta) : 0.0f;
+            x[j + (j >> 3)] = (u >= 0 && u < nu) ? ldf(row + u) * fdk_weight(P, u, nu, fV, beta) : 0.0f;
         }
     }
     __syncthreads();
     const long long term = M * khp;
     for (int r = 0; r < nr; ++r) {
         const long long m = m0 + r;
-        const float *x = xs + r * W + PADL;  // x[-PADL .. nu + PADL)
+        const float *x = xs + r * WS;  // logical columns -PADL .. nu + PADR - 1 through at()
         const int v = (int)(m / na);
         T *orow = dst + (long long)v * dst_v + (m - (long long)v * na) * dst_row;
-        for (int n = threadIdx.x; n < nu; n += SPLIT_THREADS) {
-            float acc = 0.5f * x[n];
-#pragma unroll 8
-            for (int t = 0; t < (RAMP_TC_BAND + 1) / 2; ++t) {
-                const int d = 2 * t + 1;
-                acc = fmaf(taps[t], x[n - d] + x[n + d], acc);
+        // 8 consecutive outputs per thread; L[j] = x[n0 + j - d], R[j] = x[n0 + j + d],
+        // slid by two columns per odd tap d
+        for (int g = threadIdx.x; g < (nu + 7) / 8; g += SPLIT_THREADS) {
+            const int n0 = 8 * g;
+            float acc[8], Lw[8], Rw[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                acc[j] = 0.5f * at(x, n0 + j);
+                Lw[j] = at(x, n0 + j - 1);
+                Rw[j] = at(x, n0 + j + 1);
             }
-            orow[n] = stf<T>(acc);
+#pragma unroll 4
+            for (int t = 0; t < (RAMP_TC_BAND + 1) / 2; ++t) {
+                const float c = taps[t];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[j] = fmaf(c, Lw[j] + Rw[j], acc[j]);
+                const int d = 2 * t + 1;
+#pragma unroll
+                for (int j = 7; j >= 2; --j) Lw[j] = Lw[j - 2];
+                Lw[0] = at(x, n0 - d - 2);
+                Lw[1] = at(x, n0 - d - 1);
+#pragma unroll
+                for (int j = 0; j < 6; ++j) Rw[j] = Rw[j + 2];
+                Rw[6] = at(x, n0 + d + 8);
+                Rw[7] = at(x, n0 + d + 9);
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (n0 + j < nu) orow[n0 + j] = stf<T>(acc[j]);
         }
         __nv_bfloat16 *e = out + m * khp;
         for (int j = threadIdx.x; j < khp; j += SPLIT_THREADS) {
             const int u0 = 2 * j, u1 = 2 * j + 1;
-            const float x0 = (u0 < nu) ? x[u0] : 0.0f;
-            const float x1 = (u1 < nu) ? x[u1] : 0.0f;
+            const float x0 = (u0 < nu) ? at(x, u0) : 0.0f;
+            const float x1 = (u1 < nu) ? at(x, u1) : 0.0f;
             __nv_bfloat16 t0, t1, t2;
             split3(x0, t0, t1, t2);
             e[j] = t0;
@@ -388,7 +419,8 @@ static b2t_status run_filter(const b2t_dims3d &d, const FDKWeights &P, const std
         if (st == B2T_OK) {
             __nv_bfloat16 *a = sa.as<__nv_bfloat16>();
             const long long blocks = (M + SPLIT_ROWS - 1) / SPLIT_ROWS;
-            const size_t smem = sizeof(float) * SPLIT_ROWS * ((size_t)d.det_u + 2 * RAMP_TC_BAND + 2);
+            const size_t wrow = (size_t)d.det_u + 2 * RAMP_TC_BAND + 12;  // PADL + nu + PADR
+            const size_t smem = sizeof(float) * SPLIT_ROWS * (wrow + wrow / 8 + 1);
             if (blocks > 0x7fffffffLL || smem > 200 * 1024)
                 return fail(B2T_ERR_UNSUPPORTED, "ramp filter: %lld rows of %u columns are too many", M, d.det_u);
             if (dtype == B2T_F32)

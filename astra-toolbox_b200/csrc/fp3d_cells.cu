@@ -24,7 +24,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "b2t_internal.h"
@@ -45,6 +49,11 @@ template <typename T> __device__ __forceinline__ T vstore(float v);
 template <> __device__ __forceinline__ float vstore<float>(float v) { return v; }
 template <> __device__ __forceinline__ __half vstore<__half>(float v) { return __float2half_rn(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 vstore<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+template <typename T> struct CellDtype;
+template <> struct CellDtype<float> { static constexpr int32_t value = B2T_F32; };
+template <> struct CellDtype<__half> { static constexpr int32_t value = B2T_F16; };
+template <> struct CellDtype<__nv_bfloat16> { static constexpr int32_t value = B2T_BF16; };
 
 // Cell storage per type: 16 bytes (float coefficients) or 8 bytes (corners).
 template <typename T> struct CellT;
@@ -260,12 +269,39 @@ __global__ void __launch_bounds__(32 * VROWS * VPC, 2048 / (32 * VROWS * VPC)) f
     *out = vstore<T>(r);
 }
 
-// Views per CTA of the cell kernel: B2T_FP_VPC (1, 2, 4 or 8) or 4.
-static int cells_vpc()
+// Launch shape of the cell forward projector: views per CTA.
+struct CellShape {
+    int vpc;
+};
+
+// Shapes chosen by b2t_autotune_fp3d, per problem class, for this process.
+static std::mutex g_shape_mutex;
+static std::map<std::string, CellShape> g_shapes;
+// Set by the autotuner while it times one candidate on this thread.
+static thread_local const CellShape *t_shape_override = nullptr;
+
+static std::string shape_key(const b2t_geom3d *g, const b2t_params3d *p, int32_t dtype)
 {
-    const char *e = std::getenv("B2T_FP_VPC");
-    const int v = e ? std::atoi(e) : 4;
-    return (v == 1 || v == 2 || v == 8) ? v : 4;
+    const b2t_dims3d &d = g->dims;
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "%d/%d/%u/%u/%u/%u/%u/%u/%u", g->kind, dtype, d.vol_x, d.vol_y, d.vol_z, d.angles,
+                  d.det_u, d.det_v, p->det_supersample);
+    return buf;
+}
+
+// The autotuner's candidate while it runs; else B2T_FP_VPC (1, 2, 4 or 8)
+// from the environment; else the tuned shape of this problem class; else 4
+// views per CTA.
+static CellShape choose_shape(const std::string &key)
+{
+    if (t_shape_override) return *t_shape_override;
+    if (const char *e = std::getenv("B2T_FP_VPC")) {
+        const int v = std::atoi(e);
+        return CellShape{(v == 1 || v == 2 || v == 8) ? v : 4};
+    }
+    std::lock_guard<std::mutex> lock(g_shape_mutex);
+    auto it = g_shapes.find(key);
+    return it != g_shapes.end() ? it->second : CellShape{4};
 }
 
 template <typename T, int VPC, int VROWS>
@@ -279,9 +315,10 @@ static b2t_status launch_cells_shape(const FPLaunch &P, int nviews, const b2t_di
 }
 
 template <typename T>
-static b2t_status launch_cells(const FPLaunch &P, int nviews, const b2t_dims3d &d, cudaStream_t s)
+static b2t_status launch_cells(const FPLaunch &P, int nviews, const b2t_dims3d &d, const CellShape &shape,
+                               cudaStream_t s)
 {
-    switch (cells_vpc()) {
+    switch (shape.vpc) {
     case 1: return launch_cells_shape<T, 1, 8>(P, nviews, d, s);
     case 2: return launch_cells_shape<T, 2, 4>(P, nviews, d, s);
     case 8: return launch_cells_shape<T, 8, 2>(P, nviews, d, s);
@@ -323,6 +360,7 @@ b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
         }
         base[dir] = cs[dir].as<C>() + 2 * st2[dir] + 2;
     }
+    const CellShape shape = choose_shape(shape_key(g, p, CellDtype<T>::value));
     FPLaunch *Lp = new FPLaunch;
     FPLaunch &P = *Lp;
     const bool force_noncube = p->det_supersample > 1;
@@ -354,7 +392,7 @@ b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
                 fp_view_coeffs(g->kind, g->views[a], d, dir, P.views[i]);
                 P.views[i].a = a;
             }
-            st = launch_cells<T>(P, (int)cn, d, s);
+            st = launch_cells<T>(P, (int)cn, d, shape, s);
             if (st != B2T_OK) break;
         }
     }
@@ -363,6 +401,59 @@ b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
 }
 
 }  // namespace
+
+b2t_status fp3d_autotune_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch,
+                              void *proj, size_t proj_pitch, int32_t dtype, cudaStream_t s, int32_t *vpc_out)
+{
+    B2T_TRY(validate3d(g, "b2t_autotune_fp3d"));
+    if (!p || !vol || !proj) return fail(B2T_ERR_INVALID_ARG, "b2t_autotune_fp3d: null argument");
+    if (!dtype_valid(dtype)) return fail(B2T_ERR_INVALID_ARG, "b2t_autotune_fp3d: bad dtype %d", dtype);
+    static const CellShape cands[] = {{1}, {2}, {4}, {8}};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    B2T_CUDA_TRY(cudaEventCreate(&e0), "autotune event");
+    cudaError_t ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_fail(ce, "autotune event");
+    }
+    CellShape best{4};
+    float best_ms = 1e30f;
+    b2t_status st = B2T_OK;
+    for (const CellShape &c : cands) {
+        t_shape_override = &c;
+        // one untimed run, then the best of two timed runs of the whole call
+        st = fp3d_impl(g, p, vol, vol_pitch, proj, proj_pitch, dtype, B2T_MODE_SET, s);
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2 && st == B2T_OK; ++rep) {
+            cudaEventRecord(e0, s);
+            st = fp3d_impl(g, p, vol, vol_pitch, proj, proj_pitch, dtype, B2T_MODE_SET, s);
+            cudaEventRecord(e1, s);
+            ce = cudaEventSynchronize(e1);
+            if (ce != cudaSuccess) {
+                st = cuda_fail(ce, "autotune timing");
+                break;
+            }
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms = std::min(ms, t);
+        }
+        t_shape_override = nullptr;
+        if (st != B2T_OK) break;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != B2T_OK) return st;
+    {
+        std::lock_guard<std::mutex> lock(g_shape_mutex);
+        g_shapes[shape_key(g, p, dtype)] = best;
+    }
+    if (vpc_out) *vpc_out = best.vpc;
+    return B2T_OK;
+}
 
 b2t_status fp3d_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch, void *proj,
                       size_t proj_pitch, int32_t dtype, int32_t mode, const std::vector<int> &dirs, cudaStream_t s)

@@ -282,13 +282,25 @@ __global__ void __launch_bounds__(RT_THREADS, 1) ramp_tc_kernel(const __grid_con
                     stg[lane * RT_EPI_STRIDE + 2 * j + 1] = __uint_as_float(ro[j]);
                 }
                 __syncwarp();
-                // row r of this warp's 32 rows: 32 consecutive outputs, one per lane
+                // row r of this warp's 32 rows: 32 consecutive outputs, one per
+                // lane.  All 32 near-part loads are issued before any store, so
+                // they are in flight together.
                 const int n = 2 * i0 + lane;
+                const bool col_ok = n < L.nu;
+                float near[32];
+#pragma unroll
                 for (int r = 0; r < 32; ++r) {
                     T *rp = reinterpret_cast<T *>(
                         __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), r));
-                    const long long mr = (long long)mt * RT_BM + q * 32 + r;
-                    if (mr < L.M && n < L.nu) rp[n] = to_out<T>(from_out(rp[n]) + stg[r * RT_EPI_STRIDE + lane]);
+                    const bool ok = col_ok && (long long)mt * RT_BM + q * 32 + r < L.M;
+                    near[r] = ok ? from_out(rp[n]) : 0.0f;
+                }
+#pragma unroll
+                for (int r = 0; r < 32; ++r) {
+                    T *rp = reinterpret_cast<T *>(
+                        __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), r));
+                    const bool ok = col_ok && (long long)mt * RT_BM + q * 32 + r < L.M;
+                    if (ok) rp[n] = to_out<T>(near[r] + stg[r * RT_EPI_STRIDE + lane]);
                 }
                 __syncwarp();
             }

@@ -85,6 +85,19 @@ class Projector3D:
                       proj.data_ptr(), 0, _DTYPES[vol.dtype], mode, stream_handle(vol.device))
         return proj
 
+    def autotune(self, vol, proj):
+        """Time the forward projector's launch shapes on these buffers and keep
+        the fastest for this problem class (b2t_autotune_fp3d); proj is
+        overwritten with A vol.  Returns the chosen views per CTA."""
+        _check_tensor(vol, self.vol_shape, "volume")
+        _check_tensor(proj, self.proj_shape, "projection data", vol.device)
+        p = self.params()
+        vpc = ctypes.c_int32(0)
+        with torch.cuda.device(vol.device):
+            _lib.call("b2t_autotune_fp3d", ctypes.byref(self.geom.c), ctypes.byref(p), vol.data_ptr(), 0,
+                      proj.data_ptr(), 0, _DTYPES[vol.dtype], stream_handle(vol.device), ctypes.byref(vpc))
+        return vpc.value
+
     def bp(self, proj, vol, mode=_lib.MODE_SET, output_scale=1.0, kernel=None):
         """vol (=|+=) B proj on torch tensors (B = ASTRA's BP, or A^T for matched_bp)."""
         _check_tensor(vol, self.vol_shape, "volume")

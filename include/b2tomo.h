@@ -63,6 +63,13 @@ b2t_status b2t_set_device(int32_t device);
  * output is incomplete).  Synchronises the device.  The reference has no
  * device-side waits and no counterpart. */
 b2t_status b2t_device_errors(uint32_t *flags);
+/* Scratch buffers (padded copies, cell copies, filter operands) come from a
+ * stream-ordered memory pool of the library, one per device, that keeps freed
+ * blocks cached so repeated calls do not map device memory again.  This
+ * synchronises the current device and returns the cached blocks of every
+ * device to the driver.  The reference allocates and frees per call with
+ * cudaMalloc / cudaFree (cuda/3d/mem3d.cu:82-166, cuda/3d/fdk.cu:341). */
+b2t_status b2t_release_cached_memory(void);
 
 /* ---------------------------------------------------------------------- */
 /* enumerations                                                            */
@@ -393,17 +400,31 @@ b2t_status b2t_batch2d_fp(b2t_batch2d *batch, const float *vols, float *sinos, i
 /* vols (=|+=) A^T-style backprojection of sinos for every problem (the
  * reference's unmatched BP), in one persistent launch. */
 b2t_status b2t_batch2d_bp(b2t_batch2d *batch, const float *sinos, float *vols, int32_t mode, void *stream);
-/* SIRT_CUDA on every problem of the batch at once (src/CudaSirtAlgorithm.cpp):
- * run with b2t_algo_run / b2t_algo_residual_norm on the packed buffers.  Only
- * B2T_ALGO_SIRT; options as for b2t_algo_create2d without masks.  The batch
- * must outlive the algorithm. */
+/* SIRT_CUDA or CGLS_CUDA on every problem of the batch at once
+ * (src/CudaSirtAlgorithm.cpp, src/CudaCglsAlgorithm.cpp): run with
+ * b2t_algo_run / b2t_algo_residual_norm on the packed buffers.  Each problem
+ * keeps its own CGLS step sizes (per-problem FP64 inner products), so the
+ * iterates equal per-problem runs; the residual norm is over the whole batch.
+ * Options as for b2t_algo_create2d, without masks.  The batch must outlive
+ * the algorithm. */
 b2t_status b2t_algo_create_batch2d(int32_t type, b2t_batch2d *batch, const b2t_algo_options *options,
                                    b2t_algo **out);
 void b2t_batch2d_destroy(b2t_batch2d *batch);
 
 /* ---------------------------------------------------------------------- */
-/* measurement                                                             */
+/* measurement and tuning                                                  */
 /* ---------------------------------------------------------------------- */
+
+/* Choose the launch shape of the 3D forward projector for this problem class
+ * (geometry kind, storage type, volume and detector sizes, view count,
+ * supersampling) by timing every candidate on the caller's buffers: 1, 2, 4
+ * or 8 consecutive views per CTA.  The choice is kept for the process and
+ * used by every later b2t_fp3d of the same class (B2T_FP_VPC in the
+ * environment still overrides it).  Overwrites proj with A vol; synchronises
+ * the stream.  No counterpart in the reference, whose launch shapes are
+ * compile-time constants (cuda/3d/cone_fp.cu:47-53).  vpc may be NULL. */
+b2t_status b2t_autotune_fp3d(const b2t_geom3d *geom, const b2t_params3d *params, const void *vol, size_t vol_pitch,
+                             void *proj, size_t proj_pitch, int32_t dtype, void *stream, int32_t *vpc);
 
 /* On-chip load bandwidth of the current GPU in GB/s (no counterpart in the
  * reference): which = 0 streams 16-byte shared-memory loads, which = 1

@@ -306,3 +306,24 @@ def test_cell_fp_matches_padded_fp(astra, idx, dtype, monkeypatch):
     monkeypatch.delenv("B2T_SIMPLE_FP")
     tol = {"float32": 2e-6, "float16": 2e-3, "bfloat16": 1e-2}[dtype]
     assert rel_l2(a.float().cpu().numpy(), b.float().cpu().numpy()) < tol, name
+
+
+@pytest.mark.parametrize("idx", [0, 4])
+def test_autotune_fp3d_keeps_results(astra, orc, idx):
+    """The autotuner times the views-per-CTA variants and keeps the fastest;
+    every variant computes the same projections."""
+    name, vg, pg = _all_geoms(astra)[idx]
+    pr = _proj(astra, vg, pg)
+    vol = torch.from_numpy(_phantom(pr.vol_shape, idx + 40)).cuda()
+    a = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(vol, a)
+    b = torch.zeros(pr.proj_shape, device='cuda')
+    vpc = pr.autotune(vol, b)
+    assert vpc in (1, 2, 4, 8)
+    assert rel_l2(b.cpu().numpy(), a.cpu().numpy()) < 1e-6, name
+    c = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(vol, c)  # runs with the tuned shape
+    assert rel_l2(c.cpu().numpy(), a.cpu().numpy()) < 1e-6, name
+    ref = orc.fp3d(_oracle_kind(pr), pr.geom.views_array(), vol.cpu().numpy(), pr.proj_shape[2], pr.proj_shape[0],
+                   pr.geom.vol_scale)
+    assert rel_l2(c.cpu().numpy(), ref) < 1e-5, name
