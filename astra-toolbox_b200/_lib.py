@@ -23,6 +23,16 @@ F32, F16, BF16 = 0, 1, 2
 GEOM_PAR3D, GEOM_CONE, GEOM_PAR2D, GEOM_FAN2D = 1, 2, 3, 4
 KER_DEFAULT, KER_SUM_SQUARE_WEIGHTS, KER_FDK_WEIGHTING, KER_2D_WEIGHTING, KER_MATCHED_BP = 0, 1, 2, 3, 4
 FILTER_NONE, FILTER_RAMLAK = 0, 1
+# E_FBPFILTER names (src/Filters.cpp:508-532) -> codes, in the reference's order
+FILTER_NAMES = ['none', 'ram-lak', 'shepp-logan', 'cosine', 'hamming', 'hann', 'tukey', 'lanczos', 'triangular',
+                'gaussian', 'barlett-hann', 'blackman', 'nuttall', 'blackman-harris', 'blackman-nuttall',
+                'flat-top', 'kaiser', 'parzen', 'projection', 'sinogram', 'rprojection', 'rsinogram']
+FILTER_PROJECTION, FILTER_SINOGRAM, FILTER_RPROJECTION, FILTER_RSINOGRAM = 18, 19, 20, 21
+
+
+class FilterConfig(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("d", ctypes.c_float), ("parameter", ctypes.c_float),
+                ("custom", ctypes.c_void_p), ("custom_width", ctypes.c_uint32), ("custom_height", ctypes.c_uint32)]
 (OP_SET, OP_MUL_SCALAR, OP_MUL, OP_ADD_MUL, OP_ADD_SCALED, OP_SCALE_AND_ADD, OP_INVERT,
  OP_CLAMP_MIN, OP_CLAMP_MAX, OP_ADD) = range(10)
 
@@ -118,10 +128,11 @@ SIGNATURES = {
     "b2t_bp3d": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
     "b2t_fp2d": (_I32, [_P, _U32, _P, _SZ, _P, _SZ, _I32, _P]),
     "b2t_bp2d": (_I32, [_P, _U32, _I32, _P, _SZ, _P, _SZ, _I32, _P]),
-    "b2t_fdk": (_I32, [_P, _I32, _I32, _F, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
-    "b2t_fdk_weight_filter": (_I32, [_P, _I32, _I32, _P, _SZ, _I32, _P]),
-    "b2t_filter_rows": (_I32, [_P, _SZ, _U32, _SZ, _I32, _P]),
-    "b2t_fbp2d": (_I32, [_P, _I32, _I32, _P, _SZ, _P, _SZ, _I32, _P]),
+    "b2t_fdk": (_I32, [_P, _P, _I32, _F, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
+    "b2t_fdk_weight_filter": (_I32, [_P, _P, _I32, _P, _SZ, _I32, _P]),
+    "b2t_filter_rows": (_I32, [_P, _SZ, _U32, _SZ, _P, _P]),
+    "b2t_filter_taps": (_I32, [_P, _U32, _U32, _P, _P]),
+    "b2t_fbp2d": (_I32, [_P, _P, _I32, _P, _SZ, _P, _SZ, _I32, _P]),
     "b2t_algo_create3d": (_I32, [_I32, _P, _P, _P, _P]),
     "b2t_algo_create2d": (_I32, [_I32, _P, _U32, _U32, _P, _P]),
     "b2t_algo_run": (_I32, [_P, _P, _P, _I32, _I32, _P]),

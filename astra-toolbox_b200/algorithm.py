@@ -23,6 +23,25 @@ def _opt(cfg):
     return dict(cfg.get('option', {}) or {})
 
 
+def _filter_from_cfg(cfg, opt):
+    """SFilterConfig from an algorithm config (getFilterConfigForAlgorithm,
+    src/Filters.cpp:548-657): FilterType, FilterD, FilterParameter and, for
+    the custom types, FilterSinogramId (a 2D sinogram data object), as
+    options or as top-level keys."""
+    def get(key, default=None):
+        return opt.get(key, cfg.get(key, default))
+    ftype = get('FilterType', 'ram-lak')
+    code = _P.filter_code(ftype)
+    custom = None
+    if code >= _lib.FILTER_PROJECTION:
+        fid = get('FilterSinogramId')
+        if fid is None:
+            raise AstraError(1, "FilterType %r needs FilterSinogramId" % (ftype,))
+        custom = _d.lookup(fid, _d.DataObject).tensor.detach().cpu().numpy()
+    return _P.FilterSpec(code, d=float(get('FilterD', 1.0)), parameter=float(get('FilterParameter', -1.0)),
+                         custom=custom)
+
+
 def _constraints(o):
     use_min = 'MinConstraint' in o or bool(o.get('UseMinConstraint', False))
     vmin = float(o.get('MinConstraint', o.get('MinConstraintValue', 0.0)))
@@ -93,7 +112,7 @@ class _FDK(_Algorithm):
         if self.pr.geom.kind != _lib.GEOM_CONE:
             raise AstraError(2, "FDK_CUDA needs a cone or cone_vec geometry")
         self.short = bool(self.opt.get('ShortScan', False))
-        self.filter = self.opt.get('FilterType', 'ram-lak')
+        self.filter = _filter_from_cfg(cfg, self.opt)
 
     def run(self, iterations=1):
         _P.fdk(self.pr, self.proj.tensor, self.vol.tensor, short_scan=self.short, filter_type=self.filter)
@@ -161,7 +180,7 @@ class _FBP2D(_Algorithm):
         self.proj = _d.lookup(cfg['ProjectionDataId'], _d.DataObject)
         self.pr = _P.Projector2D(self.proj.geometry, self.vol.geometry, self._projector_options())
         self.short = bool(self.opt.get('ShortScan', False))
-        self.filter = self.opt.get('FilterType', 'ram-lak')
+        self.filter = _filter_from_cfg(cfg, self.opt)
 
     def run(self, iterations=1):
         _P.fbp2d(self.pr, self.proj.tensor, self.vol.tensor, short_scan=self.short, filter_type=self.filter)

@@ -1,6 +1,7 @@
 // extern "C" entry points of libb2tomo and the per-thread error state.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -12,6 +13,7 @@
 #include "batch2d.h"
 #include "b2t_internal.h"
 #include "fdk.h"
+#include "filters.h"
 #include "proj2d.h"
 #include "proj3d.h"
 
@@ -140,7 +142,7 @@ b2t_status b2t_bp2d(const b2t_geom2d *geom, uint32_t pixel_supersample, int32_t 
                      static_cast<cudaStream_t>(stream));
 }
 
-b2t_status b2t_fdk(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, float output_scale, const void *proj,
+b2t_status b2t_fdk(const b2t_geom3d *geom, const b2t_filter_config *filter, int32_t short_scan, float output_scale, const void *proj,
                    size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, void *stream)
 {
     clear_error();
@@ -148,20 +150,21 @@ b2t_status b2t_fdk(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, f
                     static_cast<cudaStream_t>(stream));
 }
 
-b2t_status b2t_fdk_weight_filter(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, void *proj,
+b2t_status b2t_fdk_weight_filter(const b2t_geom3d *geom, const b2t_filter_config *filter, int32_t short_scan, void *proj,
                                  size_t proj_pitch, int32_t dtype, void *stream)
 {
     clear_error();
     return fdk_weight_filter_impl(geom, filter, short_scan, proj, proj_pitch, dtype, static_cast<cudaStream_t>(stream));
 }
 
-b2t_status b2t_filter_rows(float *data, size_t nrows, uint32_t n, size_t pitch, int32_t filter, void *stream)
+b2t_status b2t_filter_rows(float *data, size_t nrows, uint32_t n, size_t pitch, const b2t_filter_config *filter,
+                           void *stream)
 {
     clear_error();
     return filter_rows_impl(data, nrows, n, pitch, filter, static_cast<cudaStream_t>(stream));
 }
 
-b2t_status b2t_fbp2d(const b2t_geom2d *geom, int32_t filter, int32_t short_scan, const float *sino,
+b2t_status b2t_fbp2d(const b2t_geom2d *geom, const b2t_filter_config *filter, int32_t short_scan, const float *sino,
                      size_t sino_pitch, float *vol, size_t vol_pitch, int32_t mode, void *stream)
 {
     clear_error();
@@ -263,6 +266,23 @@ b2t_status b2t_algo_create_batch2d(int32_t type, b2t_batch2d *batch, const b2t_a
 void b2t_batch2d_destroy(b2t_batch2d *batch)
 {
     delete reinterpret_cast<Batch2D *>(batch);
+}
+
+b2t_status b2t_filter_taps(const b2t_filter_config *filter, uint32_t n, uint32_t n_views, float *out, size_t *count)
+{
+    clear_error();
+    if (!count) return fail(B2T_ERR_INVALID_ARG, "b2t_filter_taps: null count");
+    if (!filter || filter->type == B2T_FILTER_NONE)
+        return fail(B2T_ERR_INVALID_ARG, "b2t_filter_taps: a filter type with taps is needed");
+    FilterTaps ft;
+    B2T_TRY(filter_taps(filter, n, n_views, ft));
+    const size_t need = ft.g.size();
+    if (out) {
+        if (*count < need) return fail(B2T_ERR_INVALID_ARG, "b2t_filter_taps: output holds %zu of %zu taps", *count, need);
+        std::copy(ft.g.begin(), ft.g.end(), out);
+    }
+    *count = need;
+    return B2T_OK;
 }
 
 b2t_status b2t_autotune_fp3d(const b2t_geom3d *geom, const b2t_params3d *params, const void *vol, size_t vol_pitch,

@@ -28,6 +28,7 @@
 #include "fdk.h"
 #include "proj2d.h"
 #include "proj3d.h"
+#include "filters.h"
 #include "ramp_tc.h"
 
 namespace b2t {
@@ -154,14 +155,19 @@ __global__ void __launch_bounds__(SPLIT_THREADS) fdk_split_kernel(
         // slid by two columns per odd tap d
         for (int g = threadIdx.x; g < (nu + 7) / 8; g += SPLIT_THREADS) {
             const int n0 = 8 * g;
+            // column n0 + c of the skewed row is xb[sk(c)]: n0 is a multiple
+            // of 8, so with the taps fully unrolled every load is the base
+            // plus a compile-time offset
+            const float *xb = x + 9 * g;
+            auto sk = [PADL](int c) { return (PADL + c) + ((PADL + c) >> 3); };
             float acc[8], Lw[8], Rw[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                acc[j] = 0.5f * at(x, n0 + j);
-                Lw[j] = at(x, n0 + j - 1);
-                Rw[j] = at(x, n0 + j + 1);
+                acc[j] = 0.5f * xb[sk(j)];
+                Lw[j] = xb[sk(j - 1)];
+                Rw[j] = xb[sk(j + 1)];
             }
-#pragma unroll 4
+#pragma unroll
             for (int t = 0; t < (RAMP_TC_BAND + 1) / 2; ++t) {
                 const float c = taps[t];
 #pragma unroll
@@ -169,12 +175,12 @@ __global__ void __launch_bounds__(SPLIT_THREADS) fdk_split_kernel(
                 const int d = 2 * t + 1;
 #pragma unroll
                 for (int j = 7; j >= 2; --j) Lw[j] = Lw[j - 2];
-                Lw[0] = at(x, n0 - d - 2);
-                Lw[1] = at(x, n0 - d - 1);
+                Lw[0] = xb[sk(-d - 2)];
+                Lw[1] = xb[sk(-d - 1)];
 #pragma unroll
                 for (int j = 0; j < 6; ++j) Rw[j] = Rw[j + 2];
-                Rw[6] = at(x, n0 + d + 8);
-                Rw[7] = at(x, n0 + d + 9);
+                Rw[6] = xb[sk(d + 8)];
+                Rw[7] = xb[sk(d + 9)];
             }
 #pragma unroll
             for (int j = 0; j < 8; ++j)
@@ -287,6 +293,71 @@ __global__ void __launch_bounds__(FILT_THREADS) fdk_weight_filter_kernel(
     }
 }
 
+// Weighted rows filtered with arbitrary taps (any b2t_filter_config other
+// than the plain Ram-Lak): y[i] = sum_{d=-(nu-1)}^{nu-1} g[d] x[i - d], taps
+// of view a at taps + (per_view ? a : 0) * (2 nu - 1).  Rows staged in
+// shared memory as in fdk_weight_filter_kernel (zero-padded by nu + 16 on both
+// sides); each thread keeps 8 consecutive outputs and a sliding window of 8
+// inputs that moves one column per offset d.
+template <typename T>
+__global__ void __launch_bounds__(FILT_THREADS) fdk_weight_toeplitz_kernel(
+    const T *src, long long src_pitch, int nu, int na, int nv, int rows, FDKWeights P,
+    const float *__restrict__ rel_angles, const float *__restrict__ taps, int per_view, T *dst,
+    long long dst_row_stride, long long dst_v_stride)
+{
+    extern __shared__ float sm[];
+    const int PADW = nu + 16;
+    const int W3 = nu + 2 * PADW;
+    const long long m0 = (long long)blockIdx.x * rows;
+    const long long mtot = (long long)na * nv;
+    const int nr = (int)min((long long)rows, mtot - m0);
+    if (nr <= 0) return;
+    for (int r = 0; r < nr; ++r) {
+        const long long m = m0 + r;
+        const int v = (int)(m / na);
+        const int a = (int)(m - (long long)v * na);
+        const float fV = ((float)v - 0.5f * (float)nv + 0.5f) * P.det_vsize + P.zshift;
+        const float beta = P.short_scan ? rel_angles[a] : 0.0f;
+        const T *row = src + m * src_pitch;
+        float *xs = sm + (size_t)r * W3;
+        for (int j = threadIdx.x; j < W3; j += FILT_THREADS) {
+            const int u = j - PADW;
+            xs[j] = (u >= 0 && u < nu) ? ldf(row + u) * fdk_weight(P, u, nu, fV, beta) : 0.0f;
+        }
+    }
+    __syncthreads();
+    const int groups = (nu + FILT_OUT - 1) / FILT_OUT;
+    const int ntap = 2 * nu - 1;
+    for (int item = threadIdx.x; item < nr * groups; item += FILT_THREADS) {
+        const int r = item / groups;
+        const int i0 = (item - r * groups) * FILT_OUT;
+        const long long m = m0 + r;
+        const int v = (int)(m / na);
+        const int a = (int)(m - (long long)v * na);
+        const float *xs = sm + (size_t)r * W3 + PADW;  // xs[i] = x_i, i in [-nu-16, 2nu+16)
+        const float *g = taps + (per_view ? (long long)a * ntap : 0) + (nu - 1);  // g[d], |d| < nu
+        float acc[FILT_OUT], w[FILT_OUT];
+        // offsets from d = nu - 1 down to -(nu - 1): w[t] = x[i0 + t - d]
+#pragma unroll
+        for (int t = 0; t < FILT_OUT; ++t) {
+            acc[t] = 0.0f;
+            w[t] = xs[i0 + t - (nu - 1)];
+        }
+        for (int d = nu - 1; d >= -(nu - 1); --d) {
+            const float c = __ldg(g + d);
+#pragma unroll
+            for (int t = 0; t < FILT_OUT; ++t) acc[t] = fmaf(c, w[t], acc[t]);
+#pragma unroll
+            for (int t = 0; t < FILT_OUT - 1; ++t) w[t] = w[t + 1];
+            w[FILT_OUT - 1] = xs[i0 + FILT_OUT - d];
+        }
+        T *out = dst + (long long)v * dst_v_stride + (long long)a * dst_row_stride;
+#pragma unroll
+        for (int t = 0; t < FILT_OUT; ++t)
+            if (i0 + t < nu) out[i0 + t] = stf<T>(acc[t]);
+    }
+}
+
 }  // namespace
 
 // Weights of FDK_PreWeight (fdk.cu:168-264) for a circular orbit given by its
@@ -379,6 +450,40 @@ static b2t_status launch_filter(const void *src, size_t src_pitch, const b2t_dim
     return B2T_OK;
 }
 
+static b2t_status validate_filter(const b2t_filter_config *filter, const char *who)
+{
+    if (filter && (filter->type < B2T_FILTER_NONE || filter->type > B2T_FILTER_RSINOGRAM))
+        return fail(B2T_ERR_INVALID_ARG, "%s: unknown filter type %d", who, filter->type);
+    return B2T_OK;
+}
+
+template <typename T>
+static b2t_status launch_toeplitz(const void *src, size_t src_pitch, const b2t_dims3d &d, const FDKWeights &P,
+                                  const float *rel_dev, const float *taps, int per_view, void *dst, long long dst_row,
+                                  long long dst_v, cudaStream_t s)
+{
+    const int nu = d.det_u;
+    const size_t row_bytes = sizeof(float) * (3 * (size_t)nu + 32);
+    const size_t budget = 200 * 1024;
+    if (row_bytes > budget)
+        return fail(B2T_ERR_UNSUPPORTED, "filter: detector rows of %d pixels exceed shared memory", nu);
+    int rows = (int)(budget / row_bytes);
+    if (rows > 8) rows = 8;
+    const size_t smem = rows * row_bytes;
+    auto kern = fdk_weight_toeplitz_kernel<T>;
+    B2T_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                 "filter smem attribute");
+    const long long mtot = (long long)d.angles * d.det_v;
+    const long long blocks = (mtot + rows - 1) / rows;
+    if (blocks > 0x7fffffffLL) return fail(B2T_ERR_UNSUPPORTED, "filter: too many rows");
+    kern<<<(unsigned)blocks, FILT_THREADS, smem, s>>>(static_cast<const T *>(src), (long long)src_pitch, nu,
+                                                      d.angles, d.det_v, rows, P, rel_dev, taps, per_view,
+                                                      static_cast<T *>(dst), dst_row, dst_v);
+    count_launches(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "filter launch");
+    return B2T_OK;
+}
+
 template <typename T>
 static b2t_status launch_split(const void *src, size_t src_pitch, const b2t_dims3d &d, const FDKWeights &P,
                                const float *rel_dev, __nv_bfloat16 *a, int khp, long long M, void *dst,
@@ -395,7 +500,8 @@ static b2t_status launch_split(const void *src, size_t src_pitch, const b2t_dims
     return B2T_OK;
 }
 
-static b2t_status run_filter(const b2t_dims3d &d, const FDKWeights &P, const std::vector<float> &rel, int filter,
+static b2t_status run_filter(const b2t_dims3d &d, const FDKWeights &P, const std::vector<float> &rel,
+                             const b2t_filter_config *filter,
                              const void *src, size_t src_pitch, void *dst, long long dst_row, long long dst_v,
                              int32_t dtype, cudaStream_t s)
 {
@@ -407,7 +513,26 @@ static b2t_status run_filter(const b2t_dims3d &d, const FDKWeights &P, const std
                      "Parker angles upload");
         rel_dev = rs.as<float>();
     }
-    const int do_filter = (filter == B2T_FILTER_RAMLAK) ? 1 : 0;
+    const int ftype = filter ? filter->type : B2T_FILTER_RAMLAK;
+    if (ftype != B2T_FILTER_NONE && !filter_is_plain_ramlak(filter)) {
+        // any other filter: its exact spatial taps (filters.cpp), SIMT Toeplitz
+        FilterTaps ft;
+        B2T_TRY(filter_taps(filter, d.det_u, d.angles, ft));
+        Scratch ts;
+        B2T_TRY(ts.alloc(sizeof(float) * ft.g.size(), s, "filter taps"));
+        B2T_CUDA_TRY(cudaMemcpyAsync(ts.as<void>(), ft.g.data(), sizeof(float) * ft.g.size(), cudaMemcpyHostToDevice,
+                                     s),
+                     "filter taps upload");
+        const int per_view = ft.nsets > 1 ? 1 : 0;
+        if (dtype == B2T_F32)
+            return launch_toeplitz<float>(src, src_pitch, d, P, rel_dev, ts.as<float>(), per_view, dst, dst_row, dst_v, s);
+        if (dtype == B2T_F16)
+            return launch_toeplitz<__half>(src, src_pitch, d, P, rel_dev, ts.as<float>(), per_view, dst, dst_row, dst_v,
+                                           s);
+        return launch_toeplitz<__nv_bfloat16>(src, src_pitch, d, P, rel_dev, ts.as<float>(), per_view, dst, dst_row,
+                                              dst_v, s);
+    }
+    const int do_filter = (ftype == B2T_FILTER_RAMLAK) ? 1 : 0;
     // Ram-Lak on the tensor cores (ramp_tc.cu) when the shape allows it and
     // its scratch fits; otherwise the SIMT Toeplitz kernel below
     RampTCPlan plan;
@@ -443,11 +568,11 @@ static b2t_status run_filter(const b2t_dims3d &d, const FDKWeights &P, const std
     return launch_filter<__nv_bfloat16>(src, src_pitch, d, P, rel_dev, do_filter, dst, dst_row, dst_v, s);
 }
 
-b2t_status filter_rows_impl(float *data, size_t nrows, uint32_t n, size_t pitch, int32_t filter, cudaStream_t s)
+b2t_status filter_rows_impl(float *data, size_t nrows, uint32_t n, size_t pitch, const b2t_filter_config *filter,
+                            cudaStream_t s)
 {
     if (!data) return fail(B2T_ERR_INVALID_ARG, "b2t_filter_rows: null data");
-    if (filter != B2T_FILTER_NONE && filter != B2T_FILTER_RAMLAK)
-        return fail(B2T_ERR_UNSUPPORTED, "b2t_filter_rows: only the none and ram-lak filters are implemented");
+    B2T_TRY(validate_filter(filter, "b2t_filter_rows"));
     if (n == 0 || nrows == 0) return B2T_OK;
     if (nrows > 0xffffffffu) return fail(B2T_ERR_INVALID_ARG, "b2t_filter_rows: too many rows");
     if (pitch == 0) pitch = n;
@@ -485,13 +610,13 @@ static bool fan_parameters(const b2t_view2d &p, uint32_t ndet, float &angle, flo
 // FBP_CUDA (cuda/2d/fbp.cu:77-190): parallel = Ram-Lak filter + BP scaled by
 // (pi/2)/n_angles; fan = FDK pre-weighting of a one-row cone (+ Parker) +
 // filter + fan BP with the FBP weighting.  sino is not modified.
-b2t_status fbp2d_impl(const b2t_geom2d *g, int32_t filter, int32_t short_scan, const float *sino, size_t sino_pitch,
+b2t_status fbp2d_impl(const b2t_geom2d *g, const b2t_filter_config *filter, int32_t short_scan, const float *sino,
+                      size_t sino_pitch,
                       float *vol, size_t vol_pitch, int32_t mode, cudaStream_t s)
 {
     B2T_TRY(validate2d(g, "b2t_fbp2d"));
     if (!sino || !vol) return fail(B2T_ERR_INVALID_ARG, "b2t_fbp2d: null data pointer");
-    if (filter != B2T_FILTER_NONE && filter != B2T_FILTER_RAMLAK)
-        return fail(B2T_ERR_UNSUPPORTED, "b2t_fbp2d: only the none and ram-lak filters are implemented");
+    B2T_TRY(validate_filter(filter, "b2t_fbp2d"));
     const b2t_dims2d &dm = g->dims;
     if (sino_pitch == 0) sino_pitch = dm.dets;
     if (sino_pitch < dm.dets) return fail(B2T_ERR_INVALID_ARG, "b2t_fbp2d: pitch below row length");
@@ -520,7 +645,7 @@ b2t_status fbp2d_impl(const b2t_geom2d *g, int32_t filter, int32_t short_scan, c
     return bp2d_impl(&q, 1, g->kind == B2T_GEOM_FAN2D ? 1 : 0, tmp.as<float>(), dm.dets, vol, vol_pitch, mode, s);
 }
 
-static b2t_status run_weight_filter(const b2t_geom3d *g, int filter, int short_scan, const void *src,
+static b2t_status run_weight_filter(const b2t_geom3d *g, const b2t_filter_config *filter, int short_scan, const void *src,
                                     size_t src_pitch, void *dst, long long dst_row, long long dst_v, int32_t dtype,
                                     cudaStream_t s)
 {
@@ -530,17 +655,16 @@ static b2t_status run_weight_filter(const b2t_geom3d *g, int filter, int short_s
     return run_filter(g->dims, P, rel, filter, src, src_pitch, dst, dst_row, dst_v, dtype, s);
 }
 
-static b2t_status validate_fdk(const b2t_geom3d *g, int filter, int32_t dtype, const char *who)
+static b2t_status validate_fdk(const b2t_geom3d *g, const b2t_filter_config *filter, int32_t dtype, const char *who)
 {
     B2T_TRY(validate3d(g, who));
     if (g->kind != B2T_GEOM_CONE) return fail(B2T_ERR_UNSUPPORTED, "%s: FDK needs a cone geometry", who);
-    if (filter != B2T_FILTER_NONE && filter != B2T_FILTER_RAMLAK)
-        return fail(B2T_ERR_UNSUPPORTED, "%s: only the none and ram-lak filters are implemented", who);
+    B2T_TRY(validate_filter(filter, who));
     if (!dtype_valid(dtype)) return fail(B2T_ERR_INVALID_ARG, "%s: bad dtype %d", who, dtype);
     return B2T_OK;
 }
 
-b2t_status fdk_weight_filter_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, void *proj,
+b2t_status fdk_weight_filter_impl(const b2t_geom3d *g, const b2t_filter_config *filter, int32_t short_scan, void *proj,
                                   size_t proj_pitch, int32_t dtype, cudaStream_t s)
 {
     B2T_TRY(validate_fdk(g, filter, dtype, "b2t_fdk_weight_filter"));
@@ -553,7 +677,8 @@ b2t_status fdk_weight_filter_impl(const b2t_geom3d *g, int32_t filter, int32_t s
                              (long long)proj_pitch * d.angles, dtype, s);
 }
 
-b2t_status fdk_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, float output_scale, const void *proj,
+b2t_status fdk_impl(const b2t_geom3d *g, const b2t_filter_config *filter, int32_t short_scan, float output_scale,
+                    const void *proj,
                     size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s)
 {
     B2T_TRY(validate_fdk(g, filter, dtype, "b2t_fdk"));

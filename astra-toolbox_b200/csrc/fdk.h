@@ -24,12 +24,13 @@ void fdk_weights(float fSrcOrigin, float fDetOrigin, float fZShift, float fDetUS
                  uint32_t n_angles, uint32_t det_u, const float *angles, int short_scan, FDKWeights &P,
                  std::vector<float> &rel);
 b2t_status fdk_setup(const b2t_geom3d *g, int short_scan, FDKWeights &P, std::vector<float> &rel);
-b2t_status filter_rows_impl(float *data, size_t nrows, uint32_t n, size_t pitch, int32_t filter, cudaStream_t s);
-b2t_status fbp2d_impl(const b2t_geom2d *g, int32_t filter, int32_t short_scan, const float *sino, size_t sino_pitch,
+b2t_status filter_rows_impl(float *data, size_t nrows, uint32_t n, size_t pitch, const b2t_filter_config *filter,
+                            cudaStream_t s);
+b2t_status fbp2d_impl(const b2t_geom2d *g, const b2t_filter_config *filter, int32_t short_scan, const float *sino, size_t sino_pitch,
                       float *vol, size_t vol_pitch, int32_t mode, cudaStream_t s);
-b2t_status fdk_weight_filter_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, void *proj,
+b2t_status fdk_weight_filter_impl(const b2t_geom3d *g, const b2t_filter_config *filter, int32_t short_scan, void *proj,
                                   size_t proj_pitch, int32_t dtype, cudaStream_t s);
-b2t_status fdk_impl(const b2t_geom3d *g, int32_t filter, int32_t short_scan, float output_scale, const void *proj,
+b2t_status fdk_impl(const b2t_geom3d *g, const b2t_filter_config *filter, int32_t short_scan, float output_scale, const void *proj,
                     size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
 
 }  // namespace b2t

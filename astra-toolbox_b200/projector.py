@@ -194,15 +194,54 @@ def bp3d(projector, vol, proj, mode=_lib.MODE_SET):
     return vol
 
 
-_FILTERS = {'none': _lib.FILTER_NONE, 'ram-lak': _lib.FILTER_RAMLAK, 'ramlak': _lib.FILTER_RAMLAK}
-
-
 def filter_code(name):
-    """FilterType option -> libb2tomo filter code (Filters.cpp:508 names)."""
+    """FilterType option -> filter code (the reference's names, src/Filters.cpp:
+    508-532, case-insensitive; 'ramlak' is accepted for 'ram-lak')."""
     key = (name or 'ram-lak').lower()
-    if key not in _FILTERS:
-        raise AstraError(2, "FilterType %r is not implemented (ram-lak and none are)" % name)
-    return _FILTERS[key]
+    if key == 'ramlak':
+        key = 'ram-lak'
+    if key not in _lib.FILTER_NAMES:
+        raise AstraError(2, "Failed to convert %r into a filter" % (name,))
+    return _lib.FILTER_NAMES.index(key)
+
+
+class FilterSpec:
+    """A filter for FDK / FBP / row filtering: SFilterConfig's fields
+    (include/astra/Filters.h:70-82).  `custom` is a 1D or 2D array for the
+    projection / sinogram / rprojection / rsinogram types."""
+
+    def __init__(self, filter_type='ram-lak', d=1.0, parameter=-1.0, custom=None):
+        self.type = filter_code(filter_type) if isinstance(filter_type, str) else int(filter_type)
+        self.d = float(d)
+        self.parameter = float(parameter)
+        self.custom = None
+        if custom is not None:
+            c = np.ascontiguousarray(np.asarray(custom, dtype=np.float32))
+            self.custom = c.reshape(1, -1) if c.ndim == 1 else c
+
+    def c(self):
+        """The ctypes b2t_filter_config (valid while this object lives)."""
+        cfg = _lib.FilterConfig(self.type, self.d, self.parameter, None, 0, 0)
+        if self.custom is not None:
+            cfg.custom = self.custom.ctypes.data
+            cfg.custom_height, cfg.custom_width = self.custom.shape
+        return cfg
+
+
+def _filter_spec(filter_type):
+    return filter_type if isinstance(filter_type, FilterSpec) else FilterSpec(filter_type)
+
+
+def filter_taps(filter_type, n, n_views=1):
+    """The filter's exact spatial taps (b2t_filter_taps): array (sets, 2n-1),
+    tap of offset d at column d + n - 1."""
+    spec = _filter_spec(filter_type)
+    cfg = spec.c()
+    count = ctypes.c_size_t(0)
+    _lib.call("b2t_filter_taps", ctypes.byref(cfg), int(n), int(n_views), None, ctypes.byref(count))
+    out = np.zeros(count.value, dtype=np.float32)
+    _lib.call("b2t_filter_taps", ctypes.byref(cfg), int(n), int(n_views), out.ctypes.data, ctypes.byref(count))
+    return out.reshape(-1, 2 * int(n) - 1)
 
 
 def fdk(projector, proj, vol, short_scan=False, filter_type='ram-lak', output_scale=1.0, mode=_lib.MODE_SET):
@@ -212,7 +251,9 @@ def fdk(projector, proj, vol, short_scan=False, filter_type='ram-lak', output_sc
     if vol.dtype != proj.dtype:
         raise AstraError(1, "volume and projection data must have the same dtype")
     with torch.cuda.device(vol.device):
-        _lib.call("b2t_fdk", ctypes.byref(projector.geom.c), filter_code(filter_type), int(bool(short_scan)),
+        spec = _filter_spec(filter_type)
+        cfg = spec.c()
+        _lib.call("b2t_fdk", ctypes.byref(projector.geom.c), ctypes.byref(cfg), int(bool(short_scan)),
                   float(output_scale), proj.data_ptr(), 0, vol.data_ptr(), 0, _DTYPES[vol.dtype], mode,
                   stream_handle(vol.device))
     return vol
@@ -223,7 +264,9 @@ def fbp2d(projector, sino, vol, short_scan=False, filter_type='ram-lak', mode=_l
     _check_tensor(vol, projector.vol_shape, "volume")
     _check_tensor(sino, projector.proj_shape, "sinogram", vol.device)
     with torch.cuda.device(vol.device):
-        _lib.call("b2t_fbp2d", ctypes.byref(projector.geom.c), filter_code(filter_type), int(bool(short_scan)),
+        spec = _filter_spec(filter_type)
+        cfg = spec.c()
+        _lib.call("b2t_fbp2d", ctypes.byref(projector.geom.c), ctypes.byref(cfg), int(bool(short_scan)),
                   sino.data_ptr(), 0, vol.data_ptr(), 0, mode, stream_handle(vol.device))
     return vol
 
@@ -278,6 +321,8 @@ def fdk_weight_filter(projector, proj, short_scan=False, filter_type='ram-lak'):
     """FDK pre-weighting and filtering of proj in place."""
     _check_tensor(proj, projector.proj_shape, "projection data")
     with torch.cuda.device(proj.device):
-        _lib.call("b2t_fdk_weight_filter", ctypes.byref(projector.geom.c), filter_code(filter_type),
+        spec = _filter_spec(filter_type)
+        cfg = spec.c()
+        _lib.call("b2t_fdk_weight_filter", ctypes.byref(projector.geom.c), ctypes.byref(cfg),
                   int(bool(short_scan)), proj.data_ptr(), 0, _DTYPES[proj.dtype], stream_handle(proj.device))
     return proj

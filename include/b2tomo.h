@@ -97,8 +97,48 @@ enum {
     B2T_KER_MATCHED_BP = 4     /* exact transpose of the forward projector   */
 };
 
-/* filter types: E_FBPFILTER subset (include/astra/Filters.h:36-60) */
-enum { B2T_FILTER_NONE = 0, B2T_FILTER_RAMLAK = 1 };
+/* filter types: E_FBPFILTER (include/astra/Filters.h:43-66) in the same order
+ * without its leading FILTER_ERROR, i.e. B2T value = E_FBPFILTER value - 1 */
+enum {
+    B2T_FILTER_NONE = 0,
+    B2T_FILTER_RAMLAK = 1,
+    B2T_FILTER_SHEPPLOGAN = 2,
+    B2T_FILTER_COSINE = 3,
+    B2T_FILTER_HAMMING = 4,
+    B2T_FILTER_HANN = 5,
+    B2T_FILTER_TUKEY = 6,          /* parameter: alpha (default 0.5)           */
+    B2T_FILTER_LANCZOS = 7,
+    B2T_FILTER_TRIANGULAR = 8,
+    B2T_FILTER_GAUSSIAN = 9,       /* parameter: sigma (default 0.4)           */
+    B2T_FILTER_BARTLETTHANN = 10,
+    B2T_FILTER_BLACKMAN = 11,      /* parameter: alpha (default 0.16)          */
+    B2T_FILTER_NUTTALL = 12,
+    B2T_FILTER_BLACKMANHARRIS = 13,
+    B2T_FILTER_BLACKMANNUTTALL = 14,
+    B2T_FILTER_FLATTOP = 15,
+    B2T_FILTER_KAISER = 16,        /* parameter: alpha (default 3)             */
+    B2T_FILTER_PARZEN = 17,
+    B2T_FILTER_PROJECTION = 18,    /* custom spectrum, shared by all views     */
+    B2T_FILTER_SINOGRAM = 19,      /* custom spectrum per view                 */
+    B2T_FILTER_RPROJECTION = 20,   /* custom spatial filter, shared            */
+    B2T_FILTER_RSINOGRAM = 21      /* custom spatial filter per view           */
+};
+
+/* SFilterConfig (include/astra/Filters.h:70-82).  d: frequency cut-off
+ * scale (FilterD, spectrum zero beyond w = pi d); parameter: FilterParameter
+ * (< 0 = the type's default).  custom: host array, custom_height rows of
+ * custom_width values: for PROJECTION / SINOGRAM the real spectrum on
+ * nextpow2(2 det) / 2 + 1 bins, for RPROJECTION / RSINOGRAM a spatial filter
+ * of any width centred on its element width / 2; one row, or one per view
+ * for the SINOGRAM types.  A NULL config means Ram-Lak with d = 1. */
+typedef struct b2t_filter_config {
+    int32_t type;
+    float d;
+    float parameter;
+    const float *custom;
+    uint32_t custom_width;
+    uint32_t custom_height;
+} b2t_filter_config;
 
 /* element-wise operations: processVol3D<op> (cuda/3d/arith3d.cu:44-111) */
 enum {
@@ -268,29 +308,42 @@ b2t_status b2t_bp2d(const b2t_geom2d *geom, uint32_t pixel_supersample, int32_t 
 
 /* FDK reconstruction of a cone geometry with a circular orbit: cosine /
  * magnification pre-weight, Parker weight if short_scan, Ram-Lak (or no)
- * filter along u, then the FDK-weighted cone BP; vol (+)= result * scale.
+ * filter along u (any b2t_filter_config), then the FDK-weighted cone BP;
+ * vol (+)= result * scale.
  * Replaces astraCUDA3d::FDK (include/astra/cuda/3d/mem3d.h:113,
  * cuda/3d/fdk.cu:415-478).  Unlike the reference, proj is left unmodified:
  * the filtered projections go to a stream-ordered scratch buffer. */
-b2t_status b2t_fdk(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, float output_scale,
+b2t_status b2t_fdk(const b2t_geom3d *geom, const b2t_filter_config *filter, int32_t short_scan, float output_scale,
                    const void *proj, size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype,
                    int32_t mode, void *stream);
 
 /* Pre-weighting (+ Parker) and filtering of proj in place: FDK_PreWeight +
  * FDK_Filter (cuda/3d/fdk.cu:168-412). */
-b2t_status b2t_fdk_weight_filter(const b2t_geom3d *geom, int32_t filter, int32_t short_scan, void *proj,
+b2t_status b2t_fdk_weight_filter(const b2t_geom3d *geom, const b2t_filter_config *filter, int32_t short_scan, void *proj,
                                  size_t proj_pitch, int32_t dtype, void *stream);
 
-/* Ram-Lak filtering of nrows rows of n f32 samples in place (row pitch in
+/* Filtering of nrows rows of n f32 samples in place (row pitch in
  * elements): the zero-padded FFT convolution of runCudaFFT / applyFilter /
- * runCudaIFFT (cuda/2d/fft.cu:52-336) evaluated as its exact Toeplitz form. */
-b2t_status b2t_filter_rows(float *data, size_t nrows, uint32_t n, size_t pitch, int32_t filter, void *stream);
+ * runCudaIFFT (cuda/2d/fft.cu:52-336) evaluated as its exact Toeplitz form.
+ * For the per-view filter types row r uses the filter of view r. */
+b2t_status b2t_filter_rows(float *data, size_t nrows, uint32_t n, size_t pitch, const b2t_filter_config *filter,
+                           void *stream);
+
+/* Host only: the spatial taps of a filter for rows of n samples, the exact
+ * Toeplitz form of the reference's filtering (genFilter, src/Filters.cpp:
+ * 131-488, and the custom types of cuda/2d/fft.cu:447-595).  out receives
+ * n_sets x (2n - 1) floats, tap of offset d (y[i] = sum_k g[i - k] x[k]) at
+ * d + n - 1; n_sets = n_views for the SINOGRAM types, else 1 (n_views is
+ * then ignored).  *count (in: capacity of out in floats, out: needed) may be
+ * queried with out = NULL. */
+b2t_status b2t_filter_taps(const b2t_filter_config *filter, uint32_t n, uint32_t n_views, float *out,
+                           size_t *count);
 
 /* 2D filtered backprojection, vol (+)= FBP(sino); sino is not modified.
  * Replaces astraCUDA::FBP (cuda/2d/fbp.cu:77-190): parallel = filter + BP
  * scaled by (pi/2)/n_angles; fan = FDK pre-weighting of a one-row cone (+
  * Parker if short_scan) + filter + FBP-weighted fan BP. */
-b2t_status b2t_fbp2d(const b2t_geom2d *geom, int32_t filter, int32_t short_scan, const float *sino,
+b2t_status b2t_fbp2d(const b2t_geom2d *geom, const b2t_filter_config *filter, int32_t short_scan, const float *sino,
                      size_t sino_pitch, float *vol, size_t vol_pitch, int32_t mode, void *stream);
 
 /* ---------------------------------------------------------------------- */

@@ -706,6 +706,41 @@ void orc_ramp_filter_rows(double *rows, long nrows, long n, int nthreads)
     free(taps);
 }
 
+/*
+ * Any row filter as its exact Toeplitz product (the reference's zero-padded
+ * FFT convolution, cuda/3d/fdk.cu:292-398 and cuda/2d/fft.cu:52-110, with the
+ * row at offset 0 of nextpow2(2n) samples, equals the linear convolution with
+ * the inverse transform g of the filter spectrum):
+ *   y[i] = sum_j g[i - j] x[j],  g of offset d at taps[set * (2n - 1) + d + n - 1].
+ * Row r uses set (r % set_mod) when nsets > 1 (one filter per view), else set 0.
+ */
+typedef struct { double *rows; long nrows, n; const double *taps; long nsets, set_mod; } orc_toep_ctx;
+
+static void orc_toep_range(void *vctx, long begin, long end)
+{
+    orc_toep_ctx *c = (orc_toep_ctx *)vctx;
+    const long n = c->n;
+    double *tmp = (double *)malloc(sizeof(double) * (size_t)n);
+    for (long r = begin; r < end; ++r) {
+        double *x = c->rows + r * n;
+        const long set = c->nsets > 1 ? r % c->set_mod : 0;
+        const double *g = c->taps + set * (2 * n - 1) + (n - 1);
+        for (long i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (long j = 0; j < n; ++j) acc += g[i - j] * x[j];
+            tmp[i] = acc;
+        }
+        memcpy(x, tmp, sizeof(double) * (size_t)n);
+    }
+    free(tmp);
+}
+
+void orc_toeplitz_rows(double *rows, long nrows, long n, const double *taps, long nsets, long set_mod, int nthreads)
+{
+    orc_toep_ctx c = {rows, nrows, n, taps, nsets, set_mod > 0 ? set_mod : 1};
+    orc_parallel(orc_toep_range, &c, nrows, nthreads);
+}
+
 /* ------------------------------------------------------------------------- */
 /* 2D parallel FP (cuda/2d/par_fp.cu) and BP (cuda/2d/par_bp.cu)              */
 /* ------------------------------------------------------------------------- */

@@ -48,6 +48,7 @@ def lib():
         L.orc_parker_weight.argtypes = [_P, _L, _L, _L, _D, _D, _D, _P, _D, _D]
         L.orc_ramp_filter_rows.argtypes = [_P, _L, _L, _I]
         L.orc_ramp_taps.argtypes = [_L, _P]
+        L.orc_toeplitz_rows.argtypes = [_P, _L, _L, _P, _L, _L, _I]
         L.orc_par_fp.argtypes = [_P, _L, _L, _L, _L, _D, _I, _I, _P, _P]
         L.orc_par_bp.argtypes = [_P, _L, _L, _L, _L, _D, _I, _I, _P, _P]
         L.orc_fan_fp.argtypes = [_P, _L, _L, _L, _L, _D, _I, _I, _P, _P]
@@ -161,12 +162,146 @@ def ramp_filter_rows(rows, nthreads=None):
     return rows
 
 
+# E_FBPFILTER order (include/astra/Filters.h:43-66) without FILTER_ERROR
+FILTERS = ['none', 'ram-lak', 'shepp-logan', 'cosine', 'hamming', 'hann', 'tukey', 'lanczos', 'triangular',
+           'gaussian', 'barlett-hann', 'blackman', 'nuttall', 'blackman-harris', 'blackman-nuttall', 'flat-top',
+           'kaiser', 'parzen', 'projection', 'sinogram', 'rprojection', 'rsinogram']
+
+
+def _next_pow2(n):
+    x = 1
+    while x < n:
+        x *= 2
+    return x
+
+
+def filter_spectrum(name, N, d=1.0, parameter=-1.0):
+    """genFilter (src/Filters.cpp:131-488) in FP64 on bins 0 .. N/2: twice the
+    real DFT of the Ram-Lak spatial taps (generateRampFilter, Filters.cpp:
+    41-69), times the window of the named type on bins >= 1, zero where
+    w = 2 pi f / N exceeds pi d."""
+    F = N // 2 + 1
+    i = np.arange(N)
+    h = np.zeros(N)
+    odd = (i % 2) == 1
+    j = np.where(2 * i > N, N - i, i)
+    h[odd] = -1.0 / (np.pi * j[odd]) ** 2
+    h[0] = 0.25
+    f = np.arange(F)
+    R = 2.0 * (np.cos(2 * np.pi * np.outer(f, i) / N) @ h)
+    n = f[1:].astype(np.float64)
+    w = 2 * np.pi * f / N
+    nm1 = F - 1.0
+    if name == 'ram-lak':
+        win = np.ones(F - 1)
+    elif name == 'shepp-logan':
+        x = w[1:] / 2 / d
+        win = np.sin(x) / x
+    elif name == 'cosine':
+        win = np.cos(w[1:] / 2 / d)
+    elif name == 'hamming':
+        win = 0.54 + 0.46 * np.cos(w[1:] / d)
+    elif name == 'hann':
+        win = (1 + np.cos(w[1:] / d)) / 2
+    elif name == 'tukey':
+        alpha = 0.5 if parameter < 0 else parameter
+        half = F / 2.0
+        a, den = alpha * half, (1 - alpha) * half
+        inside = (half - a <= n) & (n <= half + a)
+        win = np.where(inside, 1.0, 0.5 * (1 + np.cos(np.pi * (n - a) / den)))
+    elif name == 'lanczos':
+        x = np.pi * (2 * n / nm1 - 1)
+        win = np.where(np.abs(x) > 0.001, np.sin(x) / np.where(x == 0, 1, x), 1.0)
+    elif name == 'triangular':
+        win = 2 / nm1 * (nm1 / 2 - np.abs(n - nm1 / 2))
+    elif name == 'gaussian':
+        sigma = 0.4 if parameter < 0 else parameter
+        q = (F - 1) / 2.0
+        win = np.exp(-0.5 * ((n - q) / (sigma * q)) ** 2)
+    elif name == 'barlett-hann':
+        win = 0.62 - 0.48 * np.abs(n / nm1 - 0.5) - 0.38 * np.cos(2 * np.pi * n / nm1)
+    elif name == 'blackman':
+        alpha = 0.16 if parameter < 0 else parameter
+        win = (1 - alpha) / 2 - 0.5 * np.cos(np.pi * n / nm1) + alpha / 2 * np.cos(2 * np.pi * n / nm1)
+    elif name in ('nuttall', 'blackman-harris', 'blackman-nuttall', 'flat-top'):
+        a = {'nuttall': (0.355768, 0.487396, 0.144232, 0.012604, 0.0),
+             'blackman-harris': (0.35875, 0.48829, 0.14128, 0.01168, 0.0),
+             'blackman-nuttall': (0.3635819, 0.4891775, 0.1365995, 0.0106411, 0.0),
+             'flat-top': (1.0, 1.93, 1.29, 0.388, 0.032)}[name]
+        x = np.pi * n / nm1
+        win = a[0] - a[1] * np.cos(2 * x) + a[2] * np.cos(4 * x) - a[3] * np.cos(6 * x) + a[4] * np.cos(8 * x)
+    elif name == 'kaiser':
+        from scipy.special import j0
+        alpha = 3.0 if parameter < 0 else parameter
+        s = 2 * n / nm1 - 1
+        win = j0(np.pi * alpha * np.sqrt(np.clip(1 - s * s, 0, None))) / j0(np.pi * alpha)
+    elif name == 'parzen':
+        q = n / nm1
+        win = np.where(q <= 0.5, 1 - 6 * q * q * (1 - q), 2 * (1 - q) ** 3)
+    else:
+        raise ValueError("no spectrum for filter %r" % name)
+    G = R.copy()
+    G[1:] *= win
+    G[w > np.pi * d] = 0.0
+    return G
+
+
+def _spectrum_taps(G, N, n):
+    f = np.arange(1, N // 2)
+    dd = np.arange(n)
+    g = (G[0] + G[N // 2] * np.where(dd % 2 == 1, -1.0, 1.0)
+         + 2 * (np.cos(2 * np.pi * np.outer(dd, f) / N) @ G[1:N // 2])) / N
+    return np.concatenate([g[:0:-1], g])
+
+
+def filter_taps(name, n, n_views=1, d=1.0, parameter=-1.0, custom=None):
+    """Exact Toeplitz taps (sets, 2n-1) of a filter for rows of n samples, the
+    reference's zero-padded FFT filtering (cuda/2d/fft.cu:338-595): spectral
+    types from filter_spectrum, 'projection' / 'sinogram' from the custom
+    spectrum rows, 'rprojection' / 'rsinogram' from the custom spatial rows
+    centred on element width // 2."""
+    N = _next_pow2(2 * n)
+    if name in ('projection', 'sinogram'):
+        c = np.atleast_2d(np.asarray(custom, dtype=np.float64))
+        return np.array([_spectrum_taps(row, N, n) for row in c])
+    if name in ('rprojection', 'rsinogram'):
+        c = np.atleast_2d(np.asarray(custom, dtype=np.float64))
+        W = c.shape[1]
+        used = min(W, N)
+        start = (W - used) // 2
+        out = []
+        for row in c:
+            s = np.zeros(N)
+            for i in range(start, start + used):
+                s[(i + N - W // 2) % N] = row[i]
+            out.append(s[np.arange(-(n - 1), n) % N])
+        return np.array(out)
+    return _spectrum_taps(filter_spectrum(name, N, d, parameter), N, n)[None, :]
+
+
+def toeplitz_filter_rows(rows, taps, set_mod=1, nthreads=None):
+    """Filter every row of a float64 array in place with taps (sets, 2n-1);
+    with several sets, row r uses set r % set_mod."""
+    assert rows.dtype == np.float64 and rows.flags.c_contiguous
+    n = rows.shape[-1]
+    t = _c(taps, np.float64)
+    assert t.shape[-1] == 2 * n - 1
+    nsets = t.shape[0] if t.ndim == 2 else 1
+    lib().orc_toeplitz_rows(rows.ctypes.data, rows.size // n, n, t.ctypes.data, nsets, set_mod,
+                            nthreads or nthreads_default())
+    return rows
+
+
 def fdk(views, proj, vol_shape, vol_scale=(1.0, 1.0, 1.0), short_scan=False, out_scale=1.0,
-        nthreads=None):
-    """FDK: weight, ramp-filter along u, cone BP with FDK weighting (float64)."""
+        nthreads=None, taps=None):
+    """FDK: weight, filter along u (Ram-Lak, or the given taps), cone BP with
+    FDK weighting (float64)."""
     p = np.array(proj, dtype=np.float64, copy=True)
     fdk_weight(p, views, short_scan)
-    ramp_filter_rows(p, nthreads)
+    if taps is None:
+        ramp_filter_rows(p, nthreads)
+    else:
+        toeplitz_filter_rows(p, taps, set_mod=p.shape[1], nthreads=nthreads)
     return bp3d(CONE, views, p.astype(np.float32), vol_shape, vol_scale, out_scale, kernel=KER_FDK,
                 nthreads=nthreads)
 

@@ -34,6 +34,7 @@ def lib():
         L.ref_cuda_fdk.argtypes = [_P, _I, _I, _I, _I, _I, _I, _P, _I, _F, _P, _P]
         L.ref_cuda_fp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _P, _P]
         L.ref_cuda_bp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _I, _P, _P]
+        L.ref_gen_filter.argtypes = [_I, _F, _F, _I, _P]
         _lib = L
     return _lib
 
@@ -171,3 +172,13 @@ def cuda_bp2d(kind, views, sino, vol_shape, out_scale=1.0, rays=1, fbp=False):
     assert rc == 0
     torch.cuda.synchronize()
     return vol
+
+
+def gen_filter(ref_type, N, d=1.0, parameter=-1.0):
+    """The reference's genFilter spectrum (N // 2 + 1 floats) for E_FBPFILTER
+    value ref_type (FILTER_ERROR = 0, FILTER_NONE = 1, FILTER_RAMLAK = 2, ...)."""
+    out = np.zeros(N // 2 + 1, dtype=np.float32)
+    rc = lib().ref_gen_filter(int(ref_type), float(d), float(parameter), int(N), out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("genFilter refused filter %d" % ref_type)
+    return out

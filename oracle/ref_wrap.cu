@@ -372,4 +372,21 @@ int ref_cuda_bp2d(int kind, const float *views, int W, int H, int na, int ndet, 
     return ok ? 0 : 1;
 }
 
+// The reference's filter spectrum (astra::genFilter, src/Filters.cpp:131-488)
+// for an FFT of N samples: writes N / 2 + 1 floats.  type = E_FBPFILTER value.
+// Host code only (no GPU needed).
+int ref_gen_filter(int type, float d, float parameter, int N, float *out)
+{
+    astra::SFilterConfig cfg;
+    cfg.m_eType = (astra::E_FBPFILTER)type;
+    cfg.m_fD = d;
+    cfg.m_fParameter = parameter;
+    const int F = astra::calcFFTFourierSize(N);
+    float *f = astra::genFilter(cfg, N, F);
+    if (!f) return 1;
+    std::memcpy(out, f, sizeof(float) * F);
+    delete[] f;
+    return 0;
+}
+
 }  // extern "C"

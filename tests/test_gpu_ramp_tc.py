@@ -45,7 +45,8 @@ def _filter(x, pitch=None, simt=False):
     os.environ["B2T_SIMT_FILTER"] = "1" if simt else "0"
     try:
         n0 = lib.b2t_kernel_launches()
-        st = lib.b2t_filter_rows(buf.data_ptr(), nrows, nu, pitch, L.FILTER_RAMLAK,
+        cfg = L.FilterConfig(L.FILTER_RAMLAK, 1.0, -1.0, None, 0, 0)
+        st = lib.b2t_filter_rows(buf.data_ptr(), nrows, nu, pitch, ctypes.byref(cfg),
                                  torch.cuda.current_stream().cuda_stream)
         assert st == L.B2T_OK, lib.b2t_last_error()
         torch.cuda.synchronize()
