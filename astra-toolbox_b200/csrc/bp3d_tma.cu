@@ -5,18 +5,22 @@
 // is projected onto each view, the projection is sampled bilinearly and
 // weighted.  The difference is where the samples come from:
 //
-//   - a CTA owns a 32 x 8 x 16 voxel block and walks all views of the launch;
-//   - for each view, warp 0 projects the block's eight corner voxels, takes
-//     the bounding box of their detector coordinates (plus one texel of
-//     margin) and issues one cp.async.bulk.tensor load of that tile of the
-//     zero-padded projections into a ring of shared-memory stages, signalling
-//     an mbarrier; loads run STAGES-1 views ahead of the compute;
-//   - all 256 threads then interpolate from shared memory.  For circular
+//   - a CTA owns a 32 x 8 x 16 voxel block and walks all views of the launch
+//     with eight compute warps and one producer warp;
+//   - for each view the producer projects the block's eight corner voxels,
+//     takes the bounding box of their detector coordinates (plus one texel of
+//     margin), reserves the rows of that box in a ring of shared memory and
+//     loads them from the zero-padded projections with 8-row
+//     cp.async.bulk.tensor boxes, signalling the view's mbarrier.  Tiles take
+//     only the rows their footprint needs, so the ring holds several views
+//     (up to eight) ahead of the compute warps;
+//   - the compute warps interpolate from shared memory.  For circular
 //     geometries (detector v axis along z) the detector u coordinate and the
 //     ray-density weight do not depend on z, so each thread computes them once
-//     per view and only v changes along its 16-voxel column;
-//   - a tile that does not fit the stage (extreme magnification) is read from
-//     the padded projections in global memory instead.
+//     per view (from affine forms the producer folds per block) and only v
+//     changes along its 16-voxel column;
+//   - a tile that does not fit (extreme magnification) is read from the padded
+//     projections in global memory instead.
 //
 // Every mbarrier wait is bounded (about a second); on timeout the kernel sets
 // B2T_DEVERR_WAIT_TIMEOUT in g_b2t_device_errors and returns.
@@ -67,13 +71,61 @@ __device__ __forceinline__ void split_texel_t(float qm, int &k, float &f)
     f = __fadd_rn(__fadd_rn(qm, -r), 0.5f);
 }
 
+// shared-memory texel at 32-bit shared-window address a
+template <typename T> __device__ __forceinline__ float lds_sh(uint32_t a);
+template <> __device__ __forceinline__ float lds_sh<float>(uint32_t a)
+{
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+    return v;
+}
+template <> __device__ __forceinline__ float lds_sh<__half>(uint32_t a)
+{
+    unsigned short v;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
+    return __half2float(__ushort_as_half(v));
+}
+template <> __device__ __forceinline__ float lds_sh<__nv_bfloat16>(uint32_t a)
+{
+    unsigned short v;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
+    return __bfloat162float(__ushort_as_bfloat16(v));
+}
+
+// Tile width and ring row pitch in texels: a TMA box row must be a multiple
+// of 16 bytes, and rows that share shared-memory banks should be far apart
+// (84 x 4 B: 8 rows; 88 x 2 B: 16 rows).
+template <typename T> __host__ __device__ constexpr int tile_bu() { return sizeof(T) == 4 ? 84 : 88; }
+// Ring rows (multiple of BPT_CHUNK) in the BPT_RING_BYTES of shared memory.
+// An 8-row chunk is a multiple of 128 bytes for both pitches, so every chunk
+// destination (ring rows are allocated in whole chunks) is 128-byte aligned.
+template <typename T> __host__ __device__ constexpr int ring_rows()
+{
+    return (BPT_RING_BYTES / (tile_bu<T>() * (int)sizeof(T))) & ~(BPT_CHUNK - 1);
+}
+static_assert(BPT_CHUNK * 84 * 4 % 128 == 0 && BPT_CHUNK * 88 * 2 % 128 == 0, "chunk alignment");
+static_assert((84 * 4) % 16 == 0 && (88 * 2) % 16 == 0, "TMA box row bytes");
+
+// Per-view record written by the producer warp: the tile's origin in padded
+// texels (u0, v0), its first ring row and its row count (0: the footprint does
+// not fit a tile, read global memory), and for circular geometries the
+// view's coefficients folded into affine forms of the thread's offset
+// (lx, ly) inside the CTA's block at the block's first z slice, with the
+// tile origin absorbed:
+//   cone:     U = (cu.w + cu.x lx + cu.y ly) / D,  V_j = (cv.w + cv.x lx + cv.y ly + j cv.z) / D,
+//             D = cd.w + cd.x lx + cd.y ly
+//   parallel: the same without the division; cd.w is the ray weight
+// U and V are tile-relative sample positions (texel k = floor, weight frac on
+// k + 1).
 struct StageInfo {
-    int u0, v0, fits, pad;
+    int u0, v0, row0, nrows;
+    float4 cu, cv, cd;
 };
 
 // Projected detector coordinates (texture units) of voxel centre (fx, fy, fz).
+// D is the cone denominator (1 for parallel beams).
 template <int KIND>
-__device__ __forceinline__ void project(const BPView &W, float fx, float fy, float fz, float &U, float &V)
+__device__ __forceinline__ void project(const BPView &W, float fx, float fy, float fz, float &U, float &V, float &D)
 {
     float nu = fmaf(fz, W.nu.z, fmaf(fy, W.nu.y, fmaf(fx, W.nu.x, W.nu.w)));
     float nv = fmaf(fz, W.nv.z, fmaf(fy, W.nv.y, fmaf(fx, W.nv.x, W.nv.w)));
@@ -82,114 +134,275 @@ __device__ __forceinline__ void project(const BPView &W, float fx, float fy, flo
         const float fr = __frcp_rn(dn);
         U = nu * fr;
         V = nv * fr;
+        D = dn;
     } else {
         U = nu;
         V = nv;
+        D = 1.0f;
     }
 }
 
-template <typename T, int KIND, int KER, bool CIRC>
-__global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant__ BPTmaLaunch L)
+// c.w + c.x ox + c.y oy + c.z oz + k (d.w + d.x ox + d.y oy + d.z oz), in FP64
+__device__ __forceinline__ float4 fold_form(float4 c, float4 d, double k, double ox, double oy, double oz, bool keep_z)
 {
+    const double cx = (double)c.x + k * d.x, cy = (double)c.y + k * d.y, cz = (double)c.z + k * d.z;
+    const double cw = (double)c.w + k * d.w;
+    const double w0 = cw + cx * ox + cy * oy + cz * oz;
+    return make_float4((float)cx, (float)cy, keep_z ? (float)cz : 0.0f, (float)w0);
+}
+
+// Producer warp of bp3d_tma_kernel (a separate function so that its
+// registers are allocated apart from the compute warps' accumulators).
+// Lane l works out view vb + l of each batch of 32: its footprint, tile
+// origin, row count and folded record, all independent of where the tile
+// lands in the ring.  The views then go through the ring one at a time: the
+// warp finds room together (waiting for the oldest views to be released) and
+// the view's own lane issues the loads and writes the record.
+template <typename T, int KIND, bool CIRC>
+__device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t *full, uint64_t *empty,
+                                        StageInfo *info, int lane, float cx,
+                                        float cy, float fz0)
+{
+    constexpr int R = ring_rows<T>();
+    constexpr int BU = tile_bu<T>();
+    // voxel-centre extent of the block; along z the block's full BPT_Z
+    // slices, so that the voxels computed past the volume's last slice
+    // (and discarded) also project inside the tile
+    const float bx0 = (float)(blockIdx.x * 32) + cx, bx1 = (float)(min(L.nx, (int)blockIdx.x * 32 + 32) - 1) + cx;
+    const float by0 = (float)(blockIdx.y * 8) + cy, by1 = (float)(min(L.ny, (int)blockIdx.y * 8 + 8) - 1) + cy;
+    const float bz0 = fz0, bz1 = fz0 + (float)(BPT_Z - 1);
+    int j0 = 0;         // oldest view still held by the compute warps
+    int head = 0;       // next free ring row
+    int slot_row0 = 0;  // lane s < BPT_SLOTS: first ring row of the view in slot s
+    for (int vb = 0; vb < L.nviews; vb += 32) {
+        const int v = vb + lane;
+        StageInfo r;
+        r.u0 = r.v0 = r.row0 = r.nrows = 0;
+        r.cu = r.cv = r.cd = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (v < L.nviews) {
+            const BPView &W = L.views[v];
+            float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f, dmin = 3.0e38f;
+#pragma unroll 1
+            for (int c = 0; c < 8; ++c) {
+                float U, V, D;
+                project<KIND>(W, (c & 1) ? bx1 : bx0, (c & 2) ? by1 : by0, (c & 4) ? bz1 : bz0, U, V, D);
+                umin = fminf(umin, U);
+                umax = fmaxf(umax, U);
+                vmin = fminf(vmin, V);
+                vmax = fmaxf(vmax, V);
+                dmin = fminf(dmin, D);
+            }
+            // padded texel index of continuous coordinate c is floor(c - 0.5) + 2;
+            // one texel of margin on each side for rounding in the consumers.
+            // A cone denominator positive at all eight corners is positive on
+            // the whole block, which then projects inside the corners' box.
+            const float lim = 1.0e7f;
+            if (dmin > 0.0f && umin > -lim && umax < lim && vmin > -lim && vmax < lim) {
+                const int ua = (int)floorf(umin - 0.5f) + 2 - 1;
+                const int ub = (int)floorf(umax - 0.5f) + 2 + 2;
+                const int va = (int)floorf(vmin - 0.5f) + 2 - 1;
+                const int vb2 = (int)floorf(vmax - 0.5f) + 2 + 2;
+                const int u0 = ua & ~7;  // TMA: x * element size must be 16-byte aligned
+                const int rows = (vb2 - va + BPT_CHUNK) & ~(BPT_CHUNK - 1);  // rows va..vb2, whole chunks
+                if (ub - u0 < BU && rows <= BPT_BV) {
+                    r.u0 = u0;
+                    r.v0 = va;
+                    r.nrows = rows;
+                }
+            }
+            if (CIRC && r.nrows > 0) {
+                // sample position in tile texels: c + 1.5 - origin (c the
+                // continuous detector coordinate, origin the padded index)
+                const double ox = bx0, oy = by0, oz = bz0;
+                if (KIND == B2T_GEOM_CONE) {
+                    r.cu = fold_form(W.nu, W.den, 1.5 - r.u0, ox, oy, oz, false);
+                    r.cv = fold_form(W.nv, W.den, 1.5 - r.v0, ox, oy, oz, true);
+                    r.cd = fold_form(W.den, W.den, 0.0, ox, oy, oz, false);
+                } else {
+                    const float4 one = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                    r.cu = fold_form(W.nu, one, 1.5 - r.u0, ox, oy, oz, false);
+                    r.cv = fold_form(W.nv, one, 1.5 - r.v0, ox, oy, oz, true);
+                    r.cd = make_float4(0.0f, 0.0f, 0.0f, W.den.w);
+                }
+            }
+        }
+        const int cnt = min(32, L.nviews - vb);
+        for (int k = 0; k < cnt; ++k) {
+            // warp-uniform from here on: every lane follows the same room
+            // search, so each lane also acquires the released views itself
+            const int nrows = __shfl_sync(0xffffffffu, r.nrows, k);
+            const int vk = vb + k;
+            const int slot = vk % BPT_SLOTS;
+            int at = 0;
+            // room: a free slot and nrows contiguous ring rows; views leave
+            // the ring in order, so wait for the oldest
+            for (;;) {
+                const int live = vk - j0;
+                if (live < BPT_SLOTS) {
+                    if (live == 0) {
+                        head = 0;
+                        at = 0;
+                        break;
+                    }
+                    if (nrows == 0) {
+                        at = head;
+                        break;
+                    }
+                    const int tail = __shfl_sync(0xffffffffu, slot_row0, j0 % BPT_SLOTS);
+                    if (head > tail) {
+                        if (R - head >= nrows) {
+                            at = head;
+                            break;
+                        }
+                        if (tail >= nrows) {
+                            at = 0;
+                            break;
+                        }
+                    } else if (head < tail && tail - head >= nrows) {
+                        at = head;
+                        break;
+                    }
+                }
+                if (!__all_sync(0xffffffffu, mbar_wait_bounded(&empty[j0 % BPT_SLOTS],
+                                                               (uint32_t)((j0 / BPT_SLOTS) & 1), 2000000000LL))) {
+                    if (lane == 0) atomicOr(&g_b2t_device_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
+                    return;
+                }
+                ++j0;
+            }
+            if (lane == slot) slot_row0 = at;
+            if (nrows > 0) head = at + nrows;
+            if (lane == k) {
+                // the loads go out before the record is written: the view's
+                // phase cannot complete before the arrival, which releases
+                // the record
+                if (nrows > 0) {
+                    mbar_expect_tx(&full[slot], (uint32_t)(nrows * BU * sizeof(T)));
+                    for (int c = 0; c < nrows; c += BPT_CHUNK)
+                        tma_load_3d(ring + (size_t)(at + c) * BU, &L.tmap, r.u0, L.a0 + vk, r.v0 + c, &full[slot]);
+                }
+                r.row0 = at;
+                info[slot] = r;
+                mbar_arrive(&full[slot]);
+            }
+        }
+    }
+}
+
+// 288 threads: warps 0-7 backproject a 32 x 8 x BPT_Z voxel block, warp 8
+// streams the views' tiles into the ring ahead of them.
+template <typename T, int KIND, int KER, bool CIRC>
+__global__ void __launch_bounds__(288, 3) bp3d_tma_kernel(const __grid_constant__ BPTmaLaunch L)
+{
+    constexpr int R = ring_rows<T>();
+    constexpr int BU = tile_bu<T>();
     extern __shared__ __align__(128) unsigned char smraw[];
-    T *tiles = reinterpret_cast<T *>(smraw);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smraw + (size_t)BPT_STAGES * BPT_BV * BPT_BU * sizeof(T));
-    uint64_t *empty = full + BPT_STAGES;
-    StageInfo *info = reinterpret_cast<StageInfo *>(empty + BPT_STAGES);
+    T *ring = reinterpret_cast<T *>(smraw);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smraw + (size_t)R * BU * sizeof(T));
+    uint64_t *empty = full + BPT_SLOTS;
+    StageInfo *info = reinterpret_cast<StageInfo *>(empty + BPT_SLOTS);
 
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
-    // a warp covers 8 x 4 voxels, so its detector footprint in a tile row
-    // stays under 32 texels (no shared-memory bank conflicts between lanes
-    // of one row); the 8 warps tile the 32 x 8 block
-    const int x = blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7);
-    const int y = blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3);
     const int z0 = blockIdx.z * BPT_Z;
-    const bool active = (x < L.nx) && (y < L.ny);
-    const float cx = 0.5f - 0.5f * (float)L.nx, cy = 0.5f - 0.5f * (float)L.ny, cz = 0.5f - 0.5f * (float)L.nz;
-    const float fx = (float)x + cx, fy = (float)y + cy, fz0 = (float)z0 + cz;
-    // voxel-centre extent of this block (for the footprint)
-    const float bx0 = (float)(blockIdx.x * 32) + cx, bx1 = (float)(min(L.nx, (int)blockIdx.x * 32 + 32) - 1) + cx;
-    const float by0 = (float)(blockIdx.y * 8) + cy, by1 = (float)(min(L.ny, (int)blockIdx.y * 8 + 8) - 1) + cy;
-    const float bz0 = fz0, bz1 = (float)(min(L.nz, z0 + BPT_Z) - 1) + cz;
 
     if (tid == 0) {
-        for (int s = 0; s < BPT_STAGES; ++s) {
+        for (int s = 0; s < BPT_SLOTS; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 8);  // one arrival per warp when it is done with the stage
+            mbar_init(&empty[s], 8);  // one arrival per compute warp when it is done with the view
         }
         mbar_fence_init();
         tma_prefetch_map(&L.tmap);
     }
     __syncthreads();
 
-    // warp 0: footprint of view i and its tile load
-    auto produce = [&](int i) {
-        const int stage = i % BPT_STAGES;
-        const BPView &W = L.views[i];
-        float U = 0.0f, V = 0.0f;
-        if (lane < 8) {
-            project<KIND>(W, (lane & 1) ? bx1 : bx0, (lane & 2) ? by1 : by0, (lane & 4) ? bz1 : bz0, U, V);
-        }
-        float umin = (lane < 8) ? U : 3.0e38f, umax = (lane < 8) ? U : -3.0e38f;
-        float vmin = (lane < 8) ? V : 3.0e38f, vmax = (lane < 8) ? V : -3.0e38f;
-#pragma unroll
-        for (int o = 4; o > 0; o >>= 1) {
-            umin = fminf(umin, __shfl_xor_sync(0xffffffffu, umin, o));
-            umax = fmaxf(umax, __shfl_xor_sync(0xffffffffu, umax, o));
-            vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
-            vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-        }
-        if (lane == 0) {
-            // padded texel index of continuous coordinate c is floor(c - 0.5) + 2;
-            // one texel of margin on each side for rounding in the consumers
-            int fits = 0, u0 = 0, v0 = 0;
-            const float lim = 1.0e7f;
-            if (umin > -lim && umax < lim && vmin > -lim && vmax < lim) {
-                const int ua = (int)floorf(umin - 0.5f) + 2 - 1;
-                const int ub = (int)floorf(umax - 0.5f) + 2 + 2;
-                const int va = (int)floorf(vmin - 0.5f) + 2 - 1;
-                const int vb = (int)floorf(vmax - 0.5f) + 2 + 2;
-                u0 = ua & ~7;  // TMA: x * element size must be 16-byte aligned
-                v0 = va;
-                fits = (ub - u0 < BPT_BU) && (vb - v0 < BPT_BV);
-            }
-            info[stage] = StageInfo{u0, v0, fits, 0};
-            if (fits) {
-                fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&full[stage], (uint32_t)(BPT_BU * BPT_BV * sizeof(T)));
-                tma_load_3d(tiles + (size_t)stage * BPT_BV * BPT_BU, &L.tmap, u0, L.a0 + i, v0, &full[stage]);
-            } else {
-                mbar_arrive(&full[stage]);
-            }
-        }
-    };
-
-    if (warp == 0) {
-        const int n0 = min(BPT_STAGES, L.nviews);
-        for (int i = 0; i < n0; ++i) produce(i);
+    if (warp == 8) {
+        const float cx = 0.5f - 0.5f * (float)L.nx, cy = 0.5f - 0.5f * (float)L.ny;
+        const float fz0 = (float)z0 + 0.5f - 0.5f * (float)L.nz;
+        bp_produce<T, KIND, CIRC>(L, ring, full, empty, info, lane, cx, cy, fz0);
+        return;
     }
+
+    // ---- compute warps
+    // a warp covers 8 x 4 voxels, so its detector footprint in a tile row
+    // stays under 32 texels; the 8 warps tile the 32 x 8 block
+    const int x = blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7);
+    const int y = blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3);
+    const bool active = (x < L.nx) && (y < L.ny);
+    // this thread's offset inside the block
+    const float lx = (float)(x - (int)blockIdx.x * 32), ly = (float)(y - (int)blockIdx.y * 8);
 
     float acc[BPT_Z];
 #pragma unroll
     for (int j = 0; j < BPT_Z; ++j) acc[j] = 0.0f;
 
-    const T *gproj = static_cast<const T *>(L.proj);
+    int slot = 0;
+    uint32_t parity = 0;
     for (int i = 0; i < L.nviews; ++i) {
-        const int stage = i % BPT_STAGES;
-        const uint32_t parity = (uint32_t)((i / BPT_STAGES) & 1);
-        // every wait is bounded: a thread that gives up records the error
-        // and leaves; the others then give up on the barriers it no longer
-        // arrives on, so the kernel always ends
-        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[stage], parity, 2000000000LL))) {
+        // every wait is bounded: a warp that gives up records the error and
+        // leaves; the producer then gives up on the release it no longer
+        // gets, so the kernel always ends
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[slot], parity, 2000000000LL))) {
             if (lane == 0) atomicOr(&g_b2t_device_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
             return;
         }
-        const StageInfo si = info[stage];
-        const BPView &W = L.views[i];
-        if (active) {
-            const T *tile = tiles + (size_t)stage * BPT_BV * BPT_BU;
+        const int4 hd = *reinterpret_cast<const int4 *>(&info[slot]);  // u0, v0, row0, nrows
+        const T *tile = ring + (size_t)hd.z * BU;
+        bool done = false;
+        if (CIRC && active && hd.w > 0) {
+            // u and the weight are independent of z, v is linear in z
+            const float4 cu = info[slot].cu, cv = info[slot].cv, cd = info[slot].cd;
+            float Uq = fmaf(ly, cu.y, fmaf(lx, cu.x, cu.w));
+            float Vq = fmaf(ly, cv.y, fmaf(lx, cv.x, cv.w));
+            float dV = cv.z, w;
+            if (KIND == B2T_GEOM_CONE) {
+                const float fr = __frcp_rn(fmaf(ly, cd.y, fmaf(lx, cd.x, cd.w)));
+                Uq *= fr;
+                Vq *= fr;
+                dV *= fr;
+                w = (KER == B2T_KER_2D_WEIGHTING) ? fr : fr * fr;
+            } else {
+                w = cd.w;
+            }
+            const float M = 12582912.0f;  // 1.5 * 2^23: q + M rounded down holds floor(q) in its mantissa
+            // q_j = Vq + j dV is monotone in j (fmaf and rounding down are
+            // monotone), so the rows of all BPT_Z voxels are inside the tile
+            // when the first and the last are
+            const int ka = __float_as_int(__fadd_rd(Vq, M)) - 0x4B400000;
+            const int kb = __float_as_int(__fadd_rd(fmaf((float)(BPT_Z - 1), dV, Vq), M)) - 0x4B400000;
+            if (min(ka, kb) >= 0 && max(ka, kb) <= hd.w - 2) {
+                const float tU = __fadd_rd(Uq, M);
+                const float fu = Uq - (tU - M);
+                const int ku = min(max(__float_as_int(tU) - 0x4B400000, 0), BU - 2);
+                // shared address of row floor(q_j), column ku, is
+                // bits(q_j + M) * row bytes + abase (32-bit wrap-around)
+                constexpr uint32_t ROWB = BU * sizeof(T);
+                const uint32_t abase = smem_u32(tile) + (uint32_t)ku * (uint32_t)sizeof(T) - 0x4B400000u * ROWB;
+#pragma unroll
+                for (int j = 0; j < BPT_Z; ++j) {
+                    const float q = fmaf((float)j, dV, Vq);
+                    const float t = __fadd_rd(q, M);
+                    const float fv = q - (t - M);
+                    const uint32_t a = (uint32_t)__float_as_int(t) * ROWB + abase;
+                    const float v00 = lds_sh<T>(a), v10 = lds_sh<T>(a + sizeof(T));
+                    const float v01 = lds_sh<T>(a + ROWB), v11 = lds_sh<T>(a + ROWB + sizeof(T));
+                    const float av = fmaf(fu, v10 - v00, v00);
+                    const float bv = fmaf(fu, v11 - v01, v01);
+                    acc[j] = fmaf(fmaf(fv, bv - av, av), w, acc[j]);
+                }
+                done = true;
+            }
+        }
+        if (active && !done) {
+            // the general paths recompute the voxel centre here rather than
+            // keeping it live across the hot loop above
+            const T *gproj = static_cast<const T *>(L.proj);
+            const float fx = (float)(blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7)) + 0.5f - 0.5f * (float)L.nx;
+            const float fy = (float)(blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3)) + 0.5f - 0.5f * (float)L.ny;
+            const float fz0 = (float)(blockIdx.z * BPT_Z) + 0.5f - 0.5f * (float)L.nz;
+            const BPView &W = L.views[i];
+            const int u0 = hd.x, v0 = hd.y, nrows = hd.w;
             if (CIRC) {
                 // u, weight independent of z; v linear in z
                 float U, w, Vb, dV;
@@ -206,21 +419,21 @@ __global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant_
                     dV = W.nv.z;
                     w = W.den.w;
                 }
-                if (si.fits) {
+                if (nrows > 0) {
                     int ku;
                     float fu;
-                    split_texel_t(U + 1.0f - (float)si.u0, ku, fu);
-                    ku = min(max(ku, 0), BPT_BU - 2);
-                    const float vofs = 1.0f - (float)si.v0;
+                    split_texel_t(U + 1.0f - (float)u0, ku, fu);
+                    ku = min(max(ku, 0), BU - 2);
+                    const float vofs = 1.0f - (float)v0;
 #pragma unroll
                     for (int j = 0; j < BPT_Z; ++j) {
                         int kv;
                         float fv;
                         split_texel_t(fmaf((float)j, dV, Vb) + vofs, kv, fv);
-                        kv = min(max(kv, 0), BPT_BV - 2);
-                        const T *p = tile + kv * BPT_BU + ku;
+                        kv = min(max(kv, 0), nrows - 2);
+                        const T *p = tile + kv * BU + ku;
                         const float v00 = lds(p), v10 = lds(p + 1);
-                        const float v01 = lds(p + BPT_BU), v11 = lds(p + BPT_BU + 1);
+                        const float v01 = lds(p + BU), v11 = lds(p + BU + 1);
                         const float a = fmaf(fu, v10 - v00, v00);
                         const float b = fmaf(fu, v11 - v01, v01);
                         acc[j] = fmaf(fmaf(fv, b - a, a), w, acc[j]);
@@ -266,16 +479,16 @@ __global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant_
                     int ku, kv;
                     float fu, fv;
                     float v00, v10, v01, v11;
-                    if (si.fits) {
-                        split_texel_t(U + 1.0f - (float)si.u0, ku, fu);
-                        split_texel_t(Vc + 1.0f - (float)si.v0, kv, fv);
-                        ku = min(max(ku, 0), BPT_BU - 2);
-                        kv = min(max(kv, 0), BPT_BV - 2);
-                        const T *p = tile + kv * BPT_BU + ku;
+                    if (nrows > 0) {
+                        split_texel_t(U + 1.0f - (float)u0, ku, fu);
+                        split_texel_t(Vc + 1.0f - (float)v0, kv, fv);
+                        ku = min(max(ku, 0), BU - 2);
+                        kv = min(max(kv, 0), nrows - 2);
+                        const T *p = tile + kv * BU + ku;
                         v00 = lds(p);
                         v10 = lds(p + 1);
-                        v01 = lds(p + BPT_BU);
-                        v11 = lds(p + BPT_BU + 1);
+                        v01 = lds(p + BU);
+                        v11 = lds(p + BU + 1);
                     } else {
                         split_texel_t(U - 1.0f, ku, fu);
                         split_texel_t(Vc - 1.0f, kv, fv);
@@ -296,17 +509,12 @@ __global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant_
                 }
             }
         }
-        // release the stage: one arrival per warp once all its lanes are done
+        // release the view: one arrival per warp once all its lanes are done
         __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[stage]);
-        // warp 0 refills it for view i + STAGES once every warp has released
-        // it; the other warps run ahead on the stages already loaded
-        if (warp == 0 && i + BPT_STAGES < L.nviews) {
-            if (!__all_sync(0xffffffffu, mbar_wait_bounded(&empty[stage], parity, 2000000000LL))) {
-                if (lane == 0) atomicOr(&g_b2t_device_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
-                return;
-            }
-            produce(i + BPT_STAGES);
+        if (lane == 0) mbar_arrive(&empty[slot]);
+        if (++slot == BPT_SLOTS) {
+            slot = 0;
+            parity ^= 1u;
         }
     }
 
@@ -328,12 +536,13 @@ __global__ void __launch_bounds__(256, 3) bp3d_tma_kernel(const __grid_constant_
 template <typename T, int KIND, int KER, bool CIRC>
 b2t_status launch_one(const BPTmaLaunch &L, const b2t_dims3d &d, cudaStream_t s)
 {
-    const size_t smem = (size_t)BPT_STAGES * BPT_BV * BPT_BU * sizeof(T) + BPT_STAGES * (2 * sizeof(uint64_t) + 16) + 64;
+    const size_t smem =
+        (size_t)ring_rows<T>() * tile_bu<T>() * sizeof(T) + BPT_SLOTS * (2 * sizeof(uint64_t) + sizeof(StageInfo));
     auto kern = bp3d_tma_kernel<T, KIND, KER, CIRC>;
     B2T_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                  "bp3d_tma smem attribute");
     dim3 grid((d.vol_x + 31) / 32, (d.vol_y + 7) / 8, (d.vol_z + BPT_Z - 1) / BPT_Z);
-    kern<<<grid, dim3(32, 8), smem, s>>>(L);
+    kern<<<grid, dim3(32, 9), smem, s>>>(L);
     count_launches(1);
     B2T_CUDA_TRY(cudaGetLastError(), "bp3d_tma launch");
     return B2T_OK;
@@ -364,7 +573,7 @@ b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *p
     BPTmaLaunch &L = *Lp;
     const uint64_t dims[3] = {pu, d.angles, (uint64_t)d.det_v + 4};
     const uint64_t strides[2] = {pu * esz, pu * esz * d.angles};
-    const uint32_t box[3] = {(uint32_t)BPT_BU, 1u, (uint32_t)BPT_BV};
+    const uint32_t box[3] = {(uint32_t)(esz == 4 ? tile_bu<float>() : tile_bu<__half>()), 1u, (uint32_t)BPT_CHUNK};
     const CUtensorMapDataType tdt = (dtype == B2T_F32) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                     : (dtype == B2T_F16) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                          : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;

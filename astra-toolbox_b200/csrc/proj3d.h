@@ -61,11 +61,14 @@ struct BPLaunch {
     BPView views[BP_MAX_VIEWS];
 };
 
-// TMA-staged backprojection (bp3d_tma.cu): voxel block, tile box, stages.
-constexpr int BPT_Z = 16;          // voxels per thread along z
-constexpr int BPT_BU = 80;         // tile width in texels (u), multiple of 8
-constexpr int BPT_BV = 64;         // tile height in texels (v)
-constexpr int BPT_STAGES = 3;
+// TMA-staged backprojection (bp3d_tma.cu): voxel block, tile geometry and
+// the shared-memory ring the tiles stream through.
+constexpr int BPT_Z = 16;             // voxels per thread along z
+constexpr int BPT_CHUNK = 8;          // tile rows per TMA box; a view loads the chunks its footprint needs
+constexpr int BPT_BV = 64;            // most rows one view's tile may take
+constexpr int BPT_RING_BYTES = 72576; // ring of tile rows (216 f32 rows of 84, 408 f16/bf16 rows of 88);
+                                      // three CTAs of ring + records fit an SM's 228 KB
+constexpr int BPT_SLOTS = 8;          // views in flight at most (barrier pairs and stage records)
 constexpr int BPT_MAX_VIEWS = 640;
 
 struct alignas(64) BPTmaLaunch {

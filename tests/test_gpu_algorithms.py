@@ -221,3 +221,31 @@ def test_fdk_algorithm_object(astra, orc):
     assert rel_l2(astra.data3d.get(rid), want) < 1e-5
     astra.algorithm.delete(aid)
     astra.data3d.delete([sid, rid])
+
+
+def test_optomo_matches_projector_and_solves(astra, orc):
+    """OpTomo (python/astra/optomo.py interface): W * x, W.T * s on numpy and
+    CUDA tensors equal the projector's FP / BP; scipy lsqr runs on it."""
+    import scipy.sparse.linalg
+    vg, pg = _par2d_setup(astra)
+    pid = astra.create_projector('cuda', pg, vg)
+    W = astra.OpTomo(pid)
+    pr = astra.Projector2D(pg, vg)
+    x = np.random.default_rng(8).random(pr.vol_shape).astype(np.float32)
+    s = W * x
+    ref = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(torch.from_numpy(x).cuda(), ref)
+    assert np.array_equal(s, ref.cpu().numpy())
+    b = W.T * s
+    refb = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(ref, refb)
+    assert np.array_equal(b, refb.cpu().numpy())
+    # flattened vectors and CUDA tensors
+    assert np.array_equal(W.matvec(x.ravel()), s.ravel())
+    tx = torch.from_numpy(x).cuda()
+    assert torch.equal(W * tx, ref)
+    assert W.shape == (s.size, x.size)
+    sol = scipy.sparse.linalg.lsqr(W, s.ravel(), iter_lim=20)[0]
+    assert np.linalg.norm(W.matvec(sol) - s.ravel()) < 0.2 * np.linalg.norm(s)
+    rec = W.reconstruct('SIRT_CUDA', s, 20)
+    assert rec.shape == pr.vol_shape and np.isfinite(rec).all()
