@@ -634,12 +634,10 @@ b2t_status fp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
 {
     B2T_TRY(validate3d(g, "b2t_fp3d"));
     if (!p) return fail(B2T_ERR_INVALID_ARG, "b2t_fp3d: null params");
-    if (!vol || !proj) return fail(B2T_ERR_INVALID_ARG, "b2t_fp3d: null data pointer");
+    if (!proj) return fail(B2T_ERR_INVALID_ARG, "b2t_fp3d: null data pointer");
     if (!dtype_valid(dtype)) return fail(B2T_ERR_INVALID_ARG, "b2t_fp3d: bad dtype %d", dtype);
     if (mode != B2T_MODE_ADD && mode != B2T_MODE_SET)
         return fail(B2T_ERR_INVALID_ARG, "b2t_fp3d: bad mode %d", mode);
-    if (p->kernel == B2T_KER_SUM_SQUARE_WEIGHTS)
-        return fail(B2T_ERR_UNSUPPORTED, "b2t_fp3d: sum_square_weights is not implemented");
     if (p->kernel < 0 || p->kernel > B2T_KER_MATCHED_BP)
         return fail(B2T_ERR_INVALID_ARG, "b2t_fp3d: bad kernel %d", p->kernel);
     if (p->det_supersample == 0 || p->det_supersample > 16)
@@ -649,6 +647,9 @@ b2t_status fp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
     if (proj_pitch == 0) proj_pitch = d.det_u;
     if (vol_pitch < d.vol_x || proj_pitch < d.det_u)
         return fail(B2T_ERR_INVALID_ARG, "b2t_fp3d: pitch below row length");
+    // sum_square_weights reads no volume (vol may be null)
+    if (p->kernel == B2T_KER_SUM_SQUARE_WEIGHTS) return fp3d_sumsqw_impl(g, p, proj, proj_pitch, dtype, mode, s);
+    if (!vol) return fail(B2T_ERR_INVALID_ARG, "b2t_fp3d: null data pointer");
 
     std::vector<int> dirs(d.angles);
     bool need[3] = {false, false, false};

@@ -104,6 +104,8 @@ bool force_simple_fp();
 b2t_status fp3d_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch, void *proj,
                       size_t proj_pitch, int32_t dtype, int32_t mode, const std::vector<int> &dirs, cudaStream_t s);
 
+b2t_status fp3d_sumsqw_impl(const b2t_geom3d *g, const b2t_params3d *p, void *proj, size_t proj_pitch,
+                            int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status fp3d_autotune_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch,
                               void *proj, size_t proj_pitch, int32_t dtype, cudaStream_t s, int32_t *vpc_out);
 b2t_status fp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch,

@@ -270,8 +270,12 @@ b2t_status b2t_normalize_views2d(const b2t_volgeom2d *vol, int32_t kind, uint32_
 /* Forward projection proj (+)= A vol.  Replaces astraCUDA3d::FP
  * (include/astra/cuda/3d/mem3d.h:107), ConeFP (cone_fp.h:33-36) and Par3DFP
  * (par3d_fp.h:33-36).  Kernels: DEFAULT, 2D_WEIGHTING, FDK_WEIGHTING and
- * MATCHED_BP project identically (cuda/3d/mem3d.cu:355-386).  vol and proj
- * have storage type dtype (B2T_F32/F16/BF16). */
+ * MATCHED_BP project identically (cuda/3d/mem3d.cu:355-386).
+ * SUM_SQUARE_WEIGHTS (parallel-beam geometries, no detector supersampling)
+ * writes each ray's sum of squared interpolation weights times the squared
+ * ray-length factor instead, as Par3DFP_SumSqW (par3d_fp.h:43, par3d_fp.cu:607);
+ * it reads no volume and vol may be NULL.  vol and proj have storage type
+ * dtype (B2T_F32/F16/BF16). */
 b2t_status b2t_fp3d(const b2t_geom3d *geom, const b2t_params3d *params,
                     const void *vol, size_t vol_pitch, void *proj, size_t proj_pitch,
                     int32_t dtype, int32_t mode, void *stream);

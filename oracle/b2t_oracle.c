@@ -340,6 +340,62 @@ int orc_fp3d(int kind, const double *views, long nx, long ny, long nz, long na, 
 }
 
 /*
+ * Sum of squared linear-interpolation weights of one axis at texture
+ * coordinate x (texel centres at i + 0.5, zero border), the piecewise form of
+ * dirWeights (cuda/3d/par3d_fp.cu:329-340).
+ */
+static double orc_dir_sqw(double x, double n)
+{
+    if (x <= -0.5) return 0.0;
+    if (x <= 0.5) return (x + 0.5) * (x + 0.5);
+    if (x <= n - 0.5) {
+        double t = x + 0.5 - floor(x + 0.5);
+        return t * t + (1.0 - t) * (1.0 - t);
+    }
+    if (x <= n + 0.5) return (n + 0.5 - x) * (n + 0.5 - x);
+    return 0.0;
+}
+
+/*
+ * "sum_square_weights" forward projection of a parallel-beam geometry: per
+ * ray, the sum over the dominant axis's slices of the product of both plane
+ * axes' squared interpolation weights, times the squared ray-length factor
+ * with the non-cube scales (par3D_FP_SumSqW_t, cuda/3d/par3d_fp.cu:343-415;
+ * host Par3DFP_SumSqW, par3d_fp.cu:607-703, which always uses SCALE_NONCUBE
+ * and the Y-direction fScale2 = (fY/fY)^2).  No volume is read.  Writes
+ * proj[v][a][u] (rays_per_det = 1 only, as the reference).
+ */
+int orc_par3d_sumsqw(const double *views, long nx, long ny, long nz, long na, long nu, long nv,
+                     const double *vs, double out_scale, double *proj)
+{
+    for (long a = 0; a < na; ++a) {
+        const double *w = views + 12 * a;
+        int dir = orc_dominant_axis3d(ORC_PAR3D, w, nu, nv);
+        long n0, n1, n2, st0, st1, st2;
+        orc_plane3d(dir, nx, ny, nz, &n0, &n1, &n2, &st0, &st1, &st2);
+        double f1, f2, mul;
+        orc_scale_factors3d(ORC_PAR3D, dir, vs, 1, &f1, &f2, &mul);
+        for (long v = 0; v < nv; ++v) {
+            for (long u = 0; u < nu; ++u) {
+                double a1, a2, b1, b2;
+                orc_ray3d(ORC_PAR3D, w, dir, (double)u, (double)v, &a1, &a2, &b1, &b2);
+                double sum = 0.0;
+                for (long s = 0; s < n0; ++s) {
+                    double x0 = s - 0.5 * n0 + 0.5;
+                    /* texture coordinates: index-space position + 0.5 */
+                    double t1 = a1 * x0 + b1 + 0.5 * n1;
+                    double t2 = a2 * x0 + b2 + 0.5 * n2;
+                    sum += orc_dir_sqw(t1, (double)n1) * orc_dir_sqw(t2, (double)n2);
+                }
+                double sc = sqrt(a1 * a1 * f1 + a2 * a2 * f2 + 1.0) * out_scale * mul;
+                proj[(v * na + a) * nu + u] = sum * sc * sc;
+            }
+        }
+    }
+    return 0;
+}
+
+/*
  * Exact transpose of orc_fp3d (rays_per_det = 1): vol += A^T proj.  Single
  * threaded; used to check the matched (exact-adjoint) backprojector.
  */

@@ -40,6 +40,7 @@ def lib():
         L = ctypes.CDLL(LIB)
         L.orc_fp3d.argtypes = [_I, _P, _L, _L, _L, _L, _L, _L, _P, _D, _I, _I, _P, _P, _L, _L, _I]
         L.orc_fp3d_transpose.argtypes = [_I, _P, _L, _L, _L, _L, _L, _L, _P, _D, _P, _P]
+        L.orc_par3d_sumsqw.argtypes = [_P, _L, _L, _L, _L, _L, _L, _P, _D, _P]
         L.orc_bp3d.argtypes = [_I, _I, _P, _L, _L, _L, _L, _L, _L, _P, _D, _I, _I, _P, _P, _L, _L, _I]
         L.orc_dominant_axis3d.argtypes = [_I, _P, _L, _L]
         L.orc_fdk_params.argtypes = [_P, _L, _L, _L, _P, _P]
@@ -80,6 +81,20 @@ def fp3d(kind, views, vol, det_u, det_v, vol_scale=(1.0, 1.0, 1.0), out_scale=1.
     rc = lib().orc_fp3d(kind, views.ctypes.data, nx, ny, nz, na, det_u, det_v, vs.ctypes.data,
                         out_scale, rays, int(tex8), vol.ctypes.data, proj.ctypes.data, a0, a1,
                         nthreads or nthreads_default())
+    assert rc == 0
+    return proj
+
+
+def par3d_sumsqw(views, vol_shape, det_u, det_v, vol_scale=(1.0, 1.0, 1.0), out_scale=1.0):
+    """'sum_square_weights' forward projection of a parallel-beam geometry
+    (Par3DFP_SumSqW); returns float64 [det_v][n_angles][det_u]."""
+    views = _c(views, np.float64)
+    nz, ny, nx = vol_shape
+    na = views.shape[0]
+    proj = np.zeros((det_v, na, det_u), dtype=np.float64)
+    vs = _c(vol_scale, np.float64)
+    rc = lib().orc_par3d_sumsqw(views.ctypes.data, nx, ny, nz, na, det_u, det_v, vs.ctypes.data, out_scale,
+                                proj.ctypes.data)
     assert rc == 0
     return proj
 

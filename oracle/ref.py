@@ -31,6 +31,7 @@ def lib():
         L.ref_geom2d.argtypes = [_I, _I, _I, _P, _I, _I, _F, _P, _F, _F, _P, _P, _P]
         L.ref_cuda_fp3d.argtypes = [_I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _I, _P, _P]
         L.ref_cuda_bp3d.argtypes = [_I, _I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _I, _P, _P]
+        L.ref_cuda_sumsqw.argtypes = [_P, _I, _I, _I, _I, _I, _I, _P, _F, _P]
         L.ref_cuda_fdk.argtypes = [_P, _I, _I, _I, _I, _I, _I, _P, _I, _F, _P, _P]
         L.ref_cuda_fp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _P, _P]
         L.ref_cuda_bp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _I, _P, _P]
@@ -109,6 +110,22 @@ def cuda_fp3d(kind, views, vol, nu, nv, vol_scale=(1.0, 1.0, 1.0), out_scale=1.0
     torch.cuda.synchronize()
     rc = lib().ref_cuda_fp3d(kind, views.ctypes.data, nx, ny, nz, na, nu, nv, vs.ctypes.data, out_scale,
                              rays, vol.data_ptr(), proj.data_ptr())
+    assert rc == 0
+    torch.cuda.synchronize()
+    return proj
+
+
+def cuda_sumsqw(views, vol_shape, nu, nv, vol_scale=(1.0, 1.0, 1.0), out_scale=1.0):
+    """Reference Par3DFP_SumSqW ('sum_square_weights'); returns a new float32 CUDA tensor."""
+    import torch
+    views = np.ascontiguousarray(views, dtype=np.float64)
+    vs = np.ascontiguousarray(vol_scale, dtype=np.float32)
+    nz, ny, nx = vol_shape
+    na = views.shape[0]
+    proj = torch.zeros((nv, na, nu), dtype=torch.float32, device='cuda')
+    torch.cuda.synchronize()
+    rc = lib().ref_cuda_sumsqw(views.ctypes.data, nx, ny, nz, na, nu, nv, vs.ctypes.data, out_scale,
+                               proj.data_ptr())
     assert rc == 0
     torch.cuda.synchronize()
     return proj

@@ -9,6 +9,7 @@
 // Called reference functions:
 //   astra::convertAstraGeometry      src/GeometryUtil3D.cpp:754, GeometryUtil2D.cpp:357
 //   astraCUDA3d::ConeFP / Par3DFP    cuda/3d/cone_fp.cu:444, par3d_fp.cu:564
+//   astraCUDA3d::Par3DFP_SumSqW      cuda/3d/par3d_fp.cu:607
 //   astraCUDA3d::ConeBP / Par3DBP    cuda/3d/cone_bp.cu:380, par3d_bp.cu:318
 //   astraCUDA3d::FDK                 cuda/3d/fdk.cu:415
 //   astraCUDA::FP / FanFP            cuda/2d/par_fp.cu:340, fan_fp.cu:260
@@ -237,6 +238,25 @@ int ref_cuda_fp3d(int kind, const double *views, int nx, int ny, int nz, int na,
         ok = astraCUDA3d::Par3DFP(pitched(d_vol, nx, ny), pitched(d_proj, nu, na), d, &p[0], params);
     }
     return ok ? 0 : 1;
+}
+
+// Par3DFP_SumSqW (cuda/3d/par3d_fp.cu:607): accumulates into d_proj; the
+// volume is not read.
+int ref_cuda_sumsqw(const double *views, int nx, int ny, int nz, int na, int nu, int nv, const float *vs,
+                    float out_scale, float *d_proj)
+{
+    astraCUDA3d::SProjectorParams3D params;
+    params.volScale.fX = vs[0];
+    params.volScale.fY = vs[1];
+    params.volScale.fZ = vs[2];
+    params.iRaysPerDetDim = 1;
+    params.fOutputScale = out_scale;
+    params.projKernel = astraCUDA3d::ker3d_sum_square_weights;
+    SDimensions3D d = dims3(nx, ny, nz, na, nu, nv);
+    std::vector<SPar3DProjection> p(na);
+    for (int i = 0; i < na; ++i) p[i] = to_par(views + 12 * i);
+    cudaPitchedPtr none = pitched(nullptr, nx, ny);
+    return astraCUDA3d::Par3DFP_SumSqW(none, pitched(d_proj, nu, na), d, &p[0], params) ? 0 : 1;
 }
 
 // kernel: 0 default, 2 fdk_weighting, 3 2d_weighting.  Accumulates into d_vol.

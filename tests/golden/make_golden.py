@@ -3,7 +3,7 @@
 Run on a machine with a GPU after `make -f oracle/ref.mk` has built
 oracle/_ref/libastra_ref.so from the reference sources:
 
-    python tests/golden/make_golden.py OUTDIR
+    python tests/golden/make_golden.py OUTDIR [NAME_SUBSTRING]
 
 It writes one .npz per case (seeded inputs, the reference's normalised view
 vectors and its output) that tests/test_oracle_golden.py compares the FP64
@@ -66,6 +66,29 @@ def cone_vec_vectors():
     return np.array(vecs)
 
 
+def par_vec_vectors():
+    """Nine parallel-beam views whose rays run mostly along z, x and y in turn,
+    each tilted; detector centre, u and v per view (parallel3d_vec rows)."""
+    rows = []
+    for i in range(9):
+        t = 2 * np.pi * i / 9
+        if i % 3 == 0:
+            ray = np.array([0.2 * np.cos(t), 0.3 * np.sin(t), 1.0])
+        elif i % 3 == 1:
+            ray = np.array([1.0, 0.25 * np.sin(t), 0.35])
+        else:
+            ray = np.array([0.3 * np.cos(t), -1.0, 0.4])
+        ray /= np.linalg.norm(ray)
+        a = np.array([0.0, 0.0, 1.0]) if abs(ray[2]) < 0.9 else np.array([1.0, 0.0, 0.0])
+        u = np.cross(ray, a)
+        u *= 0.9 / np.linalg.norm(u)
+        v = np.cross(ray, u)
+        v *= 1.1 / np.linalg.norm(v)
+        det = np.array([0.5 * np.cos(t), -0.4, 0.3 * np.sin(t)])
+        rows.append(np.concatenate([ray, det, u, v]))
+    return np.array(rows)
+
+
 def cases():
     ang24 = np.linspace(0, 2 * np.pi, 24, endpoint=False).astype(np.float32)
     ang15 = np.linspace(0, np.pi, 15, endpoint=False).astype(np.float32)
@@ -94,6 +117,12 @@ def cases():
     # sixth slice
     out.append(("bp3d_cone_2dw", "bp3d", vol_geom3(36, 40, 1), cone[2], {'kernel': 3}))
     out.append(("bp3d_cone_fdkw", "bp3d", cone[1], cone[2], {'kernel': 2}))
+    # sum_square_weights (parallel beams only): circular, and anisotropic
+    # voxels with rays along each axis
+    out.append(("fp3d_sumsqw_par", "sumsqw", par[1], par[2], {}))
+    out.append(("fp3d_sumsqw_vec_aniso", "sumsqw", aniso[1],
+                {'type': 'parallel3d_vec', 'DetectorRowCount': 36, 'DetectorColCount': 44,
+                 'Vectors': par_vec_vectors()}, {}))
     ang72 = np.linspace(0, 2 * np.pi, 72, endpoint=False).astype(np.float32)
     fdkg = {'type': 'cone', 'DetectorSpacingX': 1.0, 'DetectorSpacingY': 1.0, 'DetectorRowCount': 40,
             'DetectorColCount': 56, 'ProjectionAngles': ang72, 'DistanceOriginSource': 200.0,
@@ -116,17 +145,26 @@ def cases():
     return out
 
 
-def main(outdir):
+def main(outdir, only=None):
     import torch
     from oracle import ref
     os.makedirs(outdir, exist_ok=True)
     for seed, (name, op, vg, pg, opt) in enumerate(cases()):
-        if op in ("fp3d", "bp3d", "fdk"):
+        if only and only not in name:
+            continue
+        if op in ("fp3d", "bp3d", "fdk", "sumsqw"):
             views, vs = ref.geom3d(vg, pg)
             kind = 2 if pg['type'] in ('cone', 'cone_vec') else 1
             vshape = (vg['GridSliceCount'], vg['GridRowCount'], vg['GridColCount'])
             na = views.shape[0]
             pshape = (pg['DetectorRowCount'], na, pg['DetectorColCount'])
+            if op == "sumsqw":
+                res = ref.cuda_sumsqw(views, vshape, pshape[2], pshape[0], vs)
+                np.savez_compressed(os.path.join(outdir, name + ".npz"), views=views, vol_scale=vs,
+                                    vol_shape=np.array(vshape), input=np.zeros(0, np.float32),
+                                    output=res.cpu().numpy(), kind=kind)
+                print("wrote", name)
+                continue
             if op == "fp3d":
                 inp = input_volume(vshape, seed)
                 res = ref.cuda_fp3d(kind, views, torch.from_numpy(inp).cuda(), pshape[2], pshape[0], vs,
@@ -160,4 +198,5 @@ def main(outdir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"),
+         sys.argv[2] if len(sys.argv) > 2 else None)

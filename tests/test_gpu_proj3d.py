@@ -327,3 +327,42 @@ def test_autotune_fp3d_keeps_results(astra, orc, idx):
     ref = orc.fp3d(_oracle_kind(pr), pr.geom.views_array(), vol.cpu().numpy(), pr.proj_shape[2], pr.proj_shape[0],
                    pr.geom.vol_scale)
     assert rel_l2(c.cpu().numpy(), ref) < 1e-5, name
+
+
+def _sumsqw_geoms(astra):
+    ang = np.linspace(0, np.pi, 15, endpoint=False).astype(np.float32)
+    par = [g for g in _all_geoms(astra) if g[0].startswith("parallel3d")]
+    return par + [("parallel3d_aniso", astra.create_vol_geom(30, 34, 26, -16.0, 18.0, -14.0, 16.0, -12.0, 14.0),
+                   astra.create_proj_geom('parallel3d', 0.9, 1.1, 36, 44, ang + 0.2))]
+
+
+@pytest.mark.parametrize("idx", range(4))
+def test_sum_square_weights_vs_oracle(astra, orc, idx):
+    """ProjectionKernel 'sum_square_weights' (Par3DFP_SumSqW): every parallel
+    geometry, incl. vec views marching along z and anisotropic voxels."""
+    name, vg, pg = _sumsqw_geoms(astra)[idx]
+    pr = _proj(astra, vg, pg, {'ProjectionKernel': 'sum_square_weights'})
+    tp = torch.full(pr.proj_shape, 7.0, device='cuda')
+    pr.fp(torch.zeros(pr.vol_shape, device='cuda'), tp)
+    nv, na, nu = pr.proj_shape
+    ref = orc.par3d_sumsqw(pr.geom.views_array(), pr.vol_shape, nu, nv, pr.geom.vol_scale)
+    assert rel_l2(tp.cpu().numpy(), ref) < TOL_F32, name
+
+
+def test_sum_square_weights_add_mode_and_refusals(astra, orc):
+    L = __import__("importlib").import_module("astra-toolbox_b200._lib")
+    name, vg, pg = _sumsqw_geoms(astra)[0]
+    pr = _proj(astra, vg, pg, {'ProjectionKernel': 'sum_square_weights'})
+    tp = torch.ones(pr.proj_shape, device='cuda')
+    pr.fp(torch.zeros(pr.vol_shape, device='cuda'), tp, mode=L.MODE_ADD)
+    nv, na, nu = pr.proj_shape
+    ref = orc.par3d_sumsqw(pr.geom.views_array(), pr.vol_shape, nu, nv, pr.geom.vol_scale)
+    assert rel_l2(tp.cpu().numpy(), ref + 1.0) < TOL_F32
+    # the reference has it for parallel beams only, without supersampling
+    _, cvg, cpg = _cone_geoms(astra)[0]
+    cone = _proj(astra, cvg, cpg, {'ProjectionKernel': 'sum_square_weights'})
+    with pytest.raises(astra.AstraError):
+        cone.fp(torch.zeros(cone.vol_shape, device='cuda'), torch.zeros(cone.proj_shape, device='cuda'))
+    ss = _proj(astra, vg, pg, {'ProjectionKernel': 'sum_square_weights', 'DetectorSuperSampling': 2})
+    with pytest.raises(astra.AstraError):
+        ss.fp(torch.zeros(ss.vol_shape, device='cuda'), torch.zeros(ss.proj_shape, device='cuda'))

@@ -19,6 +19,23 @@ def test_par3d_column_sum_known_answer(astra, geo, orc):
     assert np.abs(p[:, 0, :] - vol.astype(np.float64).sum(axis=1)).max() < 1e-6
 
 
+def test_par3d_sum_square_weights_known_answer(astra, geo, orc):
+    # axis-aligned rays through voxel centres weigh every crossed voxel by 1 in
+    # both plane axes, so each ray's sum is the slice count (2 here); a detector
+    # shifted by half a voxel puts every ray on a texel boundary: 0.5^2 + 0.5^2
+    # per axis, except the outer rays, which keep one neighbour (0.5^2)
+    g = _par3d(astra, geo, (2, 8, 6), [0.0], (6, 8))
+    p = orc.par3d_sumsqw(g.views_array(), (6, 2, 8), 8, 6, g.vol_scale)
+    assert np.abs(p[:, 0, :] - 2.0).max() < 1e-12
+    vg = astra.create_vol_geom(2, 8, 6)
+    pg = astra.create_proj_geom('parallel3d_vec', 6, 9, np.array([[0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1]], float))
+    g2 = geo.Geometry3D(vg, pg)
+    p2 = orc.par3d_sumsqw(g2.views_array(), (6, 2, 8), 9, 6, g2.vol_scale)
+    want = np.full(9, 0.5)
+    want[[0, 8]] = 0.25
+    assert np.abs(p2[:, 0, :] - 2.0 * want[None, :]).max() < 1e-12
+
+
 def test_par2d_column_sum_known_answer(astra, geo, orc):
     # python/astra/tests.py:28-39 ('cuda' projector): column sums, 1e-6
     vg = astra.create_vol_geom(2, 32)
