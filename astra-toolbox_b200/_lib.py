@@ -94,7 +94,7 @@ class Problem2D(ctypes.Structure):
     _fields_ = [("geom", Geom2D), ("det_supersample", ctypes.c_uint32), ("pixel_supersample", ctypes.c_uint32)]
 
 
-ALGO_SIRT, ALGO_CGLS = 1, 2
+ALGO_SIRT, ALGO_CGLS, ALGO_SART = 1, 2, 3
 
 
 class AlgoOptions(ctypes.Structure):
@@ -137,6 +137,7 @@ SIGNATURES = {
     "b2t_algo_create2d": (_I32, [_I32, _P, _U32, _U32, _P, _P]),
     "b2t_algo_run": (_I32, [_P, _P, _P, _I32, _I32, _P]),
     "b2t_algo_residual_norm": (_I32, [_P, _P, _P, _P, _P]),
+    "b2t_algo_set_projection_order": (_I32, [_P, _P, _U32]),
     "b2t_algo_abort": (None, [_P]),
     "b2t_algo_destroy": (None, [_P]),
     "b2t_vec_op": (_I32, [_I32, _P, _P, _P, _F, _SZ, _P]),

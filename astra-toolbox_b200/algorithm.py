@@ -5,8 +5,8 @@ Names and configuration keys follow the reference's algorithm factory
 FP3D_CUDA (src/CudaForwardProjectionAlgorithm3D.cpp), BP3D_CUDA
 (src/CudaBackProjectionAlgorithm3D.cpp), FDK_CUDA (src/CudaFDKAlgorithm3D.cpp),
 SIRT3D_CUDA (src/CudaSirtAlgorithm3D.cpp), CGLS3D_CUDA
-(src/CudaCglsAlgorithm3D.cpp), FP_CUDA, BP_CUDA, SIRT_CUDA, CGLS_CUDA, FBP_CUDA
-(src/Cuda*Algorithm.cpp).  Every one of them runs in libb2tomo.
+(src/CudaCglsAlgorithm3D.cpp), FP_CUDA, BP_CUDA, SIRT_CUDA, CGLS_CUDA, SART_CUDA,
+FBP_CUDA (src/Cuda*Algorithm.cpp).  Every one of them runs in libb2tomo.
 """
 import ctypes
 
@@ -173,6 +173,33 @@ class _Iterative(_Algorithm):
             self.handle = ctypes.c_void_p()
 
 
+class _SART(_Iterative):
+    """SART_CUDA (src/CudaSartAlgorithm.cpp): one view per iteration.
+
+    ProjectionOrder 'random' (the default, a uniform random permutation drawn
+    once, as the reference's shuffle), 'sequential', or 'custom' with
+    ProjectionOrderList; Relaxation is lambda."""
+
+    def __init__(self, cfg):
+        super().__init__(cfg, _lib.ALGO_SART, False)
+        o = self.opt
+        na = self.pr.proj_shape[0]
+        kind = o.get('ProjectionOrder', 'random')
+        if kind == 'sequential':
+            order = None
+        elif kind == 'random':
+            order = np.random.default_rng().permutation(na)
+        elif kind == 'custom':
+            if 'ProjectionOrderList' not in o:
+                raise AstraError(1, "SART_CUDA: ProjectionOrder 'custom' needs ProjectionOrderList")
+            order = np.asarray(o['ProjectionOrderList']).ravel()
+        else:
+            raise AstraError(1, "SART_CUDA: Unknown ProjectionOrder %r" % (kind,))
+        if order is not None:
+            arr = np.ascontiguousarray(order, dtype=np.int32)
+            _lib.call("b2t_algo_set_projection_order", self.handle, arr.ctypes.data, int(arr.size))
+
+
 class _FBP2D(_Algorithm):
     def __init__(self, cfg):
         super().__init__(cfg)
@@ -197,6 +224,7 @@ _FACTORY = {
     'BP_CUDA': lambda c: _BP(c, False),
     'SIRT_CUDA': lambda c: _Iterative(c, _lib.ALGO_SIRT, False),
     'CGLS_CUDA': lambda c: _Iterative(c, _lib.ALGO_CGLS, False),
+    'SART_CUDA': _SART,
     'FBP_CUDA': _FBP2D,
 }
 

@@ -3,7 +3,9 @@
 // Reference: CCudaSirtAlgorithm3D (src/CudaSirtAlgorithm3D.cpp:261-432),
 // CCudaCglsAlgorithm3D (src/CudaCglsAlgorithm3D.cpp:264-409),
 // CCudaSirtAlgorithm (src/CudaSirtAlgorithm.cpp:187-397) and
-// CCudaCglsAlgorithm (src/CudaCglsAlgorithm.cpp:166-283).  Same recurrences,
+// CCudaCglsAlgorithm (src/CudaCglsAlgorithm.cpp:166-283), and
+// CCudaSartAlgorithm (src/CudaSartAlgorithm.cpp:196-318; step kernels in
+// sart.cu).  Same recurrences,
 // same opInvert threshold (cuda/3d/arith3d.cu:87-94), same restart of CGLS at
 // every run() call, same constraint and mask semantics.
 //
@@ -27,6 +29,7 @@
 #include "b2t_internal.h"
 #include "proj2d.h"
 #include "proj3d.h"
+#include "sart.h"
 
 namespace b2t {
 
@@ -285,6 +288,9 @@ struct Algo {
     DevBuf lineW, pixW, tmpProj, tmpVol;  // SIRT
     DevBuf r, w, p, z;                     // CGLS
     DevBuf partial, scalars;               // FP64 reductions: partials, s[0..7]
+    // SART: per-view device constants, projection order, step counter, row
+    DevBuf sart_par, sart_fan, sart_bpv, sart_order, sart_step, sart_r;
+    int sart_norder = 0;
     int nparts_vol = 0, nparts_proj = 0;
     bool weights_ready = false;
     std::atomic<bool> abort_flag{false};
@@ -432,9 +438,72 @@ struct Algo {
         return xpby_ratio(p.as<float>(), z.as<float>(), 1 - g, g, s);
     }
 
+    // SART line weights: W_line = opInvert(FP(mask or 1)) (precomputeWeights,
+    // CudaSartAlgorithm.cpp:196-215); no pixel weights
+    b2t_status sart_weights(cudaStream_t s)
+    {
+        const float *vm = opt.vol_mask;
+        if (vm) {
+            B2T_TRY(op->fp(vm, lineW.as<float>(), 1.0f, B2T_MODE_SET, s));
+        } else {
+            B2T_TRY(vec_op_impl(B2T_OP_SET, tmpVol.as<float>(), nullptr, nullptr, 1.0f, nv(), s));
+            B2T_TRY(op->fp(tmpVol.as<float>(), lineW.as<float>(), 1.0f, B2T_MODE_SET, s));
+        }
+        return vec_op_impl(B2T_OP_INVERT, lineW.as<float>(), nullptr, nullptr, 0.0f, np(), s);
+    }
+
+    // one SART step: the view of the current step, then advance the counter
+    b2t_status sart_iteration(const float *sino, float *vol, cudaStream_t s)
+    {
+        const Op2D *o = static_cast<const Op2D *>(op.get());
+        const b2t_dims2d &d = o->g.dims;
+        b2t_status st;
+        const float *xv = masked(vol, tmpVol.as<float>(), s, st);
+        B2T_TRY(st);
+        SartResidualLaunch R;
+        R.vol = xv;
+        R.vol_pitch = d.vol_width;
+        R.sino = sino;
+        R.line_weight = lineW.as<float>();
+        R.r = sart_r.as<float>();
+        R.W = d.vol_width;
+        R.H = d.vol_height;
+        R.ndet = d.dets;
+        R.rays = (int)o->det_ss;
+        R.kind = o->g.kind;
+        R.out_scale = o->g.output_scale;
+        R.par = sart_par.as<ParFPView>();
+        R.fan = sart_fan.as<b2t_view2d>();
+        R.order = sart_order.as<int>();
+        R.norder = sart_norder;
+        R.step = sart_step.as<long long>();
+        B2T_TRY(sart_residual_launch(R, s));
+        SartUpdateLaunch U;
+        U.vol = vol;
+        U.vol_pitch = d.vol_width;
+        U.r = sart_r.as<float>();
+        U.mask = opt.vol_mask;
+        U.W = d.vol_width;
+        U.H = d.vol_height;
+        U.ndet = d.dets;
+        U.kind = o->g.kind;
+        U.scale = opt.relaxation * o->g.output_scale;
+        U.use_min = opt.use_min;
+        U.use_max = opt.use_max;
+        U.min_value = opt.min_value;
+        U.max_value = opt.max_value;
+        U.views = sart_bpv.as<BPView2D>();
+        U.order = sart_order.as<int>();
+        U.norder = sart_norder;
+        U.step = sart_step.as<long long>();
+        B2T_TRY(sart_update_launch(U, s));
+        return sart_advance_launch(sart_step.as<long long>(), s);
+    }
+
     b2t_status iteration(const float *sino, float *vol, int parity, cudaStream_t s)
     {
         if (type == B2T_ALGO_SIRT) return sirt_iteration(sino, vol, s);
+        if (type == B2T_ALGO_SART) return sart_iteration(sino, vol, s);
         return cgls_iteration(vol, parity, s);
     }
 };
@@ -444,7 +513,7 @@ b2t_status algo_create(int32_t type, Operator *op_raw, const b2t_algo_options *o
     std::unique_ptr<Operator> op(op_raw);
     if (!out) return fail(B2T_ERR_INVALID_ARG, "b2t_algo_create: null output");
     *out = nullptr;
-    if (type != B2T_ALGO_SIRT && type != B2T_ALGO_CGLS)
+    if (type != B2T_ALGO_SIRT && type != B2T_ALGO_CGLS && type != B2T_ALGO_SART)
         return fail(B2T_ERR_INVALID_ARG, "b2t_algo_create: unknown algorithm type %d", type);
     std::unique_ptr<Algo> a(new Algo);
     a->type = type;
@@ -454,7 +523,10 @@ b2t_status algo_create(int32_t type, Operator *op_raw, const b2t_algo_options *o
         a->opt.relaxation = 1.0f;
     }
     const size_t vb = a->nv() * sizeof(float), pb = a->np() * sizeof(float);
-    if (type == B2T_ALGO_SIRT) {
+    if (type == B2T_ALGO_SART) {
+        B2T_TRY(a->lineW.alloc(pb, "SART line weights"));
+        B2T_TRY(a->tmpVol.alloc(vb, "SART volume buffer"));
+    } else if (type == B2T_ALGO_SIRT) {
         B2T_TRY(a->lineW.alloc(pb, "SIRT line weights"));
         B2T_TRY(a->pixW.alloc(vb, "SIRT pixel weights"));
         B2T_TRY(a->tmpProj.alloc(pb, "SIRT projection buffer"));
@@ -487,11 +559,78 @@ b2t_status algo_create3d_impl(int32_t type, const b2t_geom3d *geom, const b2t_pa
     return algo_create(type, new Op3D(geom, params), opt, out);
 }
 
+// Device tables of SART: per-view FP and BP_SART constants, the sequential
+// projection order, the step counter (CudaSartAlgorithm.cpp:67-110).
+static b2t_status sart_setup(Algo *a, const Op2D *o)
+{
+    const b2t_dims2d &d = o->g.dims;
+    const uint32_t na = d.angles;
+    std::vector<ParFPView> par(na);
+    std::vector<BPView2D> bpv(na);
+    std::vector<int> order(na);
+    for (uint32_t i = 0; i < na; ++i) {
+        if (o->g.kind == B2T_GEOM_PAR2D) par_fp_view(o->g.views[i], d, o->g.output_scale, par[i]);
+        bp2d_view(o->g.kind, 0, o->g.views[i], bpv[i]);
+        order[i] = (int)i;
+    }
+    B2T_TRY(a->sart_par.alloc(sizeof(ParFPView) * na, "SART view table"));
+    B2T_TRY(a->sart_fan.alloc(sizeof(b2t_view2d) * na, "SART view table"));
+    B2T_TRY(a->sart_bpv.alloc(sizeof(BPView2D) * na, "SART view table"));
+    B2T_TRY(a->sart_order.alloc(sizeof(int) * na, "SART projection order"));
+    B2T_TRY(a->sart_step.alloc(sizeof(long long), "SART step counter"));
+    B2T_TRY(a->sart_r.alloc(sizeof(float) * d.dets, "SART residual row"));
+    B2T_CUDA_TRY(cudaMemcpy(a->sart_par.p, par.data(), sizeof(ParFPView) * na, cudaMemcpyHostToDevice), "SART upload");
+    B2T_CUDA_TRY(cudaMemcpy(a->sart_fan.p, o->g.views, sizeof(b2t_view2d) * na, cudaMemcpyHostToDevice), "SART upload");
+    B2T_CUDA_TRY(cudaMemcpy(a->sart_bpv.p, bpv.data(), sizeof(BPView2D) * na, cudaMemcpyHostToDevice), "SART upload");
+    B2T_CUDA_TRY(cudaMemcpy(a->sart_order.p, order.data(), sizeof(int) * na, cudaMemcpyHostToDevice), "SART upload");
+    a->sart_norder = (int)na;
+    return B2T_OK;
+}
+
 b2t_status algo_create2d_impl(int32_t type, const b2t_geom2d *geom, uint32_t det_ss, uint32_t pix_ss,
                               const b2t_algo_options *opt, b2t_algo **out)
 {
     B2T_TRY(validate2d(geom, "b2t_algo_create2d"));
-    return algo_create(type, new Op2D(geom, det_ss ? det_ss : 1, pix_ss ? pix_ss : 1), opt, out);
+    if (type == B2T_ALGO_SART) {
+        if (pix_ss > 1) return fail(B2T_ERR_UNSUPPORTED, "SART_CUDA: no pixel supersampling (BP_SART, par_bp.cu:265)");
+        if (opt && opt->sino_mask)
+            return fail(B2T_ERR_UNSUPPORTED, "SART_CUDA: Sinogram mask option is not supported");
+        if (opt && (opt->min_mask || opt->max_mask))
+            return fail(B2T_ERR_UNSUPPORTED, "SART_CUDA: per-pixel bounds are not supported");
+    }
+    B2T_TRY(algo_create(type, new Op2D(geom, det_ss ? det_ss : 1, pix_ss ? pix_ss : 1), opt, out));
+    if (type == B2T_ALGO_SART) {
+        Algo *a = reinterpret_cast<Algo *>(*out);
+        const b2t_status st = sart_setup(a, static_cast<const Op2D *>(a->op.get()));
+        if (st != B2T_OK) {
+            delete a;
+            *out = nullptr;
+            return st;
+        }
+    }
+    return B2T_OK;
+}
+
+b2t_status algo_set_order_impl(b2t_algo *h, const int32_t *order, uint32_t n)
+{
+    Algo *a = reinterpret_cast<Algo *>(h);
+    if (!a || !order || n == 0) return fail(B2T_ERR_INVALID_ARG, "b2t_algo_set_projection_order: null or empty order");
+    if (a->type != B2T_ALGO_SART)
+        return fail(B2T_ERR_INVALID_ARG, "b2t_algo_set_projection_order: the algorithm is not SART");
+    const uint32_t na = static_cast<const Op2D *>(a->op.get())->g.dims.angles;
+    for (uint32_t i = 0; i < n; ++i)
+        if (order[i] < 0 || (uint32_t)order[i] >= na)
+            return fail(B2T_ERR_INVALID_ARG, "b2t_algo_set_projection_order: view %d outside 0..%u", order[i], na - 1);
+    DevBuf nb;
+    B2T_TRY(nb.alloc(sizeof(int) * n, "SART projection order"));
+    B2T_CUDA_TRY(cudaMemcpy(nb.p, order, sizeof(int) * n, cudaMemcpyHostToDevice), "SART order upload");
+    std::swap(a->sart_order.p, nb.p);
+    a->sart_norder = (int)n;
+    if (a->graph) {  // the captured step holds the old order's address
+        cudaGraphExecDestroy(a->graph);
+        a->graph = nullptr;
+    }
+    return B2T_OK;
 }
 
 b2t_status algo_create_batch2d_impl(int32_t type, Batch2D *batch, const b2t_algo_options *opt, b2t_algo **out)
@@ -512,6 +651,12 @@ b2t_status algo_run_impl(b2t_algo *h, const float *sino, float *vol, int32_t ite
         // masks change the weights: recompute them every run (CudaSirtAlgorithm3D.cpp:340-341)
         if (!a->weights_ready || a->opt.vol_mask || a->opt.sino_mask) {
             B2T_TRY(a->sirt_weights(s));
+            a->weights_ready = true;
+        }
+    } else if (a->type == B2T_ALGO_SART) {
+        // with a mask the weights follow it every run (CudaSartAlgorithm.cpp:265-269)
+        if (!a->weights_ready || a->opt.vol_mask) {
+            B2T_TRY(a->sart_weights(s));
             a->weights_ready = true;
         }
     } else {
@@ -573,7 +718,7 @@ b2t_status algo_residual_impl(b2t_algo *h, const float *sino, const float *vol, 
     if (!a || !sino || !vol || !norm) return fail(B2T_ERR_INVALID_ARG, "b2t_algo_residual_norm: null argument");
     float *tp = a->tmpProj.as<float>();
     b2t_status st;
-    float *tv = (a->type == B2T_ALGO_SIRT) ? a->tmpVol.as<float>() : a->z.as<float>();
+    float *tv = (a->type == B2T_ALGO_CGLS) ? a->z.as<float>() : a->tmpVol.as<float>();
     const float *xv = a->masked(vol, tv, s, st);
     B2T_TRY(st);
     B2T_TRY(a->op->fp(xv, tp, 1.0f, B2T_MODE_SET, s));

@@ -199,6 +199,12 @@ b2t_status b2t_algo_residual_norm(b2t_algo *algo, const float *sino, const float
     return algo_residual_impl(algo, sino, vol, norm, static_cast<cudaStream_t>(stream));
 }
 
+b2t_status b2t_algo_set_projection_order(b2t_algo *algo, const int32_t *order, uint32_t n)
+{
+    clear_error();
+    return algo_set_order_impl(algo, order, n);
+}
+
 void b2t_algo_abort(b2t_algo *algo) { algo_abort_impl(algo); }
 
 void b2t_algo_destroy(b2t_algo *algo) { algo_destroy_impl(algo); }

@@ -27,28 +27,30 @@ __device__ __forceinline__ float lerp_line(const float *__restrict__ p, long lon
     return fmaf(f, b - a, a);
 }
 
-// Parallel-beam line integral of detector `det` (R sub-rays), scaled.
+// Parallel-beam line integral of detector `det` (R sub-rays), scaled; over
+// slices s0, s0 + ds, ... (all slices by default; a partial sum otherwise).
 __device__ __forceinline__ float fp2d_par_ray(const float *vol, long long pitch, int W, int H, const ParFPView &V,
-                                              int det, int R)
+                                              int det, int R, int s0 = 0, int ds = 1)
 {
     float acc = 0.0f;
     for (int r = 0; r < R; ++r) {
         const float p0 = fmaf((float)det + (0.5f + (float)r) / (float)R - 0.5f, V.detstep, V.p0);
         if (!V.vertical) {
             // slices are columns; the sample moves along the rows
-            for (int sl = 0; sl < W; ++sl)
+            for (int sl = s0; sl < W; sl += ds)
                 acc += lerp_line(vol + sl, pitch, H, fmaf((float)sl, V.slicestep, p0) - 0.5f);
         } else {
-            for (int sl = 0; sl < H; ++sl)
+            for (int sl = s0; sl < H; sl += ds)
                 acc += lerp_line(vol + (long long)sl * pitch, 1, W, fmaf((float)sl, V.slicestep, p0) - 0.5f);
         }
     }
     return acc * (V.corr / (float)R);
 }
 
-// Fan-beam line integral of detector `det` (R sub-rays), scaled.
+// Fan-beam line integral of detector `det` (R sub-rays), scaled; over slices
+// s0, s0 + ds, ... as fp2d_par_ray.
 __device__ __forceinline__ float fp2d_fan_ray(const float *vol, long long pitch, int W, int H, const b2t_view2d &V,
-                                              int det, int R, float out_scale)
+                                              int det, int R, float out_scale, int s0 = 0, int ds = 1)
 {
     // per-ray orientation choice, in float as the reference evaluates it
     const float fdx = fabsf(fmaf((float)det, V.det_u[0], V.det_s[0]) + 0.5f - V.src[0]);
@@ -67,14 +69,14 @@ __device__ __forceinline__ float fp2d_fan_ray(const float *vol, long long pitch,
             corr = (float)(sqrt(alpha * alpha + 1.0) * out_scale / R);
             const float y0 = (float)(-alpha * (0.5 - 0.5 * W) - beta + 0.5 * H - 0.5);
             const float dy = (float)-alpha;
-            for (int sl = 0; sl < W; ++sl) sum += lerp_line(vol + sl, pitch, H, fmaf((float)sl, dy, y0));
+            for (int sl = s0; sl < W; sl += ds) sum += lerp_line(vol + sl, pitch, H, fmaf((float)sl, dy, y0));
         } else {
             const double alpha = (V.src[0] - DX) / (V.src[1] - DY);
             const double beta = V.src[0] - alpha * V.src[1];
             corr = (float)(sqrt(alpha * alpha + 1.0) * out_scale / R);
             const float x0 = (float)(-alpha * (0.5 - 0.5 * H) + beta + 0.5 * W - 0.5);
             const float dx = (float)-alpha;
-            for (int sl = 0; sl < H; ++sl)
+            for (int sl = s0; sl < H; sl += ds)
                 sum += lerp_line(vol + (long long)sl * pitch, 1, W, fmaf((float)sl, dx, x0));
         }
         acc = fmaf(sum, corr, acc);

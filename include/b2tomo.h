@@ -381,10 +381,10 @@ b2t_status b2t_dot_f64_noalloc(const void *a, const void *b, size_t n, int32_t d
                                void *stream);
 
 /* ---------------------------------------------------------------------- */
-/* SIRT / CGLS reconstruction                                              */
+/* SIRT / CGLS / SART reconstruction                                       */
 /* ---------------------------------------------------------------------- */
 
-enum { B2T_ALGO_SIRT = 1, B2T_ALGO_CGLS = 2 };
+enum { B2T_ALGO_SIRT = 1, B2T_ALGO_CGLS = 2, B2T_ALGO_SART = 3 /* 2D only */ };
 
 /* Options of SIRT3D_CUDA / CGLS3D_CUDA / SIRT_CUDA / CGLS_CUDA
  * (src/ReconstructionAlgorithm3D.cpp:95-120, CudaSirtAlgorithm3D.cpp:141).
@@ -408,7 +408,11 @@ typedef struct b2t_algo b2t_algo;  /* opaque: operator, weights, work buffers */
  * src/CudaCglsAlgorithm3D.cpp).  Allocates the work buffers (cudaMalloc). */
 b2t_status b2t_algo_create3d(int32_t type, const b2t_geom3d *geom, const b2t_params3d *params,
                              const b2t_algo_options *options, b2t_algo **out);
-/* SIRT_CUDA / CGLS_CUDA (src/CudaSirtAlgorithm.cpp, src/CudaCglsAlgorithm.cpp). */
+/* SIRT_CUDA / CGLS_CUDA / SART_CUDA (src/CudaSirtAlgorithm.cpp,
+ * src/CudaCglsAlgorithm.cpp, src/CudaSartAlgorithm.cpp).  SART: one iteration
+ * is one view (in the order of b2t_algo_set_projection_order, sequential by
+ * default); "relaxation" is its lambda; no sinogram mask, no per-pixel bounds
+ * and no pixel supersampling, as the reference. */
 b2t_status b2t_algo_create2d(int32_t type, const b2t_geom2d *geom, uint32_t det_supersample,
                              uint32_t pixel_supersample, const b2t_algo_options *options, b2t_algo **out);
 /* run(iterations) (CudaSirtAlgorithm3D.cpp:301-381, CudaCglsAlgorithm3D.cpp:264-355):
@@ -421,6 +425,11 @@ b2t_status b2t_algo_run(b2t_algo *algo, const float *sino, float *vol, int32_t i
  * accumulated in FP64; synchronises the stream. */
 b2t_status b2t_algo_residual_norm(b2t_algo *algo, const float *sino, const float *vol, double *norm,
                                   void *stream);
+/* SART's projection order (CudaSartAlgorithm.cpp:76-109, "ProjectionOrder" /
+ * "ProjectionOrderList"): n view indices, used cyclically from the
+ * algorithm's running step count.  B2T_ERR_INVALID_ARG for other algorithms
+ * or out-of-range views. */
+b2t_status b2t_algo_set_projection_order(b2t_algo *algo, const int32_t *order, uint32_t n);
 /* Ask a running b2t_algo_run (on another thread) to stop between iterations
  * (astra::shouldAbort, src/Globals.cpp:49-58). */
 void b2t_algo_abort(b2t_algo *algo);

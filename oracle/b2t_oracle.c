@@ -998,4 +998,97 @@ void orc_fan_bp(const float *views, long na, long ndet, long W, long H, double o
 }
 
 /* Version tag so the loader can check it picked up this build. */
+/* ------------------------------------------------------------------------- */
+/* 2D SART (src/CudaSartAlgorithm.cpp, cuda/2d/sart.cu)                        */
+/* ------------------------------------------------------------------------- */
+
+/* Linear interpolation of a row at index q with clamp-to-edge addressing (the
+ * texture BP_SART binds with cudaAddressModeClamp, par_bp.cu:270). */
+static double orc_lerp_clamp(const double *row, long n, double q, int tex8)
+{
+    double f = floor(q);
+    long k = (long)f;
+    double a = orc_frac_weight(q - f, tex8);
+    long k0 = k < 0 ? 0 : (k >= n ? n - 1 : k);
+    long k1 = k + 1 < 0 ? 0 : (k + 1 >= n ? n - 1 : k + 1);
+    return (1.0 - a) * row[k0] + a * row[k1];
+}
+
+/*
+ * SART_CUDA: `iterations` single-view steps (CCudaSartAlgorithm::run,
+ * src/CudaSartAlgorithm.cpp:233-318).  Step it uses view
+ * order[(iter0 + it) % norder] (sequential when order is NULL):
+ *   r = (b_a - FP_a(x * mask)) * W_line[a]      FP_SART + mul_SART
+ *   x += lambda * out_scale * mask * BP_SART_a(r)
+ *   x = clamp(x)                                 opClampMin / opClampMax
+ * W_line = opInvert(FP(mask or 1)) over all views (precomputeWeights,
+ * :196-215; threshold cuda/2d/arith.cu:99-106).  BP_SART reads r with clamped
+ * addressing and no adjoint weight (devBP_SART par_bp.cu:139-159 with
+ * BP_SART :261-299; devFanBP_SART fan_bp.cu:164-201, constants with the
+ * non-FBP scale).  kind: 3 parallel, 4 fan.  vol (float, W x H) is updated.
+ */
+int orc_sart2d(int kind, const float *views, long na, long ndet, long W, long H, double out_scale, int rays_per_det,
+               const int *order, long norder, long iter0, long iterations, double lambda, int use_min,
+               double min_value, int use_max, double max_value, int tex8, const float *sino,
+               const float *vol_mask, float *vol)
+{
+    if (kind != 3 && kind != 4) return 1;
+    const long N = W * H;
+    float *src = (float *)malloc(sizeof(float) * (size_t)N);
+    double *lw = (double *)malloc(sizeof(double) * (size_t)(na * ndet));
+    double *row = (double *)malloc(sizeof(double) * (size_t)ndet);
+    for (long i = 0; i < N; ++i) src[i] = vol_mask ? vol_mask[i] : 1.0f;
+    if (kind == 3) orc_par_fp(views, na, ndet, W, H, 1.0 * out_scale, rays_per_det, tex8, src, lw);
+    else orc_fan_fp(views, na, ndet, W, H, out_scale, rays_per_det, tex8, src, lw);
+    for (long i = 0; i < na * ndet; ++i) {
+        float v = (float)lw[i];
+        lw[i] = (v > 0.000001f) ? 1.0 / (double)v : 0.0;
+    }
+    for (long it = 0; it < iterations; ++it) {
+        long a = order ? order[(iter0 + it) % norder] : (iter0 + it) % na;
+        const float *p = views + 6 * a;
+        for (long i = 0; i < N; ++i) src[i] = vol_mask ? vol[i] * vol_mask[i] : vol[i];
+        if (kind == 3) orc_par_fp(p, 1, ndet, W, H, out_scale, rays_per_det, tex8, src, row);
+        else orc_fan_fp(p, 1, ndet, W, H, out_scale, rays_per_det, tex8, src, row);
+        for (long d = 0; d < ndet; ++d) row[d] = ((double)sino[a * ndet + d] - row[d]) * lw[a * ndet + d];
+        double c[6];
+        if (kind == 3) {
+            double dd = (double)p[4] * p[1] - (double)p[5] * p[0];
+            c[0] = p[1] / dd;
+            c[1] = -p[0] / dd;
+            c[2] = ((double)p[3] * p[0] - (double)p[2] * p[1]) / dd;
+        } else {
+            double ux = p[4], uy = p[5], sx = p[0], sy = p[1], dx = p[2], dy = p[3];
+            double scale = sqrt(ux * ux + uy * uy) / (ux * (sy - dy) - uy * (sx - dx));
+            c[0] = scale * (sx * dy - sy * dx);
+            c[1] = scale * (sy - dy);
+            c[2] = -scale * (sx - dx);
+            c[3] = scale * (ux * sy - uy * sx);
+            c[4] = scale * uy;
+            c[5] = -scale * ux;
+        }
+        for (long Y = 0; Y < H; ++Y) {
+            for (long X = 0; X < W; ++X) {
+                double x = X - 0.5 * W + 0.5, y = Y - 0.5 * H + 0.5, T;
+                if (kind == 3) {
+                    T = x * c[0] - y * c[1] + c[2];
+                } else {
+                    double yw = -y;
+                    T = (c[0] + c[1] * x + c[2] * yw) / (c[3] + c[4] * x + c[5] * yw);
+                }
+                double u = lambda * out_scale * orc_lerp_clamp(row, ndet, T - 0.5, tex8);
+                if (vol_mask) u *= vol_mask[Y * W + X];
+                float nv = (float)((double)vol[Y * W + X] + u);
+                if (use_min && nv < (float)min_value) nv = (float)min_value;
+                if (use_max && nv > (float)max_value) nv = (float)max_value;
+                vol[Y * W + X] = nv;
+            }
+        }
+    }
+    free(src);
+    free(lw);
+    free(row);
+    return 0;
+}
+
 int orc_version(void) { return 1; }

@@ -54,6 +54,7 @@ def lib():
         L.orc_par_bp.argtypes = [_P, _L, _L, _L, _L, _D, _I, _I, _P, _P]
         L.orc_fan_fp.argtypes = [_P, _L, _L, _L, _L, _D, _I, _I, _P, _P]
         L.orc_fan_bp.argtypes = [_P, _L, _L, _L, _L, _D, _I, _I, _I, _P, _P]
+        L.orc_sart2d.argtypes = [_I, _P, _L, _L, _L, _L, _D, _I, _P, _L, _L, _L, _D, _I, _D, _I, _D, _I, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -362,4 +363,24 @@ def fan_bp(views, sino, vol_shape, out_scale=1.0, rays=1, fbp=False, tex8=False)
     vol = np.zeros(vol_shape, dtype=np.float64)
     lib().orc_fan_bp(views.ctypes.data, na, ndet, W, H, out_scale, rays, int(fbp), int(tex8),
                      sino.ctypes.data, vol.ctypes.data)
+    return vol
+
+
+def sart2d(kind, views, sino, vol0, out_scale, iterations, order=None, iter0=0, lam=1.0, min_value=None,
+           max_value=None, mask=None, rays=1, tex8=False):
+    """SART_CUDA's single-view steps (kind 3 parallel, 4 fan) from vol0;
+    returns the float32 volume (the state is float, as in the reference)."""
+    views = _c(views, np.float32)
+    sino = _c(sino, np.float32)
+    na, ndet = sino.shape
+    vol = np.array(vol0, dtype=np.float32, copy=True, order='C')
+    H, W = vol.shape
+    o = None if order is None else _c(order, np.int32)
+    m = None if mask is None else _c(mask, np.float32)
+    rc = lib().orc_sart2d(kind, views.ctypes.data, na, ndet, W, H, out_scale, rays,
+                          None if o is None else o.ctypes.data, 0 if o is None else o.size, iter0, iterations,
+                          lam, int(min_value is not None), float(min_value or 0.0), int(max_value is not None),
+                          float(max_value or 0.0), int(tex8), sino.ctypes.data,
+                          None if m is None else m.ctypes.data, vol.ctypes.data)
+    assert rc == 0
     return vol

@@ -36,6 +36,7 @@ def lib():
         L.ref_cuda_fp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _P, _P]
         L.ref_cuda_bp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _I, _P, _P]
         L.ref_gen_filter.argtypes = [_I, _F, _F, _I, _P]
+        L.ref_sart2d.argtypes = [_I, _I, _I, _P, _I, _I, _F, _P, _F, _F, _P, _P, _P, _I, _I, _F, _I, _F]
         _lib = L
     return _lib
 
@@ -188,6 +189,35 @@ def cuda_bp2d(kind, views, sino, vol_shape, out_scale=1.0, rays=1, fbp=False):
                              sino.data_ptr(), vol.data_ptr())
     assert rc == 0
     torch.cuda.synchronize()
+    return vol
+
+
+def sart2d(vol_geom, proj_geom, sino, vol0, iterations, min_value=None, max_value=None):
+    """Reference SART_CUDA (sequential order, relaxation 1) on host arrays;
+    returns the updated volume.  Runs the reference's CUDA code: needs a GPU."""
+    t = proj_geom['type']
+    o = vol_geom['option']
+    win = np.array([o['WindowMinX'], o['WindowMaxX'], o['WindowMinY'], o['WindowMaxY']], dtype=np.float32)
+    ndet = proj_geom['DetectorCount']
+    if 'Vectors' in proj_geom:
+        vec = np.ascontiguousarray(proj_geom['Vectors'], dtype=np.float64)
+        na = vec.shape[0]
+        ang = np.zeros(1, dtype=np.float32)
+        w = sod = odd = 0.0
+    else:
+        ang = np.ascontiguousarray(proj_geom['ProjectionAngles'], dtype=np.float32).ravel()
+        na = ang.size
+        vec = np.zeros(6, dtype=np.float64)
+        w = proj_geom['DetectorWidth']
+        sod = proj_geom.get('DistanceOriginSource', 0.0)
+        odd = proj_geom.get('DistanceOriginDetector', 0.0)
+    sino = np.ascontiguousarray(sino, dtype=np.float32)
+    vol = np.array(vol0, dtype=np.float32, copy=True, order='C')
+    rc = lib().ref_sart2d(GEOM2D_TYPES[t], vol_geom['GridColCount'], vol_geom['GridRowCount'], win.ctypes.data, na,
+                          ndet, w, ang.ctypes.data, sod, odd, vec.ctypes.data, sino.ctypes.data, vol.ctypes.data,
+                          iterations, int(min_value is not None), float(min_value or 0.0),
+                          int(max_value is not None), float(max_value or 0.0))
+    assert rc == 0
     return vol
 
 

@@ -14,6 +14,8 @@
 //   astraCUDA3d::FDK                 cuda/3d/fdk.cu:415
 //   astraCUDA::FP / FanFP            cuda/2d/par_fp.cu:340, fan_fp.cu:260
 //   astraCUDA::BP / FanBP            cuda/2d/par_bp.cu:224, fan_bp.cu:380
+//   astra::CCudaSartAlgorithm        src/CudaSartAlgorithm.cpp (C++ initialize: sequential
+//                                    projection order, relaxation 1)
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -23,6 +25,8 @@
 #include "astra/cuda/3d/util3d.h"
 #include "astra/cuda/3d/dims3d.h"
 #include "astra/ConeProjectionGeometry3D.h"
+#include "astra/CudaSartAlgorithm.h"
+#include "astra/Data2D.h"
 #include "astra/ConeVecProjectionGeometry3D.h"
 #include "astra/FanFlatProjectionGeometry2D.h"
 #include "astra/FanFlatVecProjectionGeometry2D.h"
@@ -168,11 +172,10 @@ int ref_geom3d(int type, int cols, int rows, int slices, const float *window, in
 }
 
 // type: 0 parallel, 1 fanflat, 2 parallel_vec, 3 fanflat_vec.  window: min_x, max_x, min_y, max_y.
-int ref_geom2d(int type, int cols, int rows, const float *window, int na, int ndet, float width,
-               const float *angles, float sod, float odd, const double *vecs, float *out_views,
-               float *out_scale)
+static std::unique_ptr<CProjectionGeometry2D> make_proj_geom2d(int type, int na, int ndet, float width,
+                                                               const float *angles, float sod, float odd,
+                                                               const double *vecs)
 {
-    CVolumeGeometry2D vg(cols, rows, window[0], window[2], window[1], window[3]);
     std::unique_ptr<CProjectionGeometry2D> pg;
     if (type == 0 || type == 1) {
         std::vector<float32> a(angles, angles + na);
@@ -199,6 +202,15 @@ int ref_geom2d(int type, int cols, int rows, const float *window, int na, int nd
         }
         pg.reset(new CFanFlatVecProjectionGeometry2D(na, ndet, std::move(v)));
     }
+    return pg;
+}
+
+int ref_geom2d(int type, int cols, int rows, const float *window, int na, int ndet, float width,
+               const float *angles, float sod, float odd, const double *vecs, float *out_views,
+               float *out_scale)
+{
+    CVolumeGeometry2D vg(cols, rows, window[0], window[2], window[1], window[3]);
+    std::unique_ptr<CProjectionGeometry2D> pg = make_proj_geom2d(type, na, ndet, width, angles, sod, odd, vecs);
     Geometry2DParameters g = convertAstraGeometry(&vg, pg.get());
     if (!g.isValid()) return 1;
     for (int i = 0; i < na; ++i) {
@@ -212,6 +224,26 @@ int ref_geom2d(int type, int cols, int rows, const float *window, int na, int nd
         }
     }
     *out_scale = g.getOutputScale();
+    return 0;
+}
+
+// SART_CUDA on host buffers: sino (na, ndet), vol (rows, cols) updated in
+// place by `iterations` single-angle steps in sequential order.
+int ref_sart2d(int type, int cols, int rows, const float *window, int na, int ndet, float width,
+               const float *angles, float sod, float odd, const double *vecs, const float *sino, float *vol,
+               int iterations, int use_min, float min_value, int use_max, float max_value)
+{
+    CVolumeGeometry2D vg(cols, rows, window[0], window[2], window[1], window[3]);
+    std::unique_ptr<CProjectionGeometry2D> pg = make_proj_geom2d(type, na, ndet, width, angles, sod, odd, vecs);
+    std::unique_ptr<CFloat32ProjectionData2D> S(createCFloat32ProjectionData2DMemory(*pg));
+    std::unique_ptr<CFloat32VolumeData2D> V(createCFloat32VolumeData2DMemory(vg));
+    std::memcpy(S->getFloat32Memory(), sino, sizeof(float) * (size_t)na * ndet);
+    std::memcpy(V->getFloat32Memory(), vol, sizeof(float) * (size_t)rows * cols);
+    CCudaSartAlgorithm alg;
+    if (!alg.initialize(nullptr, S.get(), V.get())) return 1;
+    alg.setConstraints(use_min != 0, min_value, use_max != 0, max_value);
+    if (!alg.run(iterations)) return 2;
+    std::memcpy(vol, V->getFloat32Memory(), sizeof(float) * (size_t)rows * cols);
     return 0;
 }
 

@@ -249,3 +249,81 @@ def test_optomo_matches_projector_and_solves(astra, orc):
     assert np.linalg.norm(W.matvec(sol) - s.ravel()) < 0.2 * np.linalg.norm(s)
     rec = W.reconstruct('SIRT_CUDA', s, 20)
     assert rec.shape == pr.vol_shape and np.isfinite(rec).all()
+
+
+def _fan2d_setup(astra):
+    ang = np.linspace(0, 2 * np.pi, 50, endpoint=False).astype(np.float32)
+    vg = astra.create_vol_geom(36, 40)
+    pg = astra.create_proj_geom('fanflat', 1.2, 70, ang, 110.0, 50.0)
+    return vg, pg
+
+
+@pytest.mark.parametrize("geom", ["parallel", "fanflat"])
+def test_sart2d_vs_oracle(astra, orc, geom):
+    """SART_CUDA, sequential order, two sweeps, min constraint and relaxation,
+    against the oracle's single-view steps (float state in both: 1e-4)."""
+    vg, pg = (_par2d_setup if geom == "parallel" else _fan2d_setup)(astra)
+    pr = astra.Projector2D(pg, vg)
+    kind = pr.geom.kind
+    views, sc = pr.geom.views_array(), pr.geom.output_scale
+    fp = orc.par_fp if kind == 3 else orc.fan_fp
+    x_true = np.random.default_rng(5).random(pr.vol_shape).astype(np.float32)
+    b = fp(views, x_true, pr.proj_shape[1], sc).astype(np.float32)
+    iters = 2 * pr.proj_shape[0]
+    opts = {'ProjectionOrder': 'sequential', 'MinConstraint': 0.0, 'Relaxation': 0.8}
+    got, res = _run(astra, vg, pg, False, 'SART_CUDA', b, iters, opts)
+    want = orc.sart2d(kind, views, b, np.zeros(pr.vol_shape), sc, iters, lam=0.8, min_value=0.0)
+    assert rel_l2(got, want) < 1e-4, rel_l2(got, want)
+    assert got.min() >= 0.0
+    assert abs(res - np.linalg.norm(b - fp(views, got, pr.proj_shape[1], sc))) < 1e-4 * np.linalg.norm(b)
+
+
+def test_sart2d_custom_order_runs_resume_and_graph(astra, orc):
+    """A custom ProjectionOrderList used cyclically; the step count carries
+    over between run() calls; the CUDA-graph replay gives identical results."""
+    vg, pg = _par2d_setup(astra)
+    pr = astra.Projector2D(pg, vg)
+    views, sc = pr.geom.views_array(), pr.geom.output_scale
+    x_true = np.random.default_rng(6).random(pr.vol_shape).astype(np.float32)
+    b = orc.par_fp(views, x_true, pr.proj_shape[1], sc).astype(np.float32)
+    order = np.random.default_rng(7).permutation(pr.proj_shape[0])[:25]
+    want = orc.sart2d(3, views, b, np.zeros(pr.vol_shape), sc, 70, order=order)
+    outs = []
+    for graph in (False, True):
+        sid = astra.data2d.create('-sino', pg, b)
+        rid = astra.data2d.create('-vol', vg, 0)
+        cfg = astra.astra_dict('SART_CUDA')
+        cfg['ProjectionDataId'] = sid
+        cfg['ReconstructionDataId'] = rid
+        cfg['option'] = {'ProjectionOrder': 'custom', 'ProjectionOrderList': order, 'UseGraph': graph}
+        aid = astra.algorithm.create(cfg)
+        astra.algorithm.run(aid, 30)
+        astra.algorithm.run(aid, 40)
+        outs.append(astra.data2d.get(rid))
+        astra.algorithm.delete(aid)
+        astra.data2d.delete([sid, rid])
+    assert rel_l2(outs[0], want) < 1e-4
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_sart2d_mask_and_refusals(astra, orc):
+    vg, pg = _fan2d_setup(astra)
+    pr = astra.Projector2D(pg, vg)
+    views, sc = pr.geom.views_array(), pr.geom.output_scale
+    x_true = np.random.default_rng(8).random(pr.vol_shape).astype(np.float32)
+    b = orc.fan_fp(views, x_true, pr.proj_shape[1], sc).astype(np.float32)
+    mask = np.zeros(pr.vol_shape, dtype=np.float32)
+    mask[5:30, 6:34] = 1.0
+    mid = astra.data2d.create('-vol', vg, mask)
+    got, _ = _run(astra, vg, pg, False, 'SART_CUDA', b, 50,
+                  {'ProjectionOrder': 'sequential', 'ReconstructionMaskId': mid})
+    want = orc.sart2d(4, views, b, np.zeros(pr.vol_shape), sc, 50, mask=mask)
+    assert rel_l2(got, want) < 1e-4
+    assert np.all(got[mask == 0] == 0.0)
+    sm = astra.data2d.create('-sino', pg, np.ones_like(b))
+    with pytest.raises(astra.AstraError):
+        _run(astra, vg, pg, False, 'SART_CUDA', b, 1, {'SinogramMaskId': sm})
+    with pytest.raises(astra.AstraError):
+        _run(astra, vg, pg, False, 'SART_CUDA', b, 1,
+             {'ProjectionOrder': 'custom', 'ProjectionOrderList': [0, 1, 999]})
+    astra.data2d.delete([mid, sm])
