@@ -20,7 +20,7 @@ STATUS_NAMES = {
 
 MODE_ADD, MODE_SET = 0, 1
 F32, F16, BF16 = 0, 1, 2
-GEOM_PAR3D, GEOM_CONE, GEOM_PAR2D, GEOM_FAN2D = 1, 2, 3, 4
+GEOM_PAR3D, GEOM_CONE, GEOM_PAR2D, GEOM_FAN2D, GEOM_CYLCONE = 1, 2, 3, 4, 5
 KER_DEFAULT, KER_SUM_SQUARE_WEIGHTS, KER_FDK_WEIGHTING, KER_2D_WEIGHTING, KER_MATCHED_BP = 0, 1, 2, 3, 4
 FILTER_NONE, FILTER_RAMLAK = 0, 1
 # E_FBPFILTER names (src/Filters.cpp:508-532) -> codes, in the reference's order
@@ -58,6 +58,15 @@ class Dims3D(ctypes.Structure):
 class Geom3D(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("dims", Dims3D), ("vol_scale", ctypes.c_float * 3),
                 ("views", ctypes.POINTER(View3D))]
+
+
+class View3DCyl(ctypes.Structure):
+    _fields_ = [("src", ctypes.c_double * 3), ("det_c", ctypes.c_double * 3), ("det_u", ctypes.c_double * 3),
+                ("det_v", ctypes.c_double * 3), ("radius", ctypes.c_double)]
+
+
+class Geom3DCyl(ctypes.Structure):
+    _fields_ = [("dims", Dims3D), ("vol_scale", ctypes.c_float * 3), ("views", ctypes.POINTER(View3DCyl))]
 
 
 class Params3D(ctypes.Structure):
@@ -126,6 +135,9 @@ SIGNATURES = {
     "b2t_normalize_views2d": (_I32, [_P, _I32, _U32, _P, _P]),
     "b2t_fp3d": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
     "b2t_bp3d": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
+    "b2t_normalize_views3d_cyl": (_I32, [_P, _U32, _P, _P]),
+    "b2t_fp3d_cyl": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _P]),
+    "b2t_bp3d_cyl": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _P]),
     "b2t_fp2d": (_I32, [_P, _U32, _P, _SZ, _P, _SZ, _I32, _P]),
     "b2t_bp2d": (_I32, [_P, _U32, _I32, _P, _SZ, _P, _SZ, _I32, _P]),
     "b2t_fdk": (_I32, [_P, _P, _I32, _F, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
@@ -134,6 +146,7 @@ SIGNATURES = {
     "b2t_filter_taps": (_I32, [_P, _U32, _U32, _P, _P]),
     "b2t_fbp2d": (_I32, [_P, _P, _I32, _P, _SZ, _P, _SZ, _I32, _P]),
     "b2t_algo_create3d": (_I32, [_I32, _P, _P, _P, _P]),
+    "b2t_algo_create3d_cyl": (_I32, [_I32, _P, _P, _P, _P]),
     "b2t_algo_create2d": (_I32, [_I32, _P, _U32, _U32, _P, _P]),
     "b2t_algo_run": (_I32, [_P, _P, _P, _I32, _I32, _P]),
     "b2t_algo_residual_norm": (_I32, [_P, _P, _P, _P, _P]),

@@ -146,7 +146,8 @@ class _Iterative(_Algorithm):
         self.use_graph = int(bool(o.get('UseGraph', False)))
         self.handle = ctypes.c_void_p()
         if is3d:
-            _lib.call("b2t_algo_create3d", kind, ctypes.byref(self.pr.geom.c), ctypes.byref(self.pr.params()),
+            create = "b2t_algo_create3d_cyl" if self.pr.is_cyl else "b2t_algo_create3d"
+            _lib.call(create, kind, ctypes.byref(self.pr.geom.c), ctypes.byref(self.pr.params()),
                       ctypes.byref(self.c_opt), ctypes.byref(self.handle))
         else:
             _lib.call("b2t_algo_create2d", kind, ctypes.byref(self.pr.geom.c), self.pr.det_ss, self.pr.pix_ss,

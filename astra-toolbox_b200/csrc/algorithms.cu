@@ -210,6 +210,33 @@ struct Op3D : Operator {
     }
 };
 
+// cyl_cone_vec geometry (cyl.cu): FP32, no supersampling; the BP is the
+// voxel-driven one or, with B2T_KER_MATCHED_BP, the FP's transpose
+struct Op3DCyl : Operator {
+    b2t_geom3d_cyl g;
+    std::vector<b2t_view3d_cyl> views;
+    b2t_params3d p;
+    Op3DCyl(const b2t_geom3d_cyl *geom, const b2t_params3d *params)
+        : g(*geom), views(geom->views, geom->views + geom->dims.angles), p(*params)
+    {
+        g.views = views.data();
+        nvol = (size_t)g.dims.vol_x * g.dims.vol_y * g.dims.vol_z;
+        nproj = (size_t)g.dims.det_u * g.dims.angles * g.dims.det_v;
+    }
+    b2t_status fp(const float *vol, float *proj, float scale, int mode, cudaStream_t s) override
+    {
+        b2t_params3d q = p;
+        q.output_scale *= scale;
+        return fp3d_cyl_impl(&g, &q, vol, 0, proj, 0, mode, s);
+    }
+    b2t_status bp(const float *proj, float *vol, float scale, int mode, cudaStream_t s) override
+    {
+        b2t_params3d q = p;
+        q.output_scale *= scale;
+        return bp3d_cyl_impl(&g, &q, proj, 0, vol, 0, mode, s);
+    }
+};
+
 struct Op2D : Operator {
     b2t_geom2d g;
     std::vector<b2t_view2d> views;
@@ -554,6 +581,7 @@ b2t_status algo_create(int32_t type, Operator *op_raw, const b2t_algo_options *o
 b2t_status algo_create3d_impl(int32_t type, const b2t_geom3d *geom, const b2t_params3d *params,
                               const b2t_algo_options *opt, b2t_algo **out)
 {
+    if (type == B2T_ALGO_SART) return fail(B2T_ERR_INVALID_ARG, "b2t_algo_create3d: SART is 2D only");
     B2T_TRY(validate3d(geom, "b2t_algo_create3d"));
     if (!params) return fail(B2T_ERR_INVALID_ARG, "b2t_algo_create3d: null params");
     return algo_create(type, new Op3D(geom, params), opt, out);
@@ -585,6 +613,17 @@ static b2t_status sart_setup(Algo *a, const Op2D *o)
     B2T_CUDA_TRY(cudaMemcpy(a->sart_order.p, order.data(), sizeof(int) * na, cudaMemcpyHostToDevice), "SART upload");
     a->sart_norder = (int)na;
     return B2T_OK;
+}
+
+b2t_status algo_create3d_cyl_impl(int32_t type, const b2t_geom3d_cyl *geom, const b2t_params3d *params,
+                                  const b2t_algo_options *opt, b2t_algo **out)
+{
+    if (!geom || !geom->views || !params) return fail(B2T_ERR_INVALID_ARG, "b2t_algo_create3d_cyl: null argument");
+    if (type == B2T_ALGO_SART) return fail(B2T_ERR_INVALID_ARG, "b2t_algo_create3d_cyl: SART is 2D only");
+    if (params->det_supersample > 1 || params->voxel_supersample > 1)
+        return fail(B2T_ERR_UNSUPPORTED,
+                    "Detector/voxel supersampling is not supported for cyl_cone_vec geometry.");
+    return algo_create(type, new Op3DCyl(geom, params), opt, out);
 }
 
 b2t_status algo_create2d_impl(int32_t type, const b2t_geom2d *geom, uint32_t det_ss, uint32_t pix_ss,

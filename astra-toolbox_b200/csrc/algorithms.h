@@ -12,6 +12,8 @@ namespace b2t {
 
 b2t_status algo_create3d_impl(int32_t type, const b2t_geom3d *geom, const b2t_params3d *params,
                               const b2t_algo_options *opt, b2t_algo **out);
+b2t_status algo_create3d_cyl_impl(int32_t type, const b2t_geom3d_cyl *geom, const b2t_params3d *params,
+                                  const b2t_algo_options *opt, b2t_algo **out);
 b2t_status algo_create2d_impl(int32_t type, const b2t_geom2d *geom, uint32_t det_ss, uint32_t pix_ss,
                               const b2t_algo_options *opt, b2t_algo **out);
 struct Batch2D;

@@ -127,6 +127,20 @@ b2t_status b2t_bp3d(const b2t_geom3d *geom, const b2t_params3d *params, const vo
                      static_cast<cudaStream_t>(stream));
 }
 
+b2t_status b2t_fp3d_cyl(const b2t_geom3d_cyl *geom, const b2t_params3d *params, const float *vol,
+                        size_t vol_pitch, float *proj, size_t proj_pitch, int32_t mode, void *stream)
+{
+    clear_error();
+    return fp3d_cyl_impl(geom, params, vol, vol_pitch, proj, proj_pitch, mode, static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_bp3d_cyl(const b2t_geom3d_cyl *geom, const b2t_params3d *params, const float *proj,
+                        size_t proj_pitch, float *vol, size_t vol_pitch, int32_t mode, void *stream)
+{
+    clear_error();
+    return bp3d_cyl_impl(geom, params, proj, proj_pitch, vol, vol_pitch, mode, static_cast<cudaStream_t>(stream));
+}
+
 b2t_status b2t_fp2d(const b2t_geom2d *geom, uint32_t det_supersample, const float *vol, size_t vol_pitch, float *sino,
                     size_t sino_pitch, int32_t mode, void *stream)
 {
@@ -177,6 +191,13 @@ b2t_status b2t_algo_create3d(int32_t type, const b2t_geom3d *geom, const b2t_par
 {
     clear_error();
     return algo_create3d_impl(type, geom, params, options, out);
+}
+
+b2t_status b2t_algo_create3d_cyl(int32_t type, const b2t_geom3d_cyl *geom, const b2t_params3d *params,
+                                 const b2t_algo_options *options, b2t_algo **out)
+{
+    clear_error();
+    return algo_create3d_cyl_impl(type, geom, params, options, out);
 }
 
 b2t_status b2t_algo_create2d(int32_t type, const b2t_geom2d *geom, uint32_t det_supersample,

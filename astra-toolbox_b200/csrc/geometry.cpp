@@ -160,6 +160,40 @@ extern "C" b2t_status b2t_normalize_views3d(const b2t_volgeom3d *vol, int32_t ki
     return B2T_OK;
 }
 
+// convertAstraGeometry_unscaled_internal (src/GeometryUtil3D.cpp:597-617):
+// the cylindrical-detector views are translated (source and detector centre)
+// but not scaled; the voxel size travels separately.
+extern "C" b2t_status b2t_normalize_views3d_cyl(const b2t_volgeom3d *vol, uint32_t n, b2t_view3d_cyl *views,
+                                                float *vol_scale_out)
+{
+    clear_error();
+    if (!vol || !views || !vol_scale_out) return fail(B2T_ERR_INVALID_ARG, "b2t_normalize_views3d_cyl: null pointer");
+    if (vol->cols == 0 || vol->rows == 0 || vol->slices == 0)
+        return fail(B2T_ERR_INVALID_ARG, "b2t_normalize_views3d_cyl: empty volume");
+    float pixX = (vol->max_x - vol->min_x) / (float)vol->cols;
+    float pixY = (vol->max_y - vol->min_y) / (float)vol->rows;
+    float pixZ = (vol->max_z - vol->min_z) / (float)vol->slices;
+    if (!(pixX > 0.0f) || !(pixY > 0.0f) || !(pixZ > 0.0f))
+        return fail(B2T_ERR_INVALID_ARG, "b2t_normalize_views3d_cyl: window min must be below max");
+    float dx = -(vol->min_x + vol->max_x) / 2;
+    float dy = -(vol->min_y + vol->max_y) / 2;
+    float dz = -(vol->min_z + vol->max_z) / 2;
+    for (uint32_t i = 0; i < n; ++i) {
+        b2t_view3d_cyl &p = views[i];
+        if (!(p.radius > 0.0)) return fail(B2T_ERR_INVALID_ARG, "b2t_normalize_views3d_cyl: radius must be > 0");
+        p.src[0] += dx;
+        p.src[1] += dy;
+        p.src[2] += dz;
+        p.det_c[0] += dx;
+        p.det_c[1] += dy;
+        p.det_c[2] += dz;
+    }
+    vol_scale_out[0] = pixX;
+    vol_scale_out[1] = pixY;
+    vol_scale_out[2] = pixZ;
+    return B2T_OK;
+}
+
 // ---------------------------------------------------------------------------
 // 2D
 // ---------------------------------------------------------------------------

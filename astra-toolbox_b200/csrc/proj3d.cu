@@ -423,6 +423,16 @@ b2t_status pad_volumes(const void *vol, size_t pitch, const b2t_dims3d &d, void 
     return B2T_OK;
 }
 
+}  // namespace
+
+b2t_status pad_volumes_f32(const float *vol, size_t pitch, const b2t_dims3d &d, float *xyz, float *zxy,
+                           cudaStream_t s)
+{
+    return pad_volumes<float>(vol, pitch, d, xyz, zxy, s);
+}
+
+namespace {
+
 template <typename T>
 b2t_status pad_projections(const void *proj, size_t pitch, const b2t_dims3d &d, void *pp,
                            cudaStream_t s)

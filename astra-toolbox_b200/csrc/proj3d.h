@@ -104,6 +104,14 @@ bool force_simple_fp();
 b2t_status fp3d_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch, void *proj,
                       size_t proj_pitch, int32_t dtype, int32_t mode, const std::vector<int> &dirs, cudaStream_t s);
 
+// Zero-padded FP32 volume copies (2-voxel border): xyz = [z+2][y+2][x+2],
+// zxy = [z+2][x+2][y+2] (either may be null).
+b2t_status pad_volumes_f32(const float *vol, size_t pitch, const b2t_dims3d &d, float *xyz, float *zxy,
+                           cudaStream_t s);
+b2t_status fp3d_cyl_impl(const b2t_geom3d_cyl *g, const b2t_params3d *p, const float *vol, size_t vol_pitch,
+                         float *proj, size_t proj_pitch, int32_t mode, cudaStream_t s);
+b2t_status bp3d_cyl_impl(const b2t_geom3d_cyl *g, const b2t_params3d *p, const float *proj, size_t proj_pitch,
+                         float *vol, size_t vol_pitch, int32_t mode, cudaStream_t s);
 b2t_status fp3d_sumsqw_impl(const b2t_geom3d *g, const b2t_params3d *p, void *proj, size_t proj_pitch,
                             int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status fp3d_autotune_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch,

@@ -5,8 +5,9 @@ python/astra/data3d_c.pyx, data2d_c.pyx).
 A data object holds a float32 torch tensor on the GPU (the reference keeps
 float32 host memory and copies it to the GPU per call; here the data stay
 resident).  Linked numpy arrays are mirrored on the device and written back
-after every operation that changes them; linked torch CUDA tensors are used in
-place (zero copy).
+after every operation that changes them; linked torch CUDA tensors, and CUDA
+arrays of other libraries passed through DLPack, are used in place (zero
+copy).
 """
 import itertools
 
@@ -62,6 +63,7 @@ class DataObject:
             self.shape = tuple(G.proj_shape(geometry))
         self.tensor = None
         self.host = None       # linked numpy array (written back after changes)
+        self.foreign = False   # linked through DLPack from another library
 
     def fill(self, data):
         dev = _device()
@@ -77,6 +79,13 @@ class DataObject:
             self.tensor = torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32)).to(dev)
 
     def link(self, data):
+        from .projector import dlpack_tensor
+        d, foreign = dlpack_tensor(data)
+        if foreign:
+            # another library's array (CuPy, JAX, ...): used in place through
+            # DLPack; results are synchronised in changed()
+            self.foreign = True
+            data = d
         if isinstance(data, torch.Tensor):
             if tuple(data.shape) != self.shape:
                 raise AstraError(1, "The dimensions of the data do not match those specified in the geometry")
@@ -101,9 +110,13 @@ class DataObject:
         self.tensor = torch.from_numpy(self.host).to(_device())
 
     def changed(self):
-        """Write device data back to a linked host array."""
+        """Write device data back to a linked host array; for data linked
+        through DLPack from another library, wait for the writes so that
+        library's streams see them."""
         if self.host is not None:
             self.host[...] = self.tensor.cpu().numpy()
+        elif self.foreign and self.tensor.is_cuda:
+            torch.cuda.current_stream(self.tensor.device).synchronize()
 
     def get(self):
         return self.tensor.cpu().numpy()

@@ -9,7 +9,8 @@ def create(datatype, geometry, data=None):
 
 
 def link(datatype, geometry, data):
-    """Link a float32 numpy array or torch tensor (CUDA tensors zero-copy)."""
+    """Link a float32 numpy array, torch tensor or DLPack object (CUDA data
+    zero-copy)."""
     return _d.create(datatype, geometry, data, link=True, dims3=True)
 
 

@@ -70,9 +70,10 @@ def create_vol_geom(*varargin):
 
 
 def create_proj_geom(intype, *args):
-    """Same call forms and dictionary as astra.create_proj_geom (flat-panel types)."""
+    """Same call forms and dictionary as astra.create_proj_geom (flat-panel
+    types and cyl_cone_vec)."""
     need = {'parallel': 3, 'parallel_vec': 2, 'fanflat': 5, 'fanflat_vec': 2,
-            'parallel3d': 5, 'cone': 7, 'cone_vec': 3, 'parallel3d_vec': 3}
+            'parallel3d': 5, 'cone': 7, 'cone_vec': 3, 'parallel3d_vec': 3, 'cyl_cone_vec': 3}
     if intype not in need:
         raise AstraError(2, "create_proj_geom: unsupported geometry type %r" % (intype,))
     if len(args) < need[intype]:
@@ -95,9 +96,10 @@ def create_proj_geom(intype, *args):
         return {'type': 'cone', 'DetectorSpacingX': args[0], 'DetectorSpacingY': args[1],
                 'DetectorRowCount': args[2], 'DetectorColCount': args[3], 'ProjectionAngles': args[4],
                 'DistanceOriginSource': args[5], 'DistanceOriginDetector': args[6]}
-    # cone_vec, parallel3d_vec
-    if args[2].shape[1] != 12:
-        raise AstraError(1, 'V should be a Nx12 matrix, with N the number of projections')
+    # cone_vec, parallel3d_vec (12 columns), cyl_cone_vec (13: the radius last)
+    ncol = 13 if intype == 'cyl_cone_vec' else 12
+    if np.asarray(args[2]).ndim != 2 or np.asarray(args[2]).shape[1] != ncol:
+        raise AstraError(1, 'V should be a Nx%d matrix, with N the number of projections' % ncol)
     return {'type': intype, 'DetectorRowCount': args[0], 'DetectorColCount': args[1], 'Vectors': args[2]}
 
 
@@ -125,7 +127,7 @@ def n_angles(proj_geom):
 def proj_shape(proj_geom):
     """numpy shape of projection data: (rows, angles, cols) in 3D, (angles, dets) in 2D."""
     t = proj_geom['type']
-    if t in ('parallel3d', 'cone', 'cone_vec', 'parallel3d_vec'):
+    if t in ('parallel3d', 'cone', 'cone_vec', 'parallel3d_vec', 'cyl_cone_vec'):
         return (proj_geom['DetectorRowCount'], n_angles(proj_geom), proj_geom['DetectorColCount'])
     return (n_angles(proj_geom), proj_geom['DetectorCount'])
 
@@ -140,10 +142,13 @@ class Geometry3D:
     def __init__(self, vol_geom, proj_geom):
         lib = _lib.load()
         t = proj_geom['type']
-        if t not in ('parallel3d', 'cone', 'cone_vec', 'parallel3d_vec'):
+        if t not in ('parallel3d', 'cone', 'cone_vec', 'parallel3d_vec', 'cyl_cone_vec'):
             raise AstraError(2, "3D projector needs a 3D projection geometry, got %r" % t)
         if not is_3d_vol(vol_geom):
             raise AstraError(1, "3D projector needs a 3D volume geometry")
+        if t == 'cyl_cone_vec':
+            self._init_cyl(vol_geom, proj_geom)
+            return
         self.kind = _lib.GEOM_CONE if t in ('cone', 'cone_vec') else _lib.GEOM_PAR3D
         rows, na, cols = proj_shape(proj_geom)
         views = (_lib.View3D * na)()
@@ -174,11 +179,38 @@ class Geometry3D:
         self.vol_shape = vol_shape(vol_geom)
         self.proj_shape = (rows, na, cols)
 
+    def _init_cyl(self, vol_geom, proj_geom):
+        """cyl_cone_vec: views translated to the volume centre, not scaled
+        (b2t_normalize_views3d_cyl); self.c is a b2t_geom3d_cyl."""
+        lib = _lib.load()
+        self.kind = _lib.GEOM_CYLCONE
+        rows, na, cols = proj_shape(proj_geom)
+        vec = np.ascontiguousarray(np.asarray(proj_geom['Vectors'], dtype=np.float64))
+        if vec.ndim != 2 or vec.shape != (na, 13):
+            raise AstraError(1, "cyl_cone_vec Vectors must be an (n, 13) array")
+        views = (_lib.View3DCyl * na)()
+        ctypes.memmove(views, vec.ctypes.data, vec.nbytes)
+        o = vol_geom['option']
+        vg = _lib.VolGeom3D(vol_geom['GridColCount'], vol_geom['GridRowCount'], vol_geom['GridSliceCount'],
+                            _f32(o['WindowMinX']), _f32(o['WindowMaxX']), _f32(o['WindowMinY']),
+                            _f32(o['WindowMaxY']), _f32(o['WindowMinZ']), _f32(o['WindowMaxZ']))
+        vs = (ctypes.c_float * 3)()
+        _lib.check(lib.b2t_normalize_views3d_cyl(ctypes.byref(vg), na, views, vs))
+        self.views = views
+        self.vol_scale = tuple(vs)
+        self.dims = _lib.Dims3D(vol_geom['GridColCount'], vol_geom['GridRowCount'], vol_geom['GridSliceCount'],
+                                na, cols, rows)
+        self.c = _lib.Geom3DCyl(self.dims, (ctypes.c_float * 3)(*vs), views)
+        self.vol_shape = vol_shape(vol_geom)
+        self.proj_shape = (rows, na, cols)
+
     def views_array(self):
-        """Per-view vectors as an (n, 12) float64 array (SConeProjection order)."""
+        """Per-view vectors as an (n, 12) float64 array (SConeProjection order),
+        (n, 13) for cyl_cone_vec (SCylConeProjection order)."""
         n = self.dims.angles
-        buf = (ctypes.c_double * (12 * n)).from_address(ctypes.addressof(self.views))
-        return np.array(buf, dtype=np.float64).reshape(n, 12)
+        w = 13 if self.kind == _lib.GEOM_CYLCONE else 12
+        buf = (ctypes.c_double * (w * n)).from_address(ctypes.addressof(self.views))
+        return np.array(buf, dtype=np.float64).reshape(n, w)
 
 
 class Geometry2D:

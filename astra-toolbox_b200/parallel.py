@@ -44,7 +44,7 @@ def shard_proj_geom(proj_geom, start, stop):
     g = copy.deepcopy(proj_geom)
     if t in ('cone', 'parallel3d'):
         g['ProjectionAngles'] = np.asarray(proj_geom['ProjectionAngles'])[start:stop].copy()
-    elif t in ('cone_vec', 'parallel3d_vec'):
+    elif t in ('cone_vec', 'parallel3d_vec', 'cyl_cone_vec'):
         g['Vectors'] = np.asarray(proj_geom['Vectors'])[start:stop].copy()
     else:
         raise AstraError(2, "angle sharding needs a 3D projection geometry, got %r" % t)

@@ -81,9 +81,23 @@ class Projector3D:
             raise AstraError(1, "volume and projection data must have the same dtype")
         p = self.params(output_scale, kernel)
         with torch.cuda.device(vol.device):
-            _lib.call("b2t_fp3d", ctypes.byref(self.geom.c), ctypes.byref(p), vol.data_ptr(), 0,
-                      proj.data_ptr(), 0, _DTYPES[vol.dtype], mode, stream_handle(vol.device))
+            if self.is_cyl:
+                self._cyl_f32(vol)
+                _lib.call("b2t_fp3d_cyl", ctypes.byref(self.geom.c), ctypes.byref(p), vol.data_ptr(), 0,
+                          proj.data_ptr(), 0, mode, stream_handle(vol.device))
+            else:
+                _lib.call("b2t_fp3d", ctypes.byref(self.geom.c), ctypes.byref(p), vol.data_ptr(), 0,
+                          proj.data_ptr(), 0, _DTYPES[vol.dtype], mode, stream_handle(vol.device))
         return proj
+
+    @property
+    def is_cyl(self):
+        return self.geom.kind == _lib.GEOM_CYLCONE
+
+    @staticmethod
+    def _cyl_f32(t):
+        if t.dtype != torch.float32:
+            raise AstraError(1, "cyl_cone_vec projectors take float32 data")
 
     def autotune(self, vol, proj):
         """Time the forward projector's launch shapes on these buffers and keep
@@ -91,6 +105,8 @@ class Projector3D:
         overwritten with A vol.  Returns the chosen views per CTA."""
         _check_tensor(vol, self.vol_shape, "volume")
         _check_tensor(proj, self.proj_shape, "projection data", vol.device)
+        if self.is_cyl:
+            raise AstraError(3, "autotune: the cyl_cone_vec projector has a single launch shape")
         p = self.params()
         vpc = ctypes.c_int32(0)
         with torch.cuda.device(vol.device):
@@ -106,8 +122,13 @@ class Projector3D:
             raise AstraError(1, "volume and projection data must have the same dtype")
         p = self.params(output_scale, kernel)
         with torch.cuda.device(vol.device):
-            _lib.call("b2t_bp3d", ctypes.byref(self.geom.c), ctypes.byref(p), proj.data_ptr(), 0,
-                      vol.data_ptr(), 0, _DTYPES[vol.dtype], mode, stream_handle(vol.device))
+            if self.is_cyl:
+                self._cyl_f32(vol)
+                _lib.call("b2t_bp3d_cyl", ctypes.byref(self.geom.c), ctypes.byref(p), proj.data_ptr(), 0,
+                          vol.data_ptr(), 0, mode, stream_handle(vol.device))
+            else:
+                _lib.call("b2t_bp3d", ctypes.byref(self.geom.c), ctypes.byref(p), proj.data_ptr(), 0,
+                          vol.data_ptr(), 0, _DTYPES[vol.dtype], mode, stream_handle(vol.device))
         return vol
 
 
@@ -153,8 +174,32 @@ class Projector2D:
         return vol
 
 
+def dlpack_tensor(x):
+    """(torch tensor sharing x's memory, True) for a DLPack object or capsule
+    other than a torch tensor or numpy array; (None, False) otherwise.
+
+    The reference takes DLPack data without a stream (its getDLPackCapsule,
+    python/astra/utils.pyx:237-260, leaves the stream argument open).  Here the
+    exchange follows the DLPack protocol: torch.from_dlpack passes the current
+    torch stream of the data's device to __dlpack__, so the producer orders its
+    pending work before the kernels that will read or write the array."""
+    if isinstance(x, (torch.Tensor, np.ndarray)):
+        return None, False
+    is_capsule = type(x).__name__ == 'PyCapsule'
+    if not (hasattr(x, '__dlpack__') or is_capsule):
+        return None, False
+    try:
+        return torch.from_dlpack(x), True
+    except Exception as e:  # unsupported device, dtype or layout
+        raise AstraError(1, "cannot use the DLPack data: %s" % (e,))
+
+
 def as_device_tensor(x, device, dtype=None):
-    """(tensor on device, copy_back) for a numpy array or torch tensor."""
+    """(tensor on device, copy_back) for a numpy array, a torch tensor or any
+    DLPack object (CUDA data in place; host data copied)."""
+    t, _ = dlpack_tensor(x)
+    if t is not None:
+        x = t
     if isinstance(x, np.ndarray):
         if x.dtype != np.float32:
             raise AstraError(1, "numpy data must be float32")
@@ -163,7 +208,24 @@ def as_device_tensor(x, device, dtype=None):
         if x.is_cuda:
             return x, False
         return x.to(device), True
-    raise AstraError(1, "data must be a numpy array or a torch tensor")
+    raise AstraError(1, "data must be a numpy array, a torch tensor or a DLPack object")
+
+
+def _finish_foreign(outputs, device):
+    """After writing into arrays that came through DLPack from another
+    library: synchronise the stream, so the producer's own streams see the
+    results (DLPack orders the hand-over, not the hand-back)."""
+    if any(dlpack_tensor(o)[1] for o in outputs):
+        torch.cuda.current_stream(device).synchronize()
+
+
+def _write_back(x, t):
+    """Copy a device result into the host object it came from."""
+    if isinstance(x, np.ndarray):
+        x[...] = t.cpu().numpy()
+        return
+    d, _ = dlpack_tensor(x)
+    (d if d is not None else x).copy_(t.cpu())
 
 
 def fp3d(projector, vol, proj, mode=_lib.MODE_SET):
@@ -173,10 +235,8 @@ def fp3d(projector, vol, proj, mode=_lib.MODE_SET):
     tp, back = as_device_tensor(proj, dev)
     projector.fp(tv, tp, mode=mode)
     if back:
-        if isinstance(proj, np.ndarray):
-            proj[...] = tp.cpu().numpy()
-        else:
-            proj.copy_(tp.cpu())
+        _write_back(proj, tp)
+    _finish_foreign([proj], dev)
     return proj
 
 
@@ -187,10 +247,8 @@ def bp3d(projector, vol, proj, mode=_lib.MODE_SET):
     tv, back = as_device_tensor(vol, dev)
     projector.bp(tp, tv, mode=mode)
     if back:
-        if isinstance(vol, np.ndarray):
-            vol[...] = tv.cpu().numpy()
-        else:
-            vol.copy_(tv.cpu())
+        _write_back(vol, tv)
+    _finish_foreign([vol], dev)
     return vol
 
 
@@ -244,8 +302,15 @@ def filter_taps(filter_type, n, n_views=1):
     return out.reshape(-1, 2 * int(n) - 1)
 
 
+def _no_cyl(projector, what):
+    # FDK needs a flat-panel cone geometry (cuda/3d/fdk.cu:415-478)
+    if getattr(projector, 'is_cyl', False):
+        raise AstraError(3, "%s needs a flat-panel cone geometry, not cyl_cone_vec" % what)
+
+
 def fdk(projector, proj, vol, short_scan=False, filter_type='ram-lak', output_scale=1.0, mode=_lib.MODE_SET):
     """FDK of proj into vol (torch CUDA tensors); proj is not modified."""
+    _no_cyl(projector, "FDK")
     _check_tensor(vol, projector.vol_shape, "volume")
     _check_tensor(proj, projector.proj_shape, "projection data", vol.device)
     if vol.dtype != proj.dtype:
@@ -319,6 +384,7 @@ def volume_geometry(i):
 
 def fdk_weight_filter(projector, proj, short_scan=False, filter_type='ram-lak'):
     """FDK pre-weighting and filtering of proj in place."""
+    _no_cyl(projector, "FDK")
     _check_tensor(proj, projector.proj_shape, "projection data")
     with torch.cuda.device(proj.device):
         spec = _filter_spec(filter_type)

@@ -85,7 +85,8 @@ enum {
     B2T_GEOM_PAR3D = 1,   /* parallel3d, parallel3d_vec -> SPar3DProjection  */
     B2T_GEOM_CONE = 2,    /* cone, cone_vec            -> SConeProjection   */
     B2T_GEOM_PAR2D = 3,   /* parallel, parallel_vec    -> SParProjection    */
-    B2T_GEOM_FAN2D = 4    /* fanflat, fanflat_vec      -> SFanProjection    */
+    B2T_GEOM_FAN2D = 4,   /* fanflat, fanflat_vec      -> SFanProjection    */
+    B2T_GEOM_CYLCONE = 5  /* cyl_cone_vec -> SCylConeProjection (b2t_geom3d_cyl) */
 };
 
 /* projection kernels: Cuda3DProjectionKernel (cuda/3d/dims3d.h:45-51) */
@@ -219,6 +220,32 @@ b2t_status b2t_vec_views3d(uint32_t n_angles, uint32_t det_cols, uint32_t det_ro
 b2t_status b2t_normalize_views3d(const b2t_volgeom3d *vol, int32_t kind, uint32_t n,
                                  b2t_view3d *views, float *vol_scale_out);
 
+/* cyl_cone_vec: one view of a cone beam on a detector curved around an axis,
+ * layout-identical to SCylConeProjection (include/astra/GeometryUtil3D.h:125-150).
+ * det_c = centre of the detector (on the cylinder); det_u = tangent from pixel
+ * (0,0) to (0,1), its length the pixel's arc length; det_v = pixel (0,0) to
+ * (1,0) along the cylinder axis; radius = cylinder radius. */
+typedef struct b2t_view3d_cyl {
+    double src[3];
+    double det_c[3];
+    double det_u[3];
+    double det_v[3];
+    double radius;
+} b2t_view3d_cyl;
+
+typedef struct b2t_geom3d_cyl {
+    b2t_dims3d dims;
+    float vol_scale[3];            /* voxel size x, y, z (world units)           */
+    const b2t_view3d_cyl *views;   /* host array of dims.angles views            */
+} b2t_geom3d_cyl;
+
+/* convertAstraGeometry for cyl_cone_vec (src/GeometryUtil3D.cpp:733-752 with
+ * convertAstraGeometry_unscaled_internal :597-617): translate source and
+ * detector centre so the volume is centred; no scaling (the kernels take the
+ * voxel size).  Writes the voxel size. */
+b2t_status b2t_normalize_views3d_cyl(const b2t_volgeom3d *vol, uint32_t n, b2t_view3d_cyl *views,
+                                     float *vol_scale_out);
+
 /* One 2D view: SFanProjection / SParProjection (GeometryUtil2D.h:53-105),
  * float fields.  src = source (fan) or ray direction (parallel); det_s =
  * detector start (pixel 0 corner); det_u = one detector pixel step. */
@@ -289,6 +316,23 @@ b2t_status b2t_fp3d(const b2t_geom3d *geom, const b2t_params3d *params,
 b2t_status b2t_bp3d(const b2t_geom3d *geom, const b2t_params3d *params,
                     const void *proj, size_t proj_pitch, void *vol, size_t vol_pitch,
                     int32_t dtype, int32_t mode, void *stream);
+
+/* Cone beam on a cylindrical detector (cyl_cone_vec), FP32 data.
+ * b2t_fp3d_cyl replaces astraCUDA3d::ConeCylFP (cuda/3d/cone_cyl.cu:197-306,
+ * 477-546, 622-682):
+ * per ray from the source to the pixel centre on the cylinder, unit steps
+ * along the dominant axis of (source - detector centre), bilinear samples,
+ * times the ray length per step.  b2t_bp3d_cyl: kernel DEFAULT replaces
+ * ConeCylBP (voxel-driven: the ray through
+ * the voxel centre meets the cylinder, weight t^2, times the voxel volume;
+ * cone_cyl_bp.cu:61-160, 235-320); MATCHED_BP is the exact transpose of
+ * b2t_fp3d_cyl (the reference's ConeCylBP_matched, cone_cyl.cu:308-475,
+ * 684-749, scatters the same model, without the output scale).
+ * No supersampling, as the reference. */
+b2t_status b2t_fp3d_cyl(const b2t_geom3d_cyl *geom, const b2t_params3d *params, const float *vol,
+                        size_t vol_pitch, float *proj, size_t proj_pitch, int32_t mode, void *stream);
+b2t_status b2t_bp3d_cyl(const b2t_geom3d_cyl *geom, const b2t_params3d *params, const float *proj,
+                        size_t proj_pitch, float *vol, size_t vol_pitch, int32_t mode, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* 2D projectors (f32 data)                                                */
@@ -408,6 +452,10 @@ typedef struct b2t_algo b2t_algo;  /* opaque: operator, weights, work buffers */
  * src/CudaCglsAlgorithm3D.cpp).  Allocates the work buffers (cudaMalloc). */
 b2t_status b2t_algo_create3d(int32_t type, const b2t_geom3d *geom, const b2t_params3d *params,
                              const b2t_algo_options *options, b2t_algo **out);
+/* SIRT3D_CUDA / CGLS3D_CUDA on a cyl_cone_vec geometry (no supersampling:
+ * CudaSirtAlgorithm3D.cpp:155-158, CudaCglsAlgorithm3D.cpp:156-159). */
+b2t_status b2t_algo_create3d_cyl(int32_t type, const b2t_geom3d_cyl *geom, const b2t_params3d *params,
+                                 const b2t_algo_options *options, b2t_algo **out);
 /* SIRT_CUDA / CGLS_CUDA / SART_CUDA (src/CudaSirtAlgorithm.cpp,
  * src/CudaCglsAlgorithm.cpp, src/CudaSartAlgorithm.cpp).  SART: one iteration
  * is one view (in the order of b2t_algo_set_projection_order, sequential by

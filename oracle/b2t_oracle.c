@@ -999,6 +999,198 @@ void orc_fan_bp(const float *views, long na, long ndet, long W, long H, double o
 
 /* Version tag so the loader can check it picked up this build. */
 /* ------------------------------------------------------------------------- */
+/* cone beam on a cylindrical detector (cyl_cone_vec)                         */
+/* ------------------------------------------------------------------------- */
+
+/* view w: src[3], det_c[3], det_u[3], det_v[3], radius (SCylConeProjection) */
+static void orc_cross(const double *a, const double *b, double *o)
+{
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+static double orc_norm3(const double *a) { return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+
+/* getCylConeAxes (src/GeometryUtil3D.cpp:542-561): radial a, tangential b,
+ * cylinder centre c. */
+static void orc_cyl_axes(const double *w, double *a, double *b, double *c)
+{
+    const double *s = w, *d = w + 3, *u = w + 6, *v = w + 9;
+    double R = w[12], uv[3];
+    orc_cross(u, v, uv);
+    double k = -R / (orc_norm3(u) * orc_norm3(v));
+    for (int i = 0; i < 3; ++i) a[i] = uv[i] * k;
+    double m[3], p[3];
+    for (int i = 0; i < 3; ++i) {
+        m[i] = d[i] - a[i] - s[i];
+        p[i] = d[i] + a[i] - s[i];
+    }
+    if (orc_norm3(m) > orc_norm3(p))
+        for (int i = 0; i < 3; ++i) a[i] = -a[i];
+    for (int i = 0; i < 3; ++i) {
+        c[i] = d[i] - a[i];
+        b[i] = u[i] * (R / orc_norm3(u));
+    }
+}
+
+/* dominant axis of source - detector centre, compared in float
+ * (ConeCylFP_Array_internal, cuda/3d/cone_cyl.cu:491-503) */
+static int orc_cyl_dir(const double *w)
+{
+    float dX = fabsf((float)(w[0] - w[3]));
+    float dY = fabsf((float)(w[1] - w[4]));
+    float dZ = fabsf((float)(w[2] - w[5]));
+    if (dX >= dY && dX >= dZ) return 0;
+    if (dY >= dX && dY >= dZ) return 1;
+    return 2;
+}
+
+/*
+ * One cylinder ray (cylcone_FP_t, cone_cyl.cu:197-306): slopes a1, a2 in
+ * texel steps per slice, offsets b1, b2 (texel units at the marching
+ * axis's world origin) and the ray length per slice.  Views are in world
+ * units, centred on the volume (convertAstraGeometry_unscaled).
+ */
+static void orc_cyl_ray(const double *w, int dir, long nu, long nv, long u, long v, const double *vs,
+                        double *a1, double *a2, double *b1, double *b2, double *corr)
+{
+    double A[3], B[3], C[3];
+    orc_cyl_axes(w, A, B, C);
+    double ut = orc_norm3(w + 6) / w[12];
+    double th = (2.0 * u - nu + 1) * 0.5 * ut;
+    double dv = v - 0.5 * nv + 0.5;
+    double D[3];
+    for (int k = 0; k < 3; ++k) D[k] = C[k] + A[k] * cos(th) + B[k] * sin(th) + w[9 + k] * dv;
+    double S0 = orc_c(w, dir, 0), S1 = orc_c(w, dir, 1), S2 = orc_c(w, dir, 2);
+    double D0 = orc_c(D, dir, 0), D1 = orc_c(D, dir, 1), D2 = orc_c(D, dir, 2);
+    double v0 = orc_c(vs, dir, 0), v1 = orc_c(vs, dir, 1), v2 = orc_c(vs, dir, 2);
+    double s1 = (S1 - D1) / (S0 - D0), s2 = (S2 - D2) / (S0 - D0);
+    *corr = sqrt(s1 * s1 + s2 * s2 + 1.0) * v0;
+    *a1 = s1 / v1 * v0;
+    *a2 = s2 / v2 * v0;
+    *b1 = S1 / v1 - s1 / v1 * S0;
+    *b2 = S2 / v2 - s2 / v2 * S0;
+}
+
+/*
+ * FP (ConeCylFP, cone_cyl.cu:622-682): per ray the bilinear samples (zero
+ * border) at every slice s of the dominant axis, texture coordinates
+ * a (s + 1/2 - n0/2) + b + n/2, times the ray length per slice and out_scale.
+ * views: (na, 13).  proj[v][a][u] written.
+ */
+int orc_cylcone_fp(const double *views, long nx, long ny, long nz, long na, long nu, long nv, const double *vs,
+                   double out_scale, int tex8, const float *vol, double *proj)
+{
+    for (long a = 0; a < na; ++a) {
+        const double *w = views + 13 * a;
+        int dir = orc_cyl_dir(w);
+        long n0, n1, n2, st0, st1, st2;
+        orc_plane3d(dir, nx, ny, nz, &n0, &n1, &n2, &st0, &st1, &st2);
+        for (long v = 0; v < nv; ++v) {
+            for (long u = 0; u < nu; ++u) {
+                double a1, a2, b1, b2, corr;
+                orc_cyl_ray(w, dir, nu, nv, u, v, vs, &a1, &a2, &b1, &b2, &corr);
+                double sum = 0.0;
+                for (long s = 0; s < n0; ++s) {
+                    double x0 = s + 0.5 - 0.5 * n0;
+                    double q1 = a1 * x0 + b1 + 0.5 * n1 - 0.5;
+                    double q2 = a2 * x0 + b2 + 0.5 * n2 - 0.5;
+                    sum += orc_bilin_f(vol + s * st0, st1, st2, n1, n2, q1, q2, tex8);
+                }
+                proj[(v * na + a) * nu + u] = sum * corr * out_scale;
+            }
+        }
+    }
+    return 0;
+}
+
+/* Exact transpose of orc_cylcone_fp: vol += A^T proj (the model of
+ * ConeCylBP_matched, cone_cyl.cu:308-475, 684-749, with out_scale). */
+int orc_cylcone_fp_transpose(const double *views, long nx, long ny, long nz, long na, long nu, long nv,
+                             const double *vs, double out_scale, const double *proj, double *vol)
+{
+    for (long a = 0; a < na; ++a) {
+        const double *w = views + 13 * a;
+        int dir = orc_cyl_dir(w);
+        long n0, n1, n2, st0, st1, st2;
+        orc_plane3d(dir, nx, ny, nz, &n0, &n1, &n2, &st0, &st1, &st2);
+        for (long v = 0; v < nv; ++v) {
+            for (long u = 0; u < nu; ++u) {
+                double a1, a2, b1, b2, corr;
+                orc_cyl_ray(w, dir, nu, nv, u, v, vs, &a1, &a2, &b1, &b2, &corr);
+                double val = proj[(v * na + a) * nu + u] * corr * out_scale;
+                for (long s = 0; s < n0; ++s) {
+                    double x0 = s + 0.5 - 0.5 * n0;
+                    double q1 = a1 * x0 + b1 + 0.5 * n1 - 0.5;
+                    double q2 = a2 * x0 + b2 + 0.5 * n2 - 0.5;
+                    orc_bilin_scatter(vol + s * st0, st1, st2, n1, n2, q1, q2, val);
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+/*
+ * Voxel-driven BP (ConeCylBP: dev_cylcone_BP cone_cyl_bp.cu:61-160,
+ * constants :162-233, host :235-320): for voxel centre x and view, the ray
+ * s + t (x - s) / sqrt|u x v| meets the cylinder (larger root t); the
+ * detector is sampled bilinearly (zero border) at angular coordinate
+ * asin(b / R) / (|u| / R) + nu/2 and axial coordinate v / |v| + nv/2 of that
+ * point; weight t^2; times out_scale and the voxel volume.  vol[z][y][x].
+ */
+int orc_cylcone_bp(const double *views, long nx, long ny, long nz, long na, long nu, long nv, const double *vs,
+                   double out_scale, int tex8, const float *proj, double *vol)
+{
+    double scale = out_scale * vs[0] * vs[1] * vs[2];
+    for (long z = 0; z < nz; ++z)
+        for (long y = 0; y < ny; ++y)
+            for (long x = 0; x < nx; ++x) vol[(z * ny + y) * nx + x] = 0.0;
+    for (long a = 0; a < na; ++a) {
+        const double *w = views + 13 * a;
+        double A[3], B[3], C[3], uv[3];
+        orc_cyl_axes(w, A, B, C);
+        double R = w[12], nA = orc_norm3(A), nB = orc_norm3(B), nV = orc_norm3(w + 9);
+        orc_cross(w + 6, w + 9, uv);
+        double f = sqrt(orc_norm3(uv));
+        double an[3], bn[3], vn[3], smc[3];
+        for (int k = 0; k < 3; ++k) {
+            an[k] = A[k] / nA;
+            bn[k] = B[k] / nB;
+            vn[k] = w[9 + k] / nV;
+            smc[k] = w[k] - C[k];
+        }
+        double sa = smc[0] * an[0] + smc[1] * an[1] + smc[2] * an[2];
+        double sb = smc[0] * bn[0] + smc[1] * bn[1] + smc[2] * bn[2];
+        double sc = smc[0] * vn[0] + smc[1] * vn[1] + smc[2] * vn[2];
+        double ut = orc_norm3(w + 6) / R;
+        for (long z = 0; z < nz; ++z) {
+            for (long y = 0; y < ny; ++y) {
+                for (long x = 0; x < nx; ++x) {
+                    double p[3] = {vs[0] * (x - 0.5 * nx + 0.5), vs[1] * (y - 0.5 * ny + 0.5),
+                                   vs[2] * (z - 0.5 * nz + 0.5)};
+                    double r[3] = {p[0] - w[0], p[1] - w[1], p[2] - w[2]};
+                    double ra = f * (r[0] * an[0] + r[1] * an[1] + r[2] * an[2]);
+                    double rb = f * (r[0] * bn[0] + r[1] * bn[1] + r[2] * bn[2]);
+                    double rc = f * (r[0] * vn[0] + r[1] * vn[1] + r[2] * vn[2]);
+                    double qa = ra * ra + rb * rb, qb = ra * sa + rb * sb, qc = sa * sa + sb * sb - R * R;
+                    double disc = qb * qb - qa * qc;
+                    if (disc < 0 || qa <= 0) continue;
+                    double t = (-qb + sqrt(disc)) / qa;
+                    double th = asin((t * rb + sb) / R) / ut;
+                    double vv = (t * rc + sc) / nV;
+                    double qu = th + 0.5 * nu - 0.5, qv = vv + 0.5 * nv - 0.5;
+                    /* detector plane of view a: u stride 1, v stride na * nu */
+                    double val = orc_bilin_f(proj + a * nu, 1, na * nu, nu, nv, qu, qv, tex8);
+                    vol[(z * ny + y) * nx + x] += val * t * t * scale;
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
 /* 2D SART (src/CudaSartAlgorithm.cpp, cuda/2d/sart.cu)                        */
 /* ------------------------------------------------------------------------- */
 

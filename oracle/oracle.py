@@ -54,6 +54,9 @@ def lib():
         L.orc_par_bp.argtypes = [_P, _L, _L, _L, _L, _D, _I, _I, _P, _P]
         L.orc_fan_fp.argtypes = [_P, _L, _L, _L, _L, _D, _I, _I, _P, _P]
         L.orc_fan_bp.argtypes = [_P, _L, _L, _L, _L, _D, _I, _I, _I, _P, _P]
+        L.orc_cylcone_fp.argtypes = [_P, _L, _L, _L, _L, _L, _L, _P, _D, _I, _P, _P]
+        L.orc_cylcone_fp_transpose.argtypes = [_P, _L, _L, _L, _L, _L, _L, _P, _D, _P, _P]
+        L.orc_cylcone_bp.argtypes = [_P, _L, _L, _L, _L, _L, _L, _P, _D, _I, _P, _P]
         L.orc_sart2d.argtypes = [_I, _P, _L, _L, _L, _L, _D, _I, _P, _L, _L, _L, _D, _I, _D, _I, _D, _I, _P, _P, _P]
         _lib = L
     return _lib
@@ -382,5 +385,48 @@ def sart2d(kind, views, sino, vol0, out_scale, iterations, order=None, iter0=0, 
                           lam, int(min_value is not None), float(min_value or 0.0), int(max_value is not None),
                           float(max_value or 0.0), int(tex8), sino.ctypes.data,
                           None if m is None else m.ctypes.data, vol.ctypes.data)
+    assert rc == 0
+    return vol
+
+
+def cylcone_fp(views, vol, det_u, det_v, vol_scale, out_scale=1.0, tex8=False):
+    """cyl_cone_vec forward projection (ConeCylFP); views (n, 13) in world
+    units centred on the volume; returns float64 [det_v][n][det_u]."""
+    views = _c(views, np.float64)
+    vol = _c(vol, np.float32)
+    nz, ny, nx = vol.shape
+    na = views.shape[0]
+    proj = np.zeros((det_v, na, det_u), dtype=np.float64)
+    vs = _c(vol_scale, np.float64)
+    rc = lib().orc_cylcone_fp(views.ctypes.data, nx, ny, nz, na, det_u, det_v, vs.ctypes.data, out_scale,
+                              int(tex8), vol.ctypes.data, proj.ctypes.data)
+    assert rc == 0
+    return proj
+
+
+def cylcone_fp_transpose(views, proj, vol_shape, vol_scale, out_scale=1.0):
+    """Exact transpose of cylcone_fp; returns float64 [z][y][x]."""
+    views = _c(views, np.float64)
+    proj = _c(proj, np.float64)
+    nv, na, nu = proj.shape
+    nz, ny, nx = vol_shape
+    vol = np.zeros(vol_shape, dtype=np.float64)
+    vs = _c(vol_scale, np.float64)
+    rc = lib().orc_cylcone_fp_transpose(views.ctypes.data, nx, ny, nz, na, nu, nv, vs.ctypes.data, out_scale,
+                                        proj.ctypes.data, vol.ctypes.data)
+    assert rc == 0
+    return vol
+
+
+def cylcone_bp(views, proj, vol_shape, vol_scale, out_scale=1.0, tex8=False):
+    """cyl_cone_vec voxel-driven backprojection (ConeCylBP); float64 [z][y][x]."""
+    views = _c(views, np.float64)
+    proj = _c(proj, np.float32)
+    nv, na, nu = proj.shape
+    nz, ny, nx = vol_shape
+    vol = np.zeros(vol_shape, dtype=np.float64)
+    vs = _c(vol_scale, np.float64)
+    rc = lib().orc_cylcone_bp(views.ctypes.data, nx, ny, nz, na, nu, nv, vs.ctypes.data, out_scale, int(tex8),
+                              proj.ctypes.data, vol.ctypes.data)
     assert rc == 0
     return vol

@@ -15,7 +15,7 @@ _P = ctypes.c_void_p
 _I = ctypes.c_int
 _F = ctypes.c_float
 
-GEOM3D_TYPES = {'parallel3d': 0, 'cone': 1, 'parallel3d_vec': 2, 'cone_vec': 3}
+GEOM3D_TYPES = {'parallel3d': 0, 'cone': 1, 'parallel3d_vec': 2, 'cone_vec': 3, 'cyl_cone_vec': 4}
 GEOM2D_TYPES = {'parallel': 0, 'fanflat': 1, 'parallel_vec': 2, 'fanflat_vec': 3}
 
 
@@ -31,6 +31,7 @@ def lib():
         L.ref_geom2d.argtypes = [_I, _I, _I, _P, _I, _I, _F, _P, _F, _F, _P, _P, _P]
         L.ref_cuda_fp3d.argtypes = [_I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _I, _P, _P]
         L.ref_cuda_bp3d.argtypes = [_I, _I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _I, _P, _P]
+        L.ref_cuda_cyl.argtypes = [_I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _P, _P]
         L.ref_cuda_sumsqw.argtypes = [_P, _I, _I, _I, _I, _I, _I, _P, _F, _P]
         L.ref_cuda_fdk.argtypes = [_P, _I, _I, _I, _I, _I, _I, _P, _I, _F, _P, _P]
         L.ref_cuda_fp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _P, _P]
@@ -60,7 +61,7 @@ def geom3d(vol_geom, proj_geom):
         sx, sy = proj_geom['DetectorSpacingX'], proj_geom['DetectorSpacingY']
         sod = proj_geom.get('DistanceOriginSource', 0.0)
         odd = proj_geom.get('DistanceOriginDetector', 0.0)
-    views = np.zeros((na, 12), dtype=np.float64)
+    views = np.zeros((na, 13 if t == 'cyl_cone_vec' else 12), dtype=np.float64)
     vs = np.zeros(3, dtype=np.float32)
     rc = lib().ref_geom3d(GEOM3D_TYPES[t], vol_geom['GridColCount'], vol_geom['GridRowCount'],
                           vol_geom['GridSliceCount'], win.ctypes.data, na, rows, cols, sx, sy,
@@ -114,6 +115,25 @@ def cuda_fp3d(kind, views, vol, nu, nv, vol_scale=(1.0, 1.0, 1.0), out_scale=1.0
     assert rc == 0
     torch.cuda.synchronize()
     return proj
+
+
+def cuda_cyl(op, views, data, vol_shape, nu, nv, vol_scale, out_scale=1.0):
+    """Reference cyl_cone_vec projector: op 'fp' (data = volume), 'bp' or
+    'bp_matched' (data = projections); returns a new float32 CUDA tensor."""
+    import torch
+    views = np.ascontiguousarray(views, dtype=np.float64)
+    vs = np.ascontiguousarray(vol_scale, dtype=np.float32)
+    nz, ny, nx = vol_shape
+    na = views.shape[0]
+    shape = (nv, na, nu) if op == 'fp' else tuple(vol_shape)
+    out = torch.zeros(shape, dtype=torch.float32, device='cuda')
+    torch.cuda.synchronize()
+    code = {'fp': 0, 'bp': 1, 'bp_matched': 2}[op]
+    rc = lib().ref_cuda_cyl(code, views.ctypes.data, nx, ny, nz, na, nu, nv, vs.ctypes.data, out_scale,
+                            data.data_ptr(), out.data_ptr())
+    assert rc == 0
+    torch.cuda.synchronize()
+    return out
 
 
 def cuda_sumsqw(views, vol_shape, nu, nv, vol_scale=(1.0, 1.0, 1.0), out_scale=1.0):

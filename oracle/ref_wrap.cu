@@ -10,6 +10,8 @@
 //   astra::convertAstraGeometry      src/GeometryUtil3D.cpp:754, GeometryUtil2D.cpp:357
 //   astraCUDA3d::ConeFP / Par3DFP    cuda/3d/cone_fp.cu:444, par3d_fp.cu:564
 //   astraCUDA3d::Par3DFP_SumSqW      cuda/3d/par3d_fp.cu:607
+//   astraCUDA3d::ConeCylFP / ConeCylBP / ConeCylBP_matched
+//                                    cuda/3d/cone_cyl.cu:622,724, cone_cyl_bp.cu:300
 //   astraCUDA3d::ConeBP / Par3DBP    cuda/3d/cone_bp.cu:380, par3d_bp.cu:318
 //   astraCUDA3d::FDK                 cuda/3d/fdk.cu:415
 //   astraCUDA::FP / FanFP            cuda/2d/par_fp.cu:340, fan_fp.cu:260
@@ -28,6 +30,7 @@
 #include "astra/CudaSartAlgorithm.h"
 #include "astra/Data2D.h"
 #include "astra/ConeVecProjectionGeometry3D.h"
+#include "astra/CylConeVecProjectionGeometry3D.h"
 #include "astra/FanFlatProjectionGeometry2D.h"
 #include "astra/FanFlatVecProjectionGeometry2D.h"
 #include "astra/Filters.h"
@@ -44,6 +47,7 @@
 #include "astra/cuda/2d/par_bp.h"
 #include "astra/cuda/2d/par_fp.h"
 #include "astra/cuda/3d/cone_bp.h"
+#include "astra/cuda/3d/cone_cyl.h"
 #include "astra/cuda/3d/cone_fp.h"
 #include "astra/cuda/3d/dims3d.h"
 #include "astra/cuda/3d/fdk.h"
@@ -60,6 +64,24 @@ void copy_cone(const SConeProjection &p, double *o)
                           p.fDetUX, p.fDetUY, p.fDetUZ, p.fDetVX, p.fDetVY, p.fDetVZ};
     memcpy(o, v, sizeof(v));
 }
+void copy_cyl(const SCylConeProjection &p, double *o)
+{
+    const double v[13] = {p.fSrcX, p.fSrcY, p.fSrcZ, p.fDetCX, p.fDetCY, p.fDetCZ, p.fDetUX, p.fDetUY,
+                          p.fDetUZ, p.fDetVX, p.fDetVY, p.fDetVZ, p.fDetR};
+    std::memcpy(o, v, sizeof(v));
+}
+
+SCylConeProjection to_cyl(const double *d)
+{
+    SCylConeProjection p;
+    p.fSrcX = d[0]; p.fSrcY = d[1]; p.fSrcZ = d[2];
+    p.fDetCX = d[3]; p.fDetCY = d[4]; p.fDetCZ = d[5];
+    p.fDetUX = d[6]; p.fDetUY = d[7]; p.fDetUZ = d[8];
+    p.fDetVX = d[9]; p.fDetVY = d[10]; p.fDetVZ = d[11];
+    p.fDetR = d[12];
+    return p;
+}
+
 void copy_par(const SPar3DProjection &p, double *o)
 {
     const double v[12] = {p.fRayX, p.fRayY, p.fRayZ, p.fDetSX, p.fDetSY, p.fDetSZ,
@@ -145,6 +167,10 @@ int ref_geom3d(int type, int cols, int rows, int slices, const float *window, in
             p.fDetSZ = d[5] - 0.5 * det_rows * p.fDetVZ - 0.5 * det_cols * p.fDetUZ;
         }
         pg.reset(new CParallelVecProjectionGeometry3D(na, det_rows, det_cols, std::move(v)));
+    } else if (type == 4) {
+        std::vector<SCylConeProjection> v(na);
+        for (int i = 0; i < na; ++i) v[i] = to_cyl(vecs + 13 * i);
+        pg.reset(new CCylConeVecProjectionGeometry3D(na, det_rows, det_cols, std::move(v)));
     } else {
         std::vector<SConeProjection> v(na);
         for (int i = 0; i < na; ++i) {
@@ -162,7 +188,8 @@ int ref_geom3d(int type, int cols, int rows, int slices, const float *window, in
     Geometry3DParameters g = convertAstraGeometry(&vg, pg.get());
     if (!g.isValid()) return 1;
     for (int i = 0; i < na; ++i) {
-        if (g.isCone()) copy_cone(g.getCone()[i], out_views + 12 * i);
+        if (g.isCylCone()) copy_cyl(g.getCylCone()[i], out_views + 13 * i);
+        else if (g.isCone()) copy_cone(g.getCone()[i], out_views + 12 * i);
         else copy_par(g.getParallel()[i], out_views + 12 * i);
     }
     out_volscale[0] = g.getVolScale().fX;
@@ -269,6 +296,30 @@ int ref_cuda_fp3d(int kind, const double *views, int nx, int ny, int nz, int na,
         for (int i = 0; i < na; ++i) p[i] = to_par(views + 12 * i);
         ok = astraCUDA3d::Par3DFP(pitched(d_vol, nx, ny), pitched(d_proj, nu, na), d, &p[0], params);
     }
+    return ok ? 0 : 1;
+}
+
+// cyl_cone_vec projectors: op 0 ConeCylFP (d_in volume, d_out projections),
+// 1 ConeCylBP, 2 ConeCylBP_matched (d_in projections, d_out volume).  views
+// (na, 13) as normalised by ref_geom3d.  Accumulates into d_out.
+int ref_cuda_cyl(int op, const double *views, int nx, int ny, int nz, int na, int nu, int nv, const float *vs,
+                 float out_scale, const float *d_in, float *d_out)
+{
+    astraCUDA3d::SProjectorParams3D params;
+    params.volScale.fX = vs[0];
+    params.volScale.fY = vs[1];
+    params.volScale.fZ = vs[2];
+    params.fOutputScale = out_scale;
+    SDimensions3D d = dims3(nx, ny, nz, na, nu, nv);
+    std::vector<SCylConeProjection> p(na);
+    for (int i = 0; i < na; ++i) p[i] = to_cyl(views + 13 * i);
+    bool ok;
+    if (op == 0)
+        ok = astraCUDA3d::ConeCylFP(pitched(d_in, nx, ny), pitched(d_out, nu, na), d, &p[0], params);
+    else if (op == 1)
+        ok = astraCUDA3d::ConeCylBP(pitched(d_out, nx, ny), pitched(d_in, nu, na), d, &p[0], params);
+    else
+        ok = astraCUDA3d::ConeCylBP_matched(pitched(d_out, nx, ny), pitched(d_in, nu, na), d, &p[0], params);
     return ok ? 0 : 1;
 }
 

@@ -21,6 +21,9 @@ def cases():
     ang = np.sort(rng.uniform(0, 2 * np.pi, 37)).astype(np.float32)
     V = rng.normal(size=(29, 12))
     V2 = rng.normal(size=(11, 6))
+    # cyl_cone_vec rows: 12 vector components and a positive radius
+    V13 = rng.normal(size=(17, 13))
+    V13[:, 12] = np.abs(V13[:, 12]) * 50.0 + 100.0
     vg3 = {'GridRowCount': 48, 'GridColCount': 40, 'GridSliceCount': 32,
            'option': {'WindowMinX': -21.3, 'WindowMaxX': 19.1, 'WindowMinY': -25.7, 'WindowMaxY': 22.9,
                       'WindowMinZ': -13.2, 'WindowMaxZ': 18.4}}
@@ -35,6 +38,8 @@ def cases():
         ('cone_vec', vg3, {'type': 'cone_vec', 'DetectorRowCount': 50, 'DetectorColCount': 60, 'Vectors': V}),
         ('parallel3d_vec', vg3, {'type': 'parallel3d_vec', 'DetectorRowCount': 50, 'DetectorColCount': 60,
                                  'Vectors': V}),
+        ('cyl_cone_vec', vg3, {'type': 'cyl_cone_vec', 'DetectorRowCount': 50, 'DetectorColCount': 60,
+                               'Vectors': V13}),
     ]
     c2 = [
         ('parallel', vg2, {'type': 'parallel', 'DetectorWidth': 1.3, 'DetectorCount': 90, 'ProjectionAngles': ang}),

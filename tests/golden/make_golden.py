@@ -66,6 +66,28 @@ def cone_vec_vectors():
     return np.array(vecs)
 
 
+def cyl_vectors():
+    """cyl_cone_vec rows (src, detector centre, u, v, radius): a circular orbit
+    on a cylinder centred at the source (radius SOD + ODD), plus views with the
+    source on the z axis (cylinder axis along y), so every marching direction
+    occurs."""
+    sod, odd, rows = 80.0, 40.0, []
+    for i in range(10):
+        t = 2 * np.pi * i / 10 + 0.1
+        src = np.array([np.sin(t) * sod, -np.cos(t) * sod, 1.5])
+        det = np.array([-np.sin(t) * odd, np.cos(t) * odd, -0.5])
+        u = np.array([np.cos(t), np.sin(t), 0.0]) * 1.1
+        v = np.array([0.0, 0.0, 0.9])
+        rows.append(np.concatenate([src, det, u, v, [sod + odd]]))
+    for sgn in (1.0, -1.0):
+        src = np.array([2.0, -1.0, -sgn * sod])
+        det = np.array([0.0, 0.0, sgn * odd])
+        u = np.array([1.2, 0.0, 0.0])
+        v = np.array([0.0, 1.0, 0.0])
+        rows.append(np.concatenate([src, det, u, v, [sod + odd]]))
+    return np.array(rows)
+
+
 def par_vec_vectors():
     """Nine parallel-beam views whose rays run mostly along z, x and y in turn,
     each tilted; detector centre, u and v per view (parallel3d_vec rows)."""
@@ -123,6 +145,12 @@ def cases():
     out.append(("fp3d_sumsqw_vec_aniso", "sumsqw", aniso[1],
                 {'type': 'parallel3d_vec', 'DetectorRowCount': 36, 'DetectorColCount': 44,
                  'Vectors': par_vec_vectors()}, {}))
+    # cyl_cone_vec: FP, voxel-driven BP, matched BP
+    cyl = ('cyl', vol_geom3(34, 30, 28, (-15.0, 15.0, -17.0, 17.0, -14.0, 14.0)),
+           {'type': 'cyl_cone_vec', 'DetectorRowCount': 40, 'DetectorColCount': 46, 'Vectors': cyl_vectors()})
+    out.append(("cyl_fp", "cylfp", cyl[1], cyl[2], {}))
+    out.append(("cyl_bp", "cylbp", cyl[1], cyl[2], {}))
+    out.append(("cyl_bpm", "cylbpm", cyl[1], cyl[2], {}))
     ang72 = np.linspace(0, 2 * np.pi, 72, endpoint=False).astype(np.float32)
     fdkg = {'type': 'cone', 'DetectorSpacingX': 1.0, 'DetectorSpacingY': 1.0, 'DetectorRowCount': 40,
             'DetectorColCount': 56, 'ProjectionAngles': ang72, 'DistanceOriginSource': 200.0,
@@ -151,6 +179,21 @@ def main(outdir, only=None):
     os.makedirs(outdir, exist_ok=True)
     for seed, (name, op, vg, pg, opt) in enumerate(cases()):
         if only and only not in name:
+            continue
+        if op in ("cylfp", "cylbp", "cylbpm"):
+            views, vs = ref.geom3d(vg, pg)
+            vshape = (vg['GridSliceCount'], vg['GridRowCount'], vg['GridColCount'])
+            pshape = (pg['DetectorRowCount'], views.shape[0], pg['DetectorColCount'])
+            if op == "cylfp":
+                inp = input_volume(vshape, seed)
+                res = ref.cuda_cyl('fp', views, torch.from_numpy(inp).cuda(), vshape, pshape[2], pshape[0], vs)
+            else:
+                inp = input_proj(pshape, seed)
+                res = ref.cuda_cyl('bp' if op == "cylbp" else 'bp_matched', views, torch.from_numpy(inp).cuda(),
+                                   vshape, pshape[2], pshape[0], vs)
+            np.savez_compressed(os.path.join(outdir, name + ".npz"), views=views, vol_scale=vs, input=inp,
+                                output=res.cpu().numpy(), kind=5)
+            print("wrote", name)
             continue
         if op in ("fp3d", "bp3d", "fdk", "sumsqw"):
             views, vs = ref.geom3d(vg, pg)

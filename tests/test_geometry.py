@@ -1,5 +1,5 @@
 """Geometry conversion (host code, CPU): libb2tomo's per-view vectors are
-bit-identical to the reference's convertAstraGeometry for all eight geometry
+bit-identical to the reference's convertAstraGeometry for all nine geometry
 types, against the committed fixtures (tests/golden/make_geometry_golden.py)
 and, when the reference build is present, against it directly."""
 import os
@@ -18,7 +18,7 @@ def _cases():
     return mg.cases()
 
 
-@pytest.mark.parametrize("i", range(4))
+@pytest.mark.parametrize("i", range(5))
 def test_3d_views_bit_exact_vs_fixture(geo, i):
     c3, _ = _cases()
     name, vg, pg = c3[i]

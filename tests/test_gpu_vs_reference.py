@@ -29,7 +29,7 @@ def _cases():
     return mg, [c for c in mg.cases()]
 
 
-@pytest.mark.parametrize("idx", range(21))
+@pytest.mark.parametrize("idx", range(24))
 def test_case_vs_reference_cuda(astra, idx):
     ref = _ref()
     mg, cases = _cases()
@@ -37,6 +37,24 @@ def test_case_vs_reference_cuda(astra, idx):
         pytest.skip("no such case")
     name, op, vg, pg, opt = cases[idx]
     P = importlib.import_module("astra-toolbox_b200.projector")
+    if op in ("cylfp", "cylbp", "cylbpm"):
+        opts = {'ProjectionKernel': 'matched_bp'} if op == "cylbpm" else {}
+        pr = P.Projector3D(pg, vg, opts)
+        views, vs = pr.geom.views_array(), pr.geom.vol_scale
+        nv, na, nu = pr.proj_shape
+        if op == "cylfp":
+            inp = torch.from_numpy(mg.input_volume(pr.vol_shape, idx)).cuda()
+            want = ref.cuda_cyl('fp', views, inp, pr.vol_shape, nu, nv, vs)
+            got = torch.zeros(pr.proj_shape, device='cuda')
+            pr.fp(inp, got)
+        else:
+            inp = torch.from_numpy(mg.input_proj(pr.proj_shape, idx)).cuda()
+            want = ref.cuda_cyl('bp' if op == "cylbp" else 'bp_matched', views, inp, pr.vol_shape, nu, nv, vs)
+            got = torch.zeros(pr.vol_shape, device='cuda')
+            pr.bp(inp, got)
+        err = rel_l2(got.cpu().numpy(), want.cpu().numpy())
+        assert err < (1e-4 if op == "cylbpm" else 2e-3), (name, err)
+        return
     if op == "sumsqw":
         pr = P.Projector3D(pg, vg, {'ProjectionKernel': 'sum_square_weights'})
         nv, na, nu = pr.proj_shape

@@ -17,7 +17,7 @@ from conftest import rel_l2
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FILES = sorted(f for f in glob.glob(os.path.join(GOLDEN, "*.npz"))
-               if os.path.basename(f).startswith(("fp", "bp", "fdk")))
+               if os.path.basename(f).startswith(("fp", "bp", "fdk", "cyl")))
 
 
 def _name(f):
@@ -33,6 +33,23 @@ def test_oracle_matches_reference_cuda(orc, path):
     inp = d["input"]
     views = d["views"]
     rays = 2 if "ss2" in name else 1
+    if name.startswith("cyl"):
+        # cyl_cone_vec; the matched BP scatters exact weights (no texture)
+        vs = d["vol_scale"]
+        if name == "cyl_fp":
+            nv, na, nu = out.shape
+            exact = orc.cylcone_fp(views, inp, nu, nv, vs)
+            tex8 = orc.cylcone_fp(views, inp, nu, nv, vs, tex8=True)
+        elif name == "cyl_bp":
+            exact = orc.cylcone_bp(views, inp, out.shape, vs)
+            tex8 = orc.cylcone_bp(views, inp, out.shape, vs, tex8=True)
+        else:
+            exact = orc.cylcone_fp_transpose(views, inp.astype(np.float64), out.shape, vs)
+            assert rel_l2(exact, out) < 1e-5, (name, rel_l2(exact, out))
+            return
+        assert rel_l2(exact, out) < 2e-3, (name, rel_l2(exact, out))
+        assert rel_l2(tex8, out) < 1e-3, (name, rel_l2(tex8, out))
+        return
     if "sumsqw" in name:
         # no texture in this kernel: the reference differs from the FP64
         # model only by its float position stepping
