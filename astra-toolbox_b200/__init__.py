@@ -19,6 +19,7 @@ from .projector import Projector2D, Projector3D
 from . import algorithm, batch, data2d, data3d, experimental, projector, projector3d  # noqa: F401
 from .batch import Batch2D  # noqa: F401
 from .optomo import OpTomo  # noqa: F401
+from .gpu import get_gpu_info, set_gpu_index  # noqa: F401
 from .algorithm import astra_dict
 from .creators import (create_backprojection, create_backprojection3d_gpu, create_projector,  # noqa: F401
                        create_reconstruction, create_sino, create_sino3d_gpu)

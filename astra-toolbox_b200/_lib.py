@@ -69,6 +69,11 @@ class Geom3DCyl(ctypes.Structure):
     _fields_ = [("dims", Dims3D), ("vol_scale", ctypes.c_float * 3), ("views", ctypes.POINTER(View3DCyl))]
 
 
+class StreamConfig(ctypes.Structure):
+    _fields_ = [("device_bytes", ctypes.c_size_t), ("n_devices", ctypes.c_uint32),
+                ("devices", ctypes.POINTER(ctypes.c_int32))]
+
+
 class Params3D(ctypes.Structure):
     _fields_ = [("det_supersample", ctypes.c_uint32), ("voxel_supersample", ctypes.c_uint32),
                 ("output_scale", ctypes.c_float), ("kernel", ctypes.c_int32)]
@@ -136,6 +141,10 @@ SIGNATURES = {
     "b2t_fp3d": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
     "b2t_bp3d": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _I32, _P]),
     "b2t_normalize_views3d_cyl": (_I32, [_P, _U32, _P, _P]),
+    "b2t_fp3d_host": (_I32, [_P, _P, _P, _P, _I32, _P]),
+    "b2t_bp3d_host": (_I32, [_P, _P, _P, _P, _I32, _P]),
+    "b2t_fdk_host": (_I32, [_P, _P, _I32, ctypes.c_float, _P, _P, _I32, _P]),
+    "b2t_stream_plan": (_I32, [_I32, _P, _P, _P, _P]),
     "b2t_fp3d_cyl": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _P]),
     "b2t_bp3d_cyl": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _P]),
     "b2t_fp2d": (_I32, [_P, _U32, _P, _SZ, _P, _SZ, _I32, _P]),

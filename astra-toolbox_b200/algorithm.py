@@ -84,9 +84,13 @@ class _FP(_Algorithm):
         self.proj = _d.lookup(cfg['ProjectionDataId'], _d.DataObject)
         cls = _P.Projector3D if is3d else _P.Projector2D
         self.pr = cls(self.proj.geometry, self.vol.geometry, self._projector_options())
+        self.is3d = is3d
 
     def run(self, iterations=1):
-        self.pr.fp(self.vol.tensor, self.proj.tensor)
+        if self.is3d and not (self.vol.tensor.is_cuda and self.proj.tensor.is_cuda):
+            _P.fp3d_host(self.pr, self.vol.tensor, self.proj.tensor)
+        else:
+            self.pr.fp(self.vol.tensor, self.proj.tensor)
         self.proj.changed()
 
 
@@ -97,9 +101,13 @@ class _BP(_Algorithm):
         self.proj = _d.lookup(cfg['ProjectionDataId'], _d.DataObject)
         cls = _P.Projector3D if is3d else _P.Projector2D
         self.pr = cls(self.proj.geometry, self.vol.geometry, self._projector_options())
+        self.is3d = is3d
 
     def run(self, iterations=1):
-        self.pr.bp(self.proj.tensor, self.vol.tensor)
+        if self.is3d and not (self.vol.tensor.is_cuda and self.proj.tensor.is_cuda):
+            _P.bp3d_host(self.pr, self.proj.tensor, self.vol.tensor)
+        else:
+            self.pr.bp(self.proj.tensor, self.vol.tensor)
         self.vol.changed()
 
 
@@ -115,7 +123,10 @@ class _FDK(_Algorithm):
         self.filter = _filter_from_cfg(cfg, self.opt)
 
     def run(self, iterations=1):
-        _P.fdk(self.pr, self.proj.tensor, self.vol.tensor, short_scan=self.short, filter_type=self.filter)
+        if not (self.vol.tensor.is_cuda and self.proj.tensor.is_cuda):
+            _P.fdk_host(self.pr, self.proj.tensor, self.vol.tensor, short_scan=self.short, filter_type=self.filter)
+        else:
+            _P.fdk(self.pr, self.proj.tensor, self.vol.tensor, short_scan=self.short, filter_type=self.filter)
         self.vol.changed()
 
 
@@ -137,8 +148,10 @@ class _Iterative(_Algorithm):
             if key not in o:
                 return None
             obj = _d.lookup(o[key], _d.DataObject)
-            self._keep.append(obj)
-            return obj.tensor.data_ptr()
+            # the library reads masks on the device: stage host-resident ones
+            t = obj.tensor if obj.tensor.is_cuda else obj.tensor.to(torch.device('cuda', torch.cuda.current_device()))
+            self._keep.extend([obj, t])
+            return t.data_ptr()
 
         self.c_opt = _lib.AlgoOptions(float(o.get('Relaxation', 1.0)), int(use_min), vmin, int(use_max), vmax,
                                       dev_ptr('ReconstructionMaskId'), dev_ptr('SinogramMaskId'),
@@ -153,19 +166,29 @@ class _Iterative(_Algorithm):
             _lib.call("b2t_algo_create2d", kind, ctypes.byref(self.pr.geom.c), self.pr.det_ss, self.pr.pix_ss,
                       ctypes.byref(self.c_opt), ctypes.byref(self.handle))
 
+    def _device_data(self):
+        """(projection, volume) device tensors: host-resident data objects are
+        staged on the GPU for the iterations (SIRT and CGLS need all of it on
+        the device, as the reference's do)."""
+        p, v = self.proj.tensor, self.vol.tensor
+        dev = torch.device('cuda', torch.cuda.current_device())
+        return (p if p.is_cuda else p.to(dev)), (v if v.is_cuda else v.to(dev))
+
     def run(self, iterations=1):
-        dev = self.vol.tensor.device
-        with torch.cuda.device(dev):
-            _lib.call("b2t_algo_run", self.handle, self.proj.tensor.data_ptr(), self.vol.tensor.data_ptr(),
-                      int(iterations), self.use_graph, _P.stream_handle(dev))
+        p, v = self._device_data()
+        with torch.cuda.device(v.device):
+            _lib.call("b2t_algo_run", self.handle, p.data_ptr(), v.data_ptr(),
+                      int(iterations), self.use_graph, _P.stream_handle(v.device))
+        if not self.vol.tensor.is_cuda:
+            self.vol.tensor.copy_(v.cpu())
         self.vol.changed()
 
     def get_res_norm(self):
-        dev = self.vol.tensor.device
+        p, v = self._device_data()
         out = ctypes.c_double(0.0)
-        with torch.cuda.device(dev):
-            _lib.call("b2t_algo_residual_norm", self.handle, self.proj.tensor.data_ptr(), self.vol.tensor.data_ptr(),
-                      ctypes.byref(out), _P.stream_handle(dev))
+        with torch.cuda.device(v.device):
+            _lib.call("b2t_algo_residual_norm", self.handle, p.data_ptr(), v.data_ptr(),
+                      ctypes.byref(out), _P.stream_handle(v.device))
         return out.value
 
     def close(self):

@@ -127,6 +127,35 @@ b2t_status b2t_bp3d(const b2t_geom3d *geom, const b2t_params3d *params, const vo
                      static_cast<cudaStream_t>(stream));
 }
 
+b2t_status b2t_fp3d_host(const b2t_geom3d *geom, const b2t_params3d *params, const float *vol, float *proj,
+                         int32_t mode, const b2t_stream_config *cfg)
+{
+    clear_error();
+    return stream3d_run(0, geom, params, nullptr, 0, 1.0f, vol, proj, mode, cfg);
+}
+
+b2t_status b2t_bp3d_host(const b2t_geom3d *geom, const b2t_params3d *params, const float *proj, float *vol,
+                         int32_t mode, const b2t_stream_config *cfg)
+{
+    clear_error();
+    return stream3d_run(1, geom, params, nullptr, 0, 1.0f, proj, vol, mode, cfg);
+}
+
+b2t_status b2t_fdk_host(const b2t_geom3d *geom, const b2t_filter_config *filter, int32_t short_scan,
+                        float output_scale, const float *proj, float *vol, int32_t mode,
+                        const b2t_stream_config *cfg)
+{
+    clear_error();
+    return stream3d_run(2, geom, nullptr, filter, short_scan, output_scale, proj, vol, mode, cfg);
+}
+
+b2t_status b2t_stream_plan(int32_t op, const b2t_geom3d *geom, const b2t_stream_config *cfg, uint32_t *slab,
+                           uint32_t *block)
+{
+    clear_error();
+    return stream3d_plan(op, geom, cfg, slab, block);
+}
+
 b2t_status b2t_fp3d_cyl(const b2t_geom3d_cyl *geom, const b2t_params3d *params, const float *vol,
                         size_t vol_pitch, float *proj, size_t proj_pitch, int32_t mode, void *stream)
 {

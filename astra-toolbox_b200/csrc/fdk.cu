@@ -664,6 +664,25 @@ static b2t_status validate_fdk(const b2t_geom3d *g, const b2t_filter_config *fil
     return B2T_OK;
 }
 
+b2t_status fdk_weight_filter_views(const b2t_geom3d *g, uint32_t a0, uint32_t n, const b2t_filter_config *filter,
+                                   int32_t short_scan, const float *src, size_t src_pitch, float *dst,
+                                   long long dst_row, long long dst_v, cudaStream_t s)
+{
+    B2T_TRY(validate_fdk(g, filter, B2T_F32, "FDK views"));
+    if (a0 + n > g->dims.angles || n == 0) return fail(B2T_ERR_INVALID_ARG, "FDK views: range outside the scan");
+    const int ftype = filter ? filter->type : B2T_FILTER_RAMLAK;
+    if ((ftype == B2T_FILTER_SINOGRAM || ftype == B2T_FILTER_RSINOGRAM) && n != g->dims.angles)
+        return fail(B2T_ERR_UNSUPPORTED, "FDK views: per-view custom filters need all views at once");
+    FDKWeights P;
+    std::vector<float> rel;
+    B2T_TRY(fdk_setup(g, short_scan, P, rel));
+    std::vector<float> sub;
+    if (!rel.empty()) sub.assign(rel.begin() + a0, rel.begin() + a0 + n);
+    b2t_dims3d d = g->dims;
+    d.angles = n;
+    return run_filter(d, P, sub, filter, src, src_pitch, dst, dst_row, dst_v, B2T_F32, s);
+}
+
 b2t_status fdk_weight_filter_impl(const b2t_geom3d *g, const b2t_filter_config *filter, int32_t short_scan, void *proj,
                                   size_t proj_pitch, int32_t dtype, cudaStream_t s)
 {

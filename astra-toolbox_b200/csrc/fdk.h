@@ -30,6 +30,13 @@ b2t_status fbp2d_impl(const b2t_geom2d *g, const b2t_filter_config *filter, int3
                       float *vol, size_t vol_pitch, int32_t mode, cudaStream_t s);
 b2t_status fdk_weight_filter_impl(const b2t_geom3d *g, const b2t_filter_config *filter, int32_t short_scan, void *proj,
                                   size_t proj_pitch, int32_t dtype, cudaStream_t s);
+// FDK pre-weighting and filtering of views [a0, a0 + n) of the scan g, with
+// the weights of the whole scan (its angle count and Parker range): src is
+// the block's projections [v][n][u] (row pitch src_pitch), dst as for the
+// padded BP input (element strides dst_row between views, dst_v between rows).
+b2t_status fdk_weight_filter_views(const b2t_geom3d *g, uint32_t a0, uint32_t n, const b2t_filter_config *filter,
+                                   int32_t short_scan, const float *src, size_t src_pitch, float *dst,
+                                   long long dst_row, long long dst_v, cudaStream_t s);
 b2t_status fdk_impl(const b2t_geom3d *g, const b2t_filter_config *filter, int32_t short_scan, float output_scale, const void *proj,
                     size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
 

@@ -112,6 +112,11 @@ b2t_status fp3d_cyl_impl(const b2t_geom3d_cyl *g, const b2t_params3d *p, const f
                          float *proj, size_t proj_pitch, int32_t mode, cudaStream_t s);
 b2t_status bp3d_cyl_impl(const b2t_geom3d_cyl *g, const b2t_params3d *p, const float *proj, size_t proj_pitch,
                          float *vol, size_t vol_pitch, int32_t mode, cudaStream_t s);
+b2t_status stream3d_run(int32_t op, const b2t_geom3d *g, const b2t_params3d *params,
+                        const b2t_filter_config *filter, int32_t short_scan, float fdk_scale, const float *in,
+                        float *out, int32_t mode, const b2t_stream_config *cfg);
+b2t_status stream3d_plan(int32_t op, const b2t_geom3d *g, const b2t_stream_config *cfg, uint32_t *slab,
+                         uint32_t *block);
 b2t_status fp3d_sumsqw_impl(const b2t_geom3d *g, const b2t_params3d *p, void *proj, size_t proj_pitch,
                             int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status fp3d_autotune_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch,

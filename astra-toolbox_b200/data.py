@@ -4,7 +4,8 @@ python/astra/data3d_c.pyx, data2d_c.pyx).
 
 A data object holds a float32 torch tensor on the GPU (the reference keeps
 float32 host memory and copies it to the GPU per call; here the data stay
-resident).  Linked numpy arrays are mirrored on the device and written back
+resident), or, for 3D data beyond the device memory budget (gpu.py), in
+pinned host memory, streamed through the GPUs per call.  Linked numpy arrays are mirrored on the device and written back
 after every operation that changes them; linked torch CUDA tensors, and CUDA
 arrays of other libraries passed through DLPack, are used in place (zero
 copy).
@@ -16,6 +17,7 @@ import torch
 
 from ._lib import AstraError
 from . import geometry as G
+from . import gpu as _gpu
 
 _ids = itertools.count(1)
 _objects = {}
@@ -65,18 +67,28 @@ class DataObject:
         self.host = None       # linked numpy array (written back after changes)
         self.foreign = False   # linked through DLPack from another library
 
+    def _host_resident(self):
+        # 3D data beyond the device budget stays in (pinned) host memory and
+        # is streamed through the GPUs by FP3D / BP3D / FDK
+        return self.is3d and _gpu.host_resident(self.shape)
+
+    def _empty(self):
+        if self._host_resident():
+            return torch.empty(self.shape, dtype=torch.float32, pin_memory=torch.cuda.is_available())
+        return torch.empty(self.shape, dtype=torch.float32, device=_device())
+
     def fill(self, data):
-        dev = _device()
+        self.tensor = self._empty()
         if data is None:
-            self.tensor = torch.zeros(self.shape, dtype=torch.float32, device=dev)
+            self.tensor.zero_()
         elif np.isscalar(data):
-            self.tensor = torch.full(self.shape, float(data), dtype=torch.float32, device=dev)
+            self.tensor.fill_(float(data))
         else:
             arr = data.detach().cpu().numpy() if isinstance(data, torch.Tensor) else np.asarray(data)
             if tuple(arr.shape) != self.shape:
                 raise AstraError(1, "The dimensions of the data %s do not match those specified in the geometry %s"
                                  % (tuple(arr.shape), self.shape))
-            self.tensor = torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32)).to(dev)
+            self.tensor.copy_(torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32)))
 
     def link(self, data):
         from .projector import dlpack_tensor
@@ -107,6 +119,11 @@ class DataObject:
             if tuple(data.shape) != self.shape:
                 raise AstraError(1, "The dimensions of the data do not match those specified in the geometry")
             self.host = data
+        if self._host_resident():
+            # streamed from the linked host array itself (no device mirror)
+            self.tensor = torch.from_numpy(self.host)
+            self.host = None
+            return
         self.tensor = torch.from_numpy(self.host).to(_device())
 
     def changed(self):

@@ -47,7 +47,10 @@ def accumulate_FP(projector_id, vol_id, proj_id):
     pr = _projector(projector_id)
     v = _d.lookup(vol_id, _d.DataObject)
     p = _d.lookup(proj_id, _d.DataObject)
-    pr.fp(v.tensor, p.tensor, mode=MODE_ADD)
+    if v.tensor.is_cuda and p.tensor.is_cuda:
+        pr.fp(v.tensor, p.tensor, mode=MODE_ADD)
+    else:
+        _P.fp3d_host(pr, v.tensor, p.tensor, mode=MODE_ADD)
     p.changed()
 
 
@@ -56,7 +59,10 @@ def accumulate_BP(projector_id, vol_id, proj_id):
     pr = _projector(projector_id)
     v = _d.lookup(vol_id, _d.DataObject)
     p = _d.lookup(proj_id, _d.DataObject)
-    pr.bp(p.tensor, v.tensor, mode=MODE_ADD)
+    if v.tensor.is_cuda and p.tensor.is_cuda:
+        pr.bp(p.tensor, v.tensor, mode=MODE_ADD)
+    else:
+        _P.bp3d_host(pr, p.tensor, v.tensor, mode=MODE_ADD)
     v.changed()
 
 
@@ -65,5 +71,8 @@ def accumulate_FDK(projector_id, vol_id, proj_id, short_scan=False):
     pr = _projector(projector_id)
     v = _d.lookup(vol_id, _d.DataObject)
     p = _d.lookup(proj_id, _d.DataObject)
-    _P.fdk(pr, p.tensor, v.tensor, short_scan=short_scan, mode=MODE_ADD)
+    if v.tensor.is_cuda and p.tensor.is_cuda:
+        _P.fdk(pr, p.tensor, v.tensor, short_scan=short_scan, mode=MODE_ADD)
+    else:
+        _P.fdk_host(pr, p.tensor, v.tensor, short_scan=short_scan, mode=MODE_ADD)
     v.changed()

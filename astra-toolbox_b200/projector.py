@@ -302,6 +302,63 @@ def filter_taps(filter_type, n, n_views=1):
     return out.reshape(-1, 2 * int(n) - 1)
 
 
+# ---------------------------------------------------------------------------
+# streamed calls on host-resident data (b2t_*_host)
+# ---------------------------------------------------------------------------
+
+def _host_f32(t):
+    if t.is_cuda:
+        return t.cpu().contiguous(), True
+    if t.dtype != torch.float32 or not t.is_contiguous():
+        raise AstraError(1, "host data must be contiguous float32")
+    return t, False
+
+
+def _stream(fn, projector, inp, out, extra_before, extra_after, mode):
+    """Run a b2t_*_host call: inputs and outputs as CPU tensors (device
+    tensors are staged through host memory)."""
+    from . import gpu as _gpu
+    if projector.is_cyl:
+        raise AstraError(3, "streamed projection covers the flat-panel geometries; cyl_cone_vec data must fit the GPU")
+    hi, _ = _host_f32(inp)
+    ho, staged = _host_f32(out)
+    cfg = _gpu.stream_config()
+    _lib.call(fn, ctypes.byref(projector.geom.c), *extra_before, hi.data_ptr(), ho.data_ptr(), mode, *extra_after,
+              ctypes.byref(cfg))
+    if staged:
+        out.copy_(ho)
+    return out
+
+
+def fp3d_host(projector, vol, proj, mode=_lib.MODE_SET):
+    """proj (=|+=) A vol, streamed through the GPUs (b2t_fp3d_host)."""
+    return _stream("b2t_fp3d_host", projector, vol, proj, [ctypes.byref(projector.params())], [], mode)
+
+
+def bp3d_host(projector, proj, vol, mode=_lib.MODE_SET):
+    """vol (=|+=) B proj, streamed through the GPUs (b2t_bp3d_host)."""
+    return _stream("b2t_bp3d_host", projector, proj, vol, [ctypes.byref(projector.params())], [], mode)
+
+
+def fdk_host(projector, proj, vol, short_scan=False, filter_type='ram-lak', output_scale=1.0, mode=_lib.MODE_SET):
+    """FDK streamed through the GPUs (b2t_fdk_host)."""
+    _no_cyl(projector, "FDK")
+    cfg = _filter_spec(filter_type).c()
+    return _stream("b2t_fdk_host", projector, proj, vol,
+                   [ctypes.byref(cfg), int(bool(short_scan)), ctypes.c_float(output_scale)], [], mode)
+
+
+def stream_plan(projector, op):
+    """(z-slab thickness, angle block size) of a streamed FP ('fp'), BP
+    ('bp') or FDK ('fdk') under the current GPU settings."""
+    from . import gpu as _gpu
+    cfg = _gpu.stream_config()
+    slab, block = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    _lib.call("b2t_stream_plan", {'fp': 0, 'bp': 1, 'fdk': 2}[op], ctypes.byref(projector.geom.c),
+              ctypes.byref(cfg), ctypes.byref(slab), ctypes.byref(block))
+    return slab.value, block.value
+
+
 def _no_cyl(projector, what):
     # FDK needs a flat-panel cone geometry (cuda/3d/fdk.cu:415-478)
     if getattr(projector, 'is_cyl', False):

@@ -317,6 +317,32 @@ b2t_status b2t_bp3d(const b2t_geom3d *geom, const b2t_params3d *params,
                     const void *proj, size_t proj_pitch, void *vol, size_t vol_pitch,
                     int32_t dtype, int32_t mode, void *stream);
 
+/* Streamed projection of host-resident FP32 data larger than the device
+ * memory (the reference's CompositeGeometryManager,
+ * src/CompositeGeometryManager.cpp:218-379, 1115-1280, 1409-1477, behind
+ * astraCUDA3d::FP/BP/FDK and astra.set_gpu_index(..., memory=...)).  The
+ * volume is cut into z-slabs, the projections into angle blocks; blocks
+ * stream through double-buffered device memory with the copies overlapping
+ * the compute (pinned host memory), jobs spread over the listed GPUs.
+ * Host arrays are tightly packed ([z][y][x], [v][angle][u]).  Calls block
+ * until the output is in host memory. */
+typedef struct b2t_stream_config {
+    size_t device_bytes;       /* device memory per GPU (0: free memory less 2 GiB) */
+    uint32_t n_devices;        /* GPUs to spread jobs over (0: the current device) */
+    const int32_t *devices;    /* their ordinals                                  */
+} b2t_stream_config;
+b2t_status b2t_fp3d_host(const b2t_geom3d *geom, const b2t_params3d *params, const float *vol, float *proj,
+                         int32_t mode, const b2t_stream_config *cfg);
+b2t_status b2t_bp3d_host(const b2t_geom3d *geom, const b2t_params3d *params, const float *proj, float *vol,
+                         int32_t mode, const b2t_stream_config *cfg);
+b2t_status b2t_fdk_host(const b2t_geom3d *geom, const b2t_filter_config *filter, int32_t short_scan,
+                        float output_scale, const float *proj, float *vol, int32_t mode,
+                        const b2t_stream_config *cfg);
+/* The split a streamed call would use: op 0 FP, 1 BP, 2 FDK; z-slab
+ * thickness and angle block size. */
+b2t_status b2t_stream_plan(int32_t op, const b2t_geom3d *geom, const b2t_stream_config *cfg, uint32_t *slab,
+                           uint32_t *block);
+
 /* Cone beam on a cylindrical detector (cyl_cone_vec), FP32 data.
  * b2t_fp3d_cyl replaces astraCUDA3d::ConeCylFP (cuda/3d/cone_cyl.cu:197-306,
  * 477-546, 622-682):
