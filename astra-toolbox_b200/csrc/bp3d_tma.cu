@@ -263,7 +263,7 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t 
                         break;
                     }
                 }
-                if (!__all_sync(0xffffffffu, mbar_wait_bounded(&empty[j0 % BPT_SLOTS],
+                if (!__all_sync(0xffffffffu, mbar_wait_bounded_sleep(&empty[j0 % BPT_SLOTS],
                                                                (uint32_t)((j0 / BPT_SLOTS) & 1), 2000000000LL))) {
                     if (lane == 0) atomicOr(&g_b2t_device_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
                     return;

@@ -142,15 +142,6 @@ __global__ void build_cells(const T *__restrict__ vol, size_t pitch, int nx, int
     }
 }
 
-__device__ __forceinline__ void split_texel_c(float qm, int &k, float &f)
-{
-    const float M = 12582912.0f;
-    float t = __fadd_rn(qm, M);
-    float r = __fadd_rn(t, -M);
-    k = __float_as_int(t) - 0x4B400000;
-    f = __fadd_rn(__fadd_rn(qm, -r), 0.5f);
-}
-
 __device__ __forceinline__ void clip_slices_c(float A, float B, float lo, float hi, float &smin, float &smax)
 {
     if (fabsf(A) < 1e-12f) {
@@ -165,11 +156,16 @@ __device__ __forceinline__ void clip_slices_c(float A, float B, float lo, float 
     smax = fminf(smax, fmaxf(s1, s2));
 }
 
-__device__ __forceinline__ bool texel_ok_c(float A, float B, int s, int n)
+// Base texel of sample position qh = qm + 1/2 by rounding down: qh + M
+// rounded toward -inf holds floor(qh) in its mantissa (|qh| < 2^22); the
+// same texel and weight as split_texel_c up to exact ties, where both give
+// the same value.
+constexpr float SPLIT_M = 12582912.0f;  // 1.5 * 2^23
+__device__ __forceinline__ int floor_texel(float qh) { return __float_as_int(__fadd_rd(qh, SPLIT_M)) - 0x4B400000; }
+
+__device__ __forceinline__ bool texel_ok_f(float A, float Bh, int s, int n)
 {
-    int k;
-    float f;
-    split_texel_c(fmaf(A, (float)s, B), k, f);
+    const int k = floor_texel(fmaf(A, (float)s, Bh));
     return k >= -2 && k <= n;
 }
 
@@ -225,39 +221,44 @@ __global__ void __launch_bounds__(32 * VROWS * VPC, 2048 / (32 * VROWS * VPC)) f
             clip_slices_c(A2, B2, -1.6f, (float)L.n2 - 0.4f, smin, smax);
             int s_lo = max(0, (int)ceilf(fmaxf(smin, -1.0f)));
             int s_hi = min(L.n0 - 1, (int)floorf(fminf(smax, n0)));
+            // sample positions plus one half: texel floor(), weight frac()
+            const float B1h = B1 + 0.5f, B2h = B2 + 0.5f;
             for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
-                if (texel_ok_c(A1, B1, s_lo, L.n1) && texel_ok_c(A2, B2, s_lo, L.n2)) break;
+                if (texel_ok_f(A1, B1h, s_lo, L.n1) && texel_ok_f(A2, B2h, s_lo, L.n2)) break;
                 ++s_lo;
             }
             for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
-                if (texel_ok_c(A1, B1, s_hi, L.n1) && texel_ok_c(A2, B2, s_hi, L.n2)) break;
+                if (texel_ok_f(A1, B1h, s_hi, L.n1) && texel_ok_f(A2, B2h, s_hi, L.n2)) break;
                 --s_hi;
             }
-            if (!(texel_ok_c(A1, B1, s_lo, L.n1) && texel_ok_c(A2, B2, s_lo, L.n2) &&
-                  texel_ok_c(A1, B1, s_hi, L.n1) && texel_ok_c(A2, B2, s_hi, L.n2)))
+            if (!(texel_ok_f(A1, B1h, s_lo, L.n1) && texel_ok_f(A2, B2h, s_lo, L.n2) &&
+                  texel_ok_f(A1, B1h, s_hi, L.n1) && texel_ok_f(A2, B2h, s_hi, L.n2)))
                 s_hi = s_lo - 1;
+            // the base texels are monotone in s, so the checks at both ends
+            // keep every access inside the cell grid.  Cell address of slice
+            // s, texels (k1, k2): cells + s st0 + k2 st2 + k1, formed from the
+            // bits of the rounded-down sums (k + 0x4B400000) with 32 x 32 ->
+            // 64-bit multiply-adds; the constant offset wraps around in 64 bits
+            const uint32_t cb = (uint32_t)sizeof(C), st0b = (uint32_t)(st0 * cb), st2b = (uint32_t)(st2 * cb);
+            const unsigned long long base0 = reinterpret_cast<unsigned long long>(cells) -
+                                             0x4B400000ull * ((unsigned long long)st2b + cb);
+            auto sample = [&](int sl) -> float {
+                const float q1 = fmaf(A1, (float)sl, B1h), q2 = fmaf(A2, (float)sl, B2h);
+                const float t1 = __fadd_rd(q1, SPLIT_M), t2 = __fadd_rd(q2, SPLIT_M);
+                const float f1 = q1 - (t1 - SPLIT_M), f2 = q2 - (t2 - SPLIT_M);
+                const unsigned long long a = base0 + (unsigned long long)(uint32_t)sl * st0b +
+                                             (unsigned long long)(uint32_t)__float_as_int(t2) * st2b +
+                                             (unsigned long long)(uint32_t)__float_as_int(t1) * cb;
+                return cell_value<T>(reinterpret_cast<const C *>(a), f1, f2);
+            };
             // two independent accumulators keep two loads in flight per thread
             float sum0 = 0.0f, sum1 = 0.0f;
             int s = s_lo;
             for (; s + 1 <= s_hi; s += 2) {
-                int k1a, k2a, k1b, k2b;
-                float f1a, f2a, f1b, f2b;
-                split_texel_c(fmaf(A1, (float)s, B1), k1a, f1a);
-                split_texel_c(fmaf(A2, (float)s, B2), k2a, f2a);
-                split_texel_c(fmaf(A1, (float)(s + 1), B1), k1b, f1b);
-                split_texel_c(fmaf(A2, (float)(s + 1), B2), k2b, f2b);
-                const C *pa = cells + (long long)s * st0 + (long long)k2a * st2 + k1a;
-                const C *pb = cells + (long long)(s + 1) * st0 + (long long)k2b * st2 + k1b;
-                sum0 += cell_value<T>(pa, f1a, f2a);
-                sum1 += cell_value<T>(pb, f1b, f2b);
+                sum0 += sample(s);
+                sum1 += sample(s + 1);
             }
-            if (s <= s_hi) {
-                int k1, k2;
-                float f1, f2;
-                split_texel_c(fmaf(A1, (float)s, B1), k1, f1);
-                split_texel_c(fmaf(A2, (float)s, B2), k2, f2);
-                sum0 += cell_value<T>(cells + (long long)s * st0 + (long long)k2 * st2 + k1, f1, f2);
-            }
+            if (s <= s_hi) sum0 += sample(s);
             const float sc = sqrtf(fmaf(A1 * A1, L.f1, fmaf(A2 * A2, L.f2, 1.0f))) * L.mul;
             acc = fmaf(sum0 + sum1, sc, acc);
         }

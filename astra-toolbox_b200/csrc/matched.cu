@@ -44,15 +44,6 @@ template <> __device__ __forceinline__ float tom<float>(float v) { return v; }
 template <> __device__ __forceinline__ __half tom<__half>(float v) { return __float2half_rn(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 tom<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 
-__device__ __forceinline__ void split_texel_m(float qm, int &k, float &f)
-{
-    const float M = 12582912.0f;
-    float t = __fadd_rn(qm, M);
-    float r = __fadd_rn(t, -M);
-    k = __float_as_int(t) - 0x4B400000;
-    f = __fadd_rn(__fadd_rn(qm, -r), 0.5f);
-}
-
 __device__ __forceinline__ void clip_slices_m(float A, float B, float lo, float hi, float &smin, float &smax)
 {
     if (fabsf(A) < 1e-12f) {
@@ -67,11 +58,22 @@ __device__ __forceinline__ void clip_slices_m(float A, float B, float lo, float 
     smax = fminf(smax, fmaxf(s1, s2));
 }
 
-__device__ __forceinline__ bool texel_ok_m(float A, float B, int s, int n)
+// The forward projectors' split (fp3d_cell_kernel, fp3d_kernel): sample
+// position plus one half qh = A s + (B + 1/2); texel floor(qh) by rounding
+// down, weight qh - floor(qh).  Identical arithmetic keeps the transpose exact.
+constexpr float SPLIT_M = 12582912.0f;  // 1.5 * 2^23
+__device__ __forceinline__ void split_floor_m(float qh, int &k, float &f)
+{
+    const float t = __fadd_rd(qh, SPLIT_M);
+    k = __float_as_int(t) - 0x4B400000;
+    f = qh - (t - SPLIT_M);
+}
+
+__device__ __forceinline__ bool texel_ok_m(float A, float Bh, int s, int n)
 {
     int k;
     float f;
-    split_texel_m(fmaf(A, (float)s, B), k, f);
+    split_floor_m(fmaf(A, (float)s, Bh), k, f);
     return k >= -2 && k <= n;
 }
 
@@ -112,24 +114,25 @@ __global__ void __launch_bounds__(256) fp3d_transpose_kernel(const __grid_consta
             clip_slices_m(A2, B2, -1.6f, (float)L.n2 - 0.4f, smin, smax);
             int s_lo = max(0, (int)ceilf(fmaxf(smin, -1.0f)));
             int s_hi = min(L.n0 - 1, (int)floorf(fminf(smax, n0)));
+            const float B1h = B1 + 0.5f, B2h = B2 + 0.5f;
             for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
-                if (texel_ok_m(A1, B1, s_lo, L.n1) && texel_ok_m(A2, B2, s_lo, L.n2)) break;
+                if (texel_ok_m(A1, B1h, s_lo, L.n1) && texel_ok_m(A2, B2h, s_lo, L.n2)) break;
                 ++s_lo;
             }
             for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
-                if (texel_ok_m(A1, B1, s_hi, L.n1) && texel_ok_m(A2, B2, s_hi, L.n2)) break;
+                if (texel_ok_m(A1, B1h, s_hi, L.n1) && texel_ok_m(A2, B2h, s_hi, L.n2)) break;
                 --s_hi;
             }
-            if (!(texel_ok_m(A1, B1, s_lo, L.n1) && texel_ok_m(A2, B2, s_lo, L.n2) &&
-                  texel_ok_m(A1, B1, s_hi, L.n1) && texel_ok_m(A2, B2, s_hi, L.n2)))
+            if (!(texel_ok_m(A1, B1h, s_lo, L.n1) && texel_ok_m(A2, B2h, s_lo, L.n2) &&
+                  texel_ok_m(A1, B1h, s_hi, L.n1) && texel_ok_m(A2, B2h, s_hi, L.n2)))
                 s_hi = s_lo - 1;
             const float sc = sqrtf(fmaf(A1 * A1, L.f1, fmaf(A2 * A2, L.f2, 1.0f))) * L.mul;
             const float w = val * sc;
             for (int s = s_lo; s <= s_hi; ++s) {
                 int k1, k2;
                 float f1, f2;
-                split_texel_m(fmaf(A1, (float)s, B1), k1, f1);
-                split_texel_m(fmaf(A2, (float)s, B2), k2, f2);
+                split_floor_m(fmaf(A1, (float)s, B1h), k1, f1);
+                split_floor_m(fmaf(A2, (float)s, B2h), k2, f2);
                 float *p = acc + (long long)s * st0 + (long long)k2 * st2 + k1;
                 const float g1 = 1.0f - f1, g2 = 1.0f - f2;
                 atomicAdd(p, g1 * g2 * w);

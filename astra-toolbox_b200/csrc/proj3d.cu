@@ -166,11 +166,22 @@ __device__ __forceinline__ void clip_slices(float A, float B, float lo, float hi
     smax = fminf(smax, fmaxf(s1, s2));
 }
 
-__device__ __forceinline__ bool fp_texel_ok(float A, float B, int s, int n)
+// The FP's split (shared with fp3d_cell_kernel and the matched BP): sample
+// position plus one half qh = A s + (B + 1/2); texel floor(qh) by rounding
+// down, weight qh - floor(qh).
+constexpr float SPLIT_M = 12582912.0f;  // 1.5 * 2^23
+__device__ __forceinline__ void split_floor(float qh, int &k, float &f)
+{
+    const float t = __fadd_rd(qh, SPLIT_M);
+    k = __float_as_int(t) - 0x4B400000;
+    f = qh - (t - SPLIT_M);
+}
+
+__device__ __forceinline__ bool fp_texel_ok(float A, float Bh, int s, int n)
 {
     int k;
     float f;
-    split_texel(fmaf(A, (float)s, B), k, f);
+    split_floor(fmaf(A, (float)s, Bh), k, f);
     return k >= -2 && k <= n;
 }
 
@@ -207,25 +218,26 @@ __global__ void __launch_bounds__(256) fp3d_kernel(const __grid_constant__ FPLau
             clip_slices(A2, B2, -1.6f, (float)L.n2 - 0.4f, smin, smax);
             int s_lo = max(0, (int)ceilf(fmaxf(smin, -1.0f)));
             int s_hi = min(L.n0 - 1, (int)floorf(fminf(smax, n0)));
+            const float B1h = B1 + 0.5f, B2h = B2 + 0.5f;
             // guarantee every access is inside the padded copy: the base
             // texel is monotone in s, so checking the end points suffices
             for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
-                if (fp_texel_ok(A1, B1, s_lo, L.n1) && fp_texel_ok(A2, B2, s_lo, L.n2)) break;
+                if (fp_texel_ok(A1, B1h, s_lo, L.n1) && fp_texel_ok(A2, B2h, s_lo, L.n2)) break;
                 ++s_lo;
             }
             for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
-                if (fp_texel_ok(A1, B1, s_hi, L.n1) && fp_texel_ok(A2, B2, s_hi, L.n2)) break;
+                if (fp_texel_ok(A1, B1h, s_hi, L.n1) && fp_texel_ok(A2, B2h, s_hi, L.n2)) break;
                 --s_hi;
             }
-            if (!(fp_texel_ok(A1, B1, s_lo, L.n1) && fp_texel_ok(A2, B2, s_lo, L.n2) &&
-                  fp_texel_ok(A1, B1, s_hi, L.n1) && fp_texel_ok(A2, B2, s_hi, L.n2)))
+            if (!(fp_texel_ok(A1, B1h, s_lo, L.n1) && fp_texel_ok(A2, B2h, s_lo, L.n2) &&
+                  fp_texel_ok(A1, B1h, s_hi, L.n1) && fp_texel_ok(A2, B2h, s_hi, L.n2)))
                 s_hi = s_lo - 1;
             float sum = 0.0f;
             for (int s = s_lo; s <= s_hi; ++s) {
                 int k1, k2;
                 float f1, f2;
-                split_texel(fmaf(A1, (float)s, B1), k1, f1);
-                split_texel(fmaf(A2, (float)s, B2), k2, f2);
+                split_floor(fmaf(A1, (float)s, B1h), k1, f1);
+                split_floor(fmaf(A2, (float)s, B2h), k2, f2);
                 const T *p = vol + (long long)s * st0 + (long long)k2 * st2 + k1;
                 const float v00 = ld(p), v10 = ld(p + 1);
                 const float v01 = ld(p + st2), v11 = ld(p + st2 + 1);

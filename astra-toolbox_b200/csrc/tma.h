@@ -72,6 +72,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return done != 0;
 }
 
+// try_wait with a suspend-time hint: the thread may sleep (without issuing)
+// for up to `ns` nanoseconds while the phase is incomplete; it resumes as soon
+// as the phase completes.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t ns)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return done != 0;
+}
+
 // Wait for phase `parity` of a barrier, giving up after ~max_cycles clock
 // cycles.  Returns false on timeout.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long max_cycles)
@@ -79,6 +95,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > max_cycles) return false;
+    }
+    return true;
+}
+
+// The same, sleeping between polls instead of spinning, for waits whose
+// end matters more than their latency (a producer waiting for room): the
+// warp leaves its issue slots to the others.
+__device__ __forceinline__ bool mbar_wait_bounded_sleep(uint64_t *bar, uint32_t parity, long long max_cycles)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait_sleep(bar, parity, 20000u)) {
         if (clock64() - t0 > max_cycles) return false;
     }
     return true;

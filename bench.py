@@ -386,6 +386,156 @@ def run_workload(args):
     return 0
 
 
+def run_extra(args):
+    """--workload stream | sart2d | cyl.
+
+    stream: FP + BP of the cone workload from pinned host memory through a
+    device budget (--budget-gb, default 4) that forces z-slabs and angle
+    blocks (b2t_fp3d_host / b2t_bp3d_host); one step = one FP + one BP,
+    host to host; metric GUPS of the pair (2 x Nx Ny Nz Nangles / time),
+    timed on the host clock around the blocking calls; the device-resident
+    FP + BP time is reported beside it.
+    sart2d: SART_CUDA on a 256^2 parallel-beam problem (180 views over pi,
+    384 detectors), sequential order, CUDA-graph steps; one step = one sweep
+    (180 single-view updates); metric sweeps/s.
+    cyl: cyl_cone_vec FP + BP, 256^3 volume, 360 views, 256 x 384 detector on
+    a cylinder centred at the source; metric GUPS of the pair."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    astra = importlib.import_module("astra-toolbox_b200")
+    lib = importlib.import_module("astra-toolbox_b200._lib").load()
+    lib.b2t_kernel_launches.restype = ctypes.c_uint64
+    P = importlib.import_module("astra-toolbox_b200.projector")
+    ph = importlib.import_module("astra-toolbox_b200.phantom")
+    stream = torch.cuda.current_stream(dev)
+    sampler = ClockSampler(0)
+    extra, roof, e2e = {}, None, None
+    if args.workload == "stream":
+        astra, vg, pg = workload(args.n, args.views, args.det)
+        pr = astra.Projector3D(pg, vg)
+        vol = ph.ellipsoids(pr.vol_shape, N_ELL, seed=0, device=dev)
+        dproj = torch.zeros(pr.proj_shape, device=dev)
+        drec = torch.zeros(pr.vol_shape, device=dev)
+        hvol = vol.cpu().pin_memory()
+        hproj = torch.zeros(pr.proj_shape).pin_memory()
+        hrec = torch.zeros(pr.vol_shape).pin_memory()
+        budget = int(args.budget_gb * 1e9)
+        astra.set_gpu_index(0, memory=budget)
+        plan = {op: P.stream_plan(pr, op) for op in ("fp", "bp")}
+
+        def step():
+            P.fp3d_host(pr, hvol, hproj)
+            P.bp3d_host(pr, hproj, hrec)
+
+        for _ in range(args.warmup):
+            step()
+        sampler.start()
+        time.sleep(0.3)
+        l0 = lib.b2t_kernel_launches()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+        ms = (time.perf_counter() - t0) * 1e3 / args.steps
+        launches = lib.b2t_kernel_launches() - l0
+        clocks = sampler.stop()
+        astra.set_gpu_index(0, memory=0)
+        ms_dev = _timed_region(torch, stream, lambda: (pr.fp(vol, dproj), pr.bp(dproj, drec)), max(1, args.steps))
+        ups = 2.0 * np.prod(pr.vol_shape) * pr.proj_shape[1]
+        value, unit, hib = ups / (ms * 1e-3) / 1e9, "GUPS", True
+        metric = "streamed FP+BP GUPS at %d^3x%d from host memory, %.1f GB device budget" % (
+            args.n, args.views, args.budget_gb)
+        extra = {"device_resident_ms": ms_dev, "device_resident_gups": ups / (ms_dev * 1e-3) / 1e9,
+                 "plan": {"fp_slab_z": plan["fp"][0], "fp_block_views": plan["fp"][1],
+                          "bp_slab_z": plan["bp"][0], "bp_block_views": plan["bp"][1]},
+                 "host_bytes_per_step": int(2 * (hvol.numel() + hproj.numel()) * 4),
+                 "timing": "host clock around the blocking host-to-host calls"}
+        e2e = {"value": value, "unit": unit, "h2d_bytes_per_step": int((hvol.numel() + hproj.numel()) * 4),
+               "d2h_bytes_per_step": int((hproj.numel() + hrec.numel()) * 4), "ms_per_step": ms,
+               "path": "b2t_fp3d_host + b2t_bp3d_host (every byte in and out of host memory)"}
+        cfgd = config_dict(args.n, args.views, args.det, {"workload_kind": "stream", "budget_gb": args.budget_gb})
+    elif args.workload == "sart2d":
+        ang = np.linspace(0, np.pi, 180, endpoint=False).astype(np.float32)
+        vg = astra.create_vol_geom(256, 256)
+        pg = astra.create_proj_geom('parallel', 1.0, 384, ang)
+        pr = astra.Projector2D(pg, vg)
+        x = ph.ellipsoids((1, 256, 256), 10, seed=0, axes=(10.0, 80.0), device=dev)[0].contiguous()
+        b = torch.zeros(pr.proj_shape, device=dev)
+        pr.fp(x, b)
+        D2 = importlib.import_module("astra-toolbox_b200.data2d")
+        A = importlib.import_module("astra-toolbox_b200.algorithm")
+        sid = D2.link('-sino', pg, b)
+        rid = D2.create('-vol', vg, 0)
+        cfg = A.astra_dict('SART_CUDA')
+        cfg['ProjectionDataId'] = sid
+        cfg['ReconstructionDataId'] = rid
+        cfg['option'] = {'UseGraph': True, 'ProjectionOrder': 'sequential'}
+        aid = A.create(cfg)
+        A.run(aid, 180 * args.warmup)
+        sampler.start()
+        time.sleep(0.3)
+        l0 = lib.b2t_kernel_launches()
+        ms = _timed_region(torch, stream, lambda: A.run(aid, 180), args.steps)
+        launches = lib.b2t_kernel_launches() - l0
+        clocks = sampler.stop()
+        res = A.get_res_norm(aid)
+        A.delete(aid)
+        D2.delete([sid, rid])
+        value, unit, hib = 1e3 / ms, "sweeps/s", True
+        metric = "SART_CUDA sweeps/s at 256^2, 180 views, 384 detectors"
+        extra = {"us_per_view_step": ms * 1e3 / 180, "relative_residual": res / float(b.double().norm()),
+                 "sweeps_before_residual": args.warmup + args.steps}
+        cfgd = {"workload": "SART_CUDA, 256^2 parallel beam, 180 views over pi, 384 detectors, 10 seeded ellipses, "
+                            "sequential order", "workload_kind": "sart2d"}
+    else:
+        n, na, rows, cols = 256, 360, 256, 384
+        sod, odd = 600.0, 300.0
+        vecs = []
+        for i in range(na):
+            t = 2 * np.pi * i / na
+            src = [np.sin(t) * sod, -np.cos(t) * sod, 0.0]
+            det = [-np.sin(t) * odd, np.cos(t) * odd, 0.0]
+            u = [np.cos(t) * 1.4, np.sin(t) * 1.4, 0.0]
+            vecs.append(src + det + u + [0.0, 0.0, 1.4, sod + odd])
+        vg = astra.create_vol_geom(n, n, n)
+        pg = astra.create_proj_geom('cyl_cone_vec', rows, cols, np.array(vecs))
+        pr = astra.Projector3D(pg, vg)
+        vol = ph.ellipsoids(pr.vol_shape, N_ELL, seed=0, axes=(10.0, 100.0), device=dev)
+        proj = torch.zeros(pr.proj_shape, device=dev)
+        rec = torch.zeros(pr.vol_shape, device=dev)
+
+        def step():
+            pr.fp(vol, proj)
+            pr.bp(proj, rec)
+
+        for _ in range(args.warmup):
+            step()
+        sampler.start()
+        time.sleep(0.3)
+        l0 = lib.b2t_kernel_launches()
+        ms = _timed_region(torch, stream, step, args.steps)
+        launches = lib.b2t_kernel_launches() - l0
+        clocks = sampler.stop()
+        ms_fp = _timed_region(torch, stream, lambda: pr.fp(vol, proj), max(1, args.steps))
+        ups = 2.0 * n ** 3 * na
+        value, unit, hib = ups / (ms * 1e-3) / 1e9, "GUPS", True
+        metric = "cyl_cone_vec FP+BP GUPS at 256^3x360"
+        extra = {"fp_ms": ms_fp, "bp_ms": ms - ms_fp}
+        cfgd = {"workload": "cyl_cone_vec FP+BP, 256^3 volume, 360 views over 2pi, 256x384 detector on a cylinder "
+                            "of radius SOD+ODD=900 centred at the source, SOD 600", "workload_kind": "cyl"}
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": hib, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfgd, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clocks, "roofline": roof, "cpu_baseline": None}
+    line.update(extra)
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -399,7 +549,9 @@ def main():
     ap.add_argument("--ref-views", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="fpbp", choices=["fpbp", "fdk", "sirt3d", "cgls3d", "batch2d"])
+    ap.add_argument("--workload", default="fpbp",
+                    choices=["fpbp", "fdk", "sirt3d", "cgls3d", "batch2d", "stream", "sart2d", "cyl"])
+    ap.add_argument("--budget-gb", type=float, default=4.0, help="device budget of --workload stream")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -407,6 +559,8 @@ def main():
         return run_reference(args)
     if args.workload == "batch2d":
         return run_batch2d(args)
+    if args.workload in ("stream", "sart2d", "cyl"):
+        return run_extra(args)
     if args.workload != "fpbp":
         return run_workload(args)
 
