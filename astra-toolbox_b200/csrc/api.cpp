@@ -111,6 +111,14 @@ b2t_status b2t_device_errors(uint32_t *flags)
     return device_errors_impl(flags);
 }
 
+b2t_status b2t_bp_path_stats(uint64_t *stats)
+{
+    clear_error();
+    if (!stats) return fail(B2T_ERR_INVALID_ARG, "b2t_bp_path_stats: null pointer");
+    B2T_CUDA_TRY(cudaDeviceSynchronize(), "b2t_bp_path_stats synchronize");
+    return bp_path_stats_impl(stats);
+}
+
 b2t_status b2t_fp3d(const b2t_geom3d *geom, const b2t_params3d *params, const void *vol, size_t vol_pitch,
                     void *proj, size_t proj_pitch, int32_t dtype, int32_t mode, void *stream)
 {

@@ -5,7 +5,7 @@
 // is projected onto each view, the projection is sampled bilinearly and
 // weighted.  The difference is where the samples come from:
 //
-//   - a CTA owns a 32 x 8 x 16 voxel block and walks all views of the launch
+//   - a CTA owns a 32 x 8 x 32 voxel block and walks all views of the launch
 //     with eight compute warps and one producer warp;
 //   - for each view the producer projects the block's eight corner voxels,
 //     takes the bounding box of their detector coordinates (plus one texel of
@@ -18,7 +18,7 @@
 //     geometries (detector v axis along z) the detector u coordinate and the
 //     ray-density weight do not depend on z, so each thread computes them once
 //     per view (from affine forms the producer folds per block) and only v
-//     changes along its 16-voxel column;
+//     changes along its 32-voxel column;
 //   - a tile that does not fit (extreme magnification) is read from the padded
 //     projections in global memory instead.
 //
@@ -42,6 +42,15 @@ namespace b2t {
 
 // error word of this translation unit (see b2t_device_errors)
 static __device__ unsigned int g_b2t_device_errors = 0;
+
+// Path statistics of the TMA backprojection, read and cleared by
+// b2t_bp_path_stats.  In voxel-column views (one thread's column of BPT_Z
+// voxels for one view): [0] the circular fast path (all samples from the
+// shared-memory tile), [1] the general path (other orbits, columns whose
+// rows leave the tile, views read from global memory), [2] lanes idle
+// because their column lies outside the volume; [3] SM cycles the compute
+// warps spent in their view loops, summed over warps.
+static __device__ unsigned long long g_bp_path_stats[4] = {0, 0, 0, 0};
 
 namespace {
 
@@ -105,6 +114,7 @@ template <typename T> __host__ __device__ constexpr int ring_rows()
 }
 static_assert(BPT_CHUNK * 84 * 4 % 128 == 0 && BPT_CHUNK * 88 * 2 % 128 == 0, "chunk alignment");
 static_assert((84 * 4) % 16 == 0 && (88 * 2) % 16 == 0, "TMA box row bytes");
+static_assert(ring_rows<float>() >= BPT_BV && ring_rows<__half>() >= BPT_BV, "the ring holds the largest view");
 
 // Per-view record written by the producer warp: the tile's origin in padded
 // texels (u0, v0), its first ring row and its row count (0: the footprint does
@@ -174,6 +184,7 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t 
     int j0 = 0;         // oldest view still held by the compute warps
     int head = 0;       // next free ring row
     int slot_row0 = 0;  // lane s < BPT_SLOTS: first ring row of the view in slot s
+    int slot_rows = 0;  // lane s < BPT_SLOTS: its row count (0: it reads global memory)
     for (int vb = 0; vb < L.nviews; vb += 32) {
         const int v = vb + lane;
         StageInfo r;
@@ -239,16 +250,22 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t 
             for (;;) {
                 const int live = vk - j0;
                 if (live < BPT_SLOTS) {
-                    if (live == 0) {
-                        head = 0;
-                        at = 0;
-                        break;
-                    }
                     if (nrows == 0) {
                         at = head;
                         break;
                     }
-                    const int tail = __shfl_sync(0xffffffffu, slot_row0, j0 % BPT_SLOTS);
+                    // the occupied rows start at the oldest live view that
+                    // holds rows; with none the ring is empty
+                    int tail = -1;
+                    for (int q = j0; q < vk && tail < 0; ++q) {
+                        const int r0 = __shfl_sync(0xffffffffu, slot_row0, q % BPT_SLOTS);
+                        if (__shfl_sync(0xffffffffu, slot_rows, q % BPT_SLOTS) > 0) tail = r0;
+                    }
+                    if (tail < 0) {
+                        head = 0;
+                        at = 0;
+                        break;
+                    }
                     if (head > tail) {
                         if (R - head >= nrows) {
                             at = head;
@@ -270,7 +287,10 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t 
                 }
                 ++j0;
             }
-            if (lane == slot) slot_row0 = at;
+            if (lane == slot) {
+                slot_row0 = at;
+                slot_rows = nrows;
+            }
             if (nrows > 0) head = at + nrows;
             if (lane == k) {
                 // the loads go out before the record is written: the view's
@@ -292,7 +312,7 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t 
 // 288 threads: warps 0-7 backproject a 32 x 8 x BPT_Z voxel block, warp 8
 // streams the views' tiles into the ring ahead of them.
 template <typename T, int KIND, int KER, bool CIRC>
-__global__ void __launch_bounds__(288, 3) bp3d_tma_kernel(const __grid_constant__ BPTmaLaunch L)
+__global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __grid_constant__ BPTmaLaunch L)
 {
     constexpr int R = ring_rows<T>();
     constexpr int BU = tile_bu<T>();
@@ -337,6 +357,8 @@ __global__ void __launch_bounds__(288, 3) bp3d_tma_kernel(const __grid_constant_
 #pragma unroll
     for (int j = 0; j < BPT_Z; ++j) acc[j] = 0.0f;
 
+    unsigned long long n_fast = 0, n_general = 0, n_idle = 0;  // this thread's column-views by path
+    const long long t_loop = clock64();
     int slot = 0;
     uint32_t parity = 0;
     for (int i = 0; i < L.nviews; ++i) {
@@ -394,6 +416,9 @@ __global__ void __launch_bounds__(288, 3) bp3d_tma_kernel(const __grid_constant_
                 done = true;
             }
         }
+        if (done) ++n_fast;
+        else if (active) ++n_general;
+        else ++n_idle;
         if (active && !done) {
             // the general paths recompute the voxel centre here rather than
             // keeping it live across the hot loop above
@@ -518,13 +543,27 @@ __global__ void __launch_bounds__(288, 3) bp3d_tma_kernel(const __grid_constant_
         }
     }
 
-    if (active) {
+    // per-thread counts are at most the launch's views, so 32-bit sums hold
+    const unsigned w_fast = __reduce_add_sync(0xffffffffu, (unsigned)n_fast);
+    const unsigned w_general = __reduce_add_sync(0xffffffffu, (unsigned)n_general);
+    const unsigned w_idle = __reduce_add_sync(0xffffffffu, (unsigned)n_idle);
+    if (lane == 0) {
+        atomicAdd(&g_bp_path_stats[0], (unsigned long long)w_fast);
+        atomicAdd(&g_bp_path_stats[1], (unsigned long long)w_general);
+        atomicAdd(&g_bp_path_stats[2], (unsigned long long)w_idle);
+        atomicAdd(&g_bp_path_stats[3], (unsigned long long)(clock64() - t_loop));
+    }
+    // the voxel indices are recomputed here rather than kept live across
+    // the view loop (register pressure: 32 accumulators at 96 registers)
+    const int xo = blockIdx.x * 32 + (threadIdx.y & 3) * 8 + (threadIdx.x & 7);
+    const int yo = blockIdx.y * 8 + (threadIdx.y >> 2) * 4 + (threadIdx.x >> 3);
+    if (xo < L.nx && yo < L.ny) {
         T *out = static_cast<T *>(L.vol);
 #pragma unroll
         for (int j = 0; j < BPT_Z; ++j) {
-            const int z = z0 + j;
+            const int z = (int)blockIdx.z * BPT_Z + j;
             if (z < L.nz) {
-                T *o = out + ((size_t)z * L.ny + y) * L.vol_pitch + x;
+                T *o = out + ((size_t)z * L.ny + yo) * L.vol_pitch + xo;
                 float r = acc[j] * L.out_scale;
                 if (L.accumulate) r += lds(o);
                 *o = tot<T>(r);
@@ -636,6 +675,16 @@ b2t_status encode_tensor_map(CUtensorMap *map, CUtensorMapDataType dtype, uint32
                         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(B2T_ERR_CUDA, "cuTensorMapEncodeTiled failed (CUresult %d)", (int)r);
+    return B2T_OK;
+}
+
+b2t_status bp_path_stats_impl(uint64_t *stats)
+{
+    unsigned long long v[4] = {0, 0, 0, 0};
+    B2T_CUDA_TRY(cudaMemcpyFromSymbol(v, g_bp_path_stats, sizeof(v)), "read BP path statistics");
+    const unsigned long long zero[4] = {0, 0, 0, 0};
+    B2T_CUDA_TRY(cudaMemcpyToSymbol(g_bp_path_stats, zero, sizeof(zero)), "clear BP path statistics");
+    for (int k = 0; k < 4; ++k) stats[k] = v[k];
     return B2T_OK;
 }
 

@@ -63,11 +63,12 @@ struct BPLaunch {
 
 // TMA-staged backprojection (bp3d_tma.cu): voxel block, tile geometry and
 // the shared-memory ring the tiles stream through.
-constexpr int BPT_Z = 16;             // voxels per thread along z
+constexpr int BPT_Z = 32;             // voxels per thread along z
 constexpr int BPT_CHUNK = 8;          // tile rows per TMA box; a view loads the chunks its footprint needs
-constexpr int BPT_BV = 64;            // most rows one view's tile may take
-constexpr int BPT_RING_BYTES = 72576; // ring of tile rows (216 f32 rows of 84, 408 f16/bf16 rows of 88);
-                                      // three CTAs of ring + records fit an SM's 228 KB
+constexpr int BPT_BV = 96;            // most rows one view's tile may take
+constexpr int BPT_RING_BYTES = 96768; // ring of tile rows (288 f32 rows of 84, 544 f16/bf16 rows of 88);
+                                      // two CTAs of ring + records fit an SM's 228 KB
+constexpr int BPT_CTAS_PER_SM = 2;    // resident CTAs (96 registers a thread with 32 accumulators)
 constexpr int BPT_SLOTS = 8;          // views in flight at most (barrier pairs and stage records)
 constexpr int BPT_MAX_VIEWS = 640;
 
@@ -92,6 +93,7 @@ inline size_t padded_pu(uint32_t det_u) { return ((size_t)det_u + 4 + 7) & ~(siz
 b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *padded, void *vol, size_t vol_pitch,
                     int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status device_errors_impl(uint32_t *flags);
+b2t_status bp_path_stats_impl(uint64_t *stats);
 
 int dominant_axis(int kind, const b2t_view3d &w, const b2t_dims3d &d);
 void fp_view_coeffs(int kind, const b2t_view3d &w, const b2t_dims3d &d, int dir, FPView &o);

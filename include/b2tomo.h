@@ -63,6 +63,18 @@ b2t_status b2t_set_device(int32_t device);
  * output is incomplete).  Synchronises the device.  The reference has no
  * device-side waits and no counterpart. */
 b2t_status b2t_device_errors(uint32_t *flags);
+/* Read and clear, for the current device, the path statistics of the
+ * TMA-staged cone/parallel backprojection since the last call.  Counts are in
+ * voxel-column views (one thread's column of 32 voxels for one view):
+ * stats[0] took the circular-orbit fast path (detector u fixed along the
+ * column, every sample from the shared-memory tile of the view's footprint);
+ * stats[1] took the general path (non-circular orbits, columns whose rows
+ * leave the tile, views whose footprint does not fit a tile and read global
+ * memory); stats[2] were idle lanes (columns outside the volume).  stats[3]
+ * is the SM cycles the compute warps spent in their view loops, summed over
+ * warps.  Synchronises the device.  A performance diagnostic; the reference
+ * has no counterpart. */
+b2t_status b2t_bp_path_stats(uint64_t stats[4]);
 /* Scratch buffers (padded copies, cell copies, filter operands) come from a
  * stream-ordered memory pool of the library, one per device, that keeps freed
  * blocks cached so repeated calls do not map device memory again.  This
