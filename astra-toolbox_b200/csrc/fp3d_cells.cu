@@ -142,6 +142,64 @@ __global__ void build_cells(const T *__restrict__ vol, size_t pitch, int nx, int
     }
 }
 
+template <typename T>
+__device__ __forceinline__ void store_cell(typename CellT<T>::type *dst, float v00, float v10, float v01, float v11)
+{
+    if constexpr (sizeof(typename CellT<T>::type) == 16) {
+        *dst = make_cell(v00, v10, v01, v11, nullptr);
+    } else {
+        *dst = pack_corners<T>(v00, v10, v01, v11);
+    }
+}
+
+// Builds the columns layout of direction dir (0: slices along x, k1 = y;
+// 1: slices along y, k1 = x; k2 = z for both): cell (j1, s, j2) at
+// (j1 n0 + s) m2 + j2, j = k + 2, m = n + 4.  A CTA stages a tile of the
+// volume in shared memory, read along x, and writes 32 x 32 cells along j2:
+//   dir 0: blockIdx = (j2 tile, s tile, j1), tile[p][zi][xi] = vol(s0 + xi, k1 + p, k2_0 + zi);
+//   dir 1: blockIdx = (j2 tile, j1 tile, s), tile[0][zi][xi] = vol(k1_0 + xi, s, k2_0 + zi).
+// Rows of 33 floats keep the column reads of the write phase conflict-free.
+template <typename T>
+__global__ void __launch_bounds__(256) build_cells_cols(const T *__restrict__ vol, size_t pitch, int nx, int ny,
+                                                        int nz, int dir, typename CellT<T>::type *__restrict__ cells)
+{
+    __shared__ float t[2][33][33];
+    const int n0 = (dir == 0) ? nx : ny;
+    const int m1 = ((dir == 0) ? ny : nx) + 4, m2 = nz + 4;
+    const int j2_0 = blockIdx.x * 32, k2_0 = j2_0 - 2;
+    const int tid = threadIdx.x;
+    const int ji = tid & 31, j2 = j2_0 + ji;
+    if (dir == 0) {
+        const int s0 = blockIdx.y * 32, j1 = blockIdx.z, k1 = j1 - 2;
+        for (int e = tid; e < 2 * 33 * 32; e += 256) {
+            const int xi = e & 31, zi = (e >> 5) % 33, pk = e / (33 * 32);
+            const int x = s0 + xi, y = k1 + pk, z = k2_0 + zi;
+            float val = 0.0f;
+            if (x < nx && y >= 0 && y < ny && z >= 0 && z < nz) val = vload(vol + ((size_t)z * ny + y) * pitch + x);
+            t[pk][zi][xi] = val;
+        }
+        __syncthreads();
+        if (j2 >= m2) return;
+        for (int si = tid >> 5; si < 32 && s0 + si < n0; si += 8)
+            store_cell<T>(cells + ((size_t)j1 * n0 + s0 + si) * m2 + j2, t[0][ji][si], t[1][ji][si], t[0][ji + 1][si],
+                          t[1][ji + 1][si]);
+    } else {
+        const int j1_0 = blockIdx.y * 32, k1_0 = j1_0 - 2, sl = blockIdx.z;
+        for (int e = tid; e < 33 * 33; e += 256) {
+            const int xi = e % 33, zi = e / 33;
+            const int x = k1_0 + xi, z = k2_0 + zi;
+            float val = 0.0f;
+            if (x >= 0 && x < nx && z >= 0 && z < nz) val = vload(vol + ((size_t)z * ny + sl) * pitch + x);
+            t[0][zi][xi] = val;
+        }
+        __syncthreads();
+        if (j2 >= m2) return;
+        for (int i1 = tid >> 5; i1 < 32 && j1_0 + i1 < m1; i1 += 8)
+            store_cell<T>(cells + ((size_t)(j1_0 + i1) * n0 + sl) * m2 + j2, t[0][ji][i1], t[0][ji][i1 + 1],
+                          t[0][ji + 1][i1], t[0][ji + 1][i1 + 1]);
+    }
+}
+
 __device__ __forceinline__ void clip_slices_c(float A, float B, float lo, float hi, float &smin, float &smax)
 {
     if (fabsf(A) < 1e-12f) {
@@ -179,26 +237,138 @@ __device__ __forceinline__ float cell_value(const typename CellT<T>::type *p, fl
     }
 }
 
-// L.vol points at the cell of padded texel (k1 = 0, k2 = 0) of slice 0, i.e.
-// the cell array base + 2 * st2 + 2 (strides in cells).
-//
-// A CTA traces one 32 x VROWS tile of detector pixels for VPC consecutive
-// views (threadIdx.z selects the view).  Neighbouring views sample nearly the
-// same cells at the same slice (the orbit turns by a fraction of a degree
-// per view), and the warps of one CTA share an SM, so the views of a CTA
-// reuse each other's cells in L1 instead of fetching them again from L2.
+// One ray through the rows layout (ray set-up and slice clipping of
+// fp3d_kernel): acc + the sum of its samples times the ray length factor.
+// L.vol points at the cell of slice 0, texels (k1 = 0, k2 = 0); the cell of
+// slice s, texels (k1, k2) is at L.vol + s st0 + k1 + k2 st2 (strides in
+// cells).  UNR independent accumulators keep UNR cell loads in flight.
+template <typename T, int UNR>
+__device__ __forceinline__ float trace_rows(const FPLaunch &L, const FPView &V, float uu, float vv, float acc)
+{
+    using C = typename CellT<T>::type;
+    const float n0 = (float)L.n0;
+    const float den = fmaf(vv, V.e[2], fmaf(uu, V.e[1], V.e[0]));
+    const float inv = 1.0f / den;
+    const float A1 = fmaf(vv, V.m1[2], fmaf(uu, V.m1[1], V.m1[0])) * inv;
+    const float A2 = fmaf(vv, V.m2[2], fmaf(uu, V.m2[1], V.m2[0])) * inv;
+    const float B1 = fmaf(vv, V.n1[2], fmaf(uu, V.n1[1], V.n1[0])) * inv;
+    const float B2 = fmaf(vv, V.n2[2], fmaf(uu, V.n2[1], V.n2[0])) * inv;
+    float smin = 0.0f, smax = n0 - 1.0f;
+    clip_slices_c(A1, B1, -1.6f, (float)L.n1 - 0.4f, smin, smax);
+    clip_slices_c(A2, B2, -1.6f, (float)L.n2 - 0.4f, smin, smax);
+    int s_lo = max(0, (int)ceilf(fmaxf(smin, -1.0f)));
+    int s_hi = min(L.n0 - 1, (int)floorf(fminf(smax, n0)));
+    // sample positions plus one half: texel floor(), weight frac()
+    const float B1h = B1 + 0.5f, B2h = B2 + 0.5f;
+    for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
+        if (texel_ok_f(A1, B1h, s_lo, L.n1) && texel_ok_f(A2, B2h, s_lo, L.n2)) break;
+        ++s_lo;
+    }
+    for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
+        if (texel_ok_f(A1, B1h, s_hi, L.n1) && texel_ok_f(A2, B2h, s_hi, L.n2)) break;
+        --s_hi;
+    }
+    if (!(texel_ok_f(A1, B1h, s_lo, L.n1) && texel_ok_f(A2, B2h, s_lo, L.n2) &&
+          texel_ok_f(A1, B1h, s_hi, L.n1) && texel_ok_f(A2, B2h, s_hi, L.n2)))
+        s_hi = s_lo - 1;
+    // the base texels are monotone in s, so the checks at both ends keep
+    // every access inside the cell grid.  The cell address is formed from
+    // the bits of the rounded-down sums (k + 0x4B400000) with 32 x 32 ->
+    // 64-bit multiply-adds; the constant offset wraps around in 64 bits
+    constexpr uint32_t cb = (uint32_t)sizeof(C);
+    const uint32_t st0b = (uint32_t)(L.st0 * cb), st2b = (uint32_t)(L.st2 * cb);
+    const unsigned long long base0 =
+        reinterpret_cast<unsigned long long>(L.vol) - 0x4B400000ull * ((unsigned long long)st2b + cb);
+    auto sample = [&](int sl) -> float {
+        const float q1 = fmaf(A1, (float)sl, B1h), q2 = fmaf(A2, (float)sl, B2h);
+        const float t1 = __fadd_rd(q1, SPLIT_M), t2 = __fadd_rd(q2, SPLIT_M);
+        const float f1 = q1 - (t1 - SPLIT_M), f2 = q2 - (t2 - SPLIT_M);
+        const unsigned long long a = base0 + (unsigned long long)(uint32_t)sl * st0b +
+                                     (unsigned long long)(uint32_t)__float_as_int(t2) * st2b +
+                                     (unsigned long long)(uint32_t)__float_as_int(t1) * cb;
+        return cell_value<T>(reinterpret_cast<const C *>(a), f1, f2);
+    };
+    float sum[UNR];
+#pragma unroll
+    for (int k = 0; k < UNR; ++k) sum[k] = 0.0f;
+    int s = s_lo;
+    for (; s + UNR - 1 <= s_hi; s += UNR) {
+#pragma unroll
+        for (int k = 0; k < UNR; ++k) sum[k] += sample(s + k);
+    }
+    for (; s <= s_hi; ++s) sum[0] += sample(s);
+#pragma unroll
+    for (int w = UNR / 2; w >= 1; w /= 2) {
+#pragma unroll
+        for (int k = 0; k < w; ++k) sum[k] += sum[k + w];
+    }
+    return fmaf(sum[0], sqrtf(fmaf(A1 * A1, L.f1, fmaf(A2 * A2, L.f2, 1.0f))) * L.mul, acc);
+}
+
+template <typename T>
+__device__ __forceinline__ void store_ray(const FPLaunch &L, int a, int u, int v, float acc)
+{
+    T *out = static_cast<T *>(L.proj) + ((size_t)v * L.na + a) * L.proj_pitch + u;
+    if (L.accumulate) acc += (float)(*out);
+    *out = vstore<T>(acc);
+}
+
+// Rows layout (k1 stride 1), used for z-major views: a CTA traces one
+// 32 x VROWS tile of detector pixels for VPC consecutive views (threadIdx.z
+// selects the view).  Neighbouring views sample nearly the same cells at the
+// same slice (the orbit turns by a fraction of a degree per view), and the
+// warps of one CTA share an SM, so the views of a CTA reuse each other's
+// cells in L1 instead of fetching them again from L2.
 template <typename T, int VPC, int VROWS>
 __global__ void __launch_bounds__(32 * VROWS * VPC, 2048 / (32 * VROWS * VPC)) fp3d_cell_kernel(const __grid_constant__ FPLaunch L)
 {
-    using C = typename CellT<T>::type;
     const int vi = blockIdx.x * VPC + threadIdx.z;
     if (vi >= L.nviews) return;
     const FPView &V = L.views[vi];
     const int u = blockIdx.y * 32 + threadIdx.x;
     const int v = blockIdx.z * VROWS + threadIdx.y;
     if (u >= L.nu || v >= L.nv) return;
+    const int R = L.rays;
+    float acc = 0.0f;
+    for (int iu = 0; iu < R; ++iu) {
+        for (int iv = 0; iv < R; ++iv) {
+            float uu = (float)u + 0.5f - 0.5f * (float)L.nu;
+            float vv = (float)v + 0.5f - 0.5f * (float)L.nv;
+            if (R > 1) {
+                uu += -0.5f + (0.5f + (float)iu) / (float)R;
+                vv += -0.5f + (0.5f + (float)iv) / (float)R;
+            }
+            acc = trace_rows<T, 2>(L, V, uu, vv, acc);
+        }
+    }
+    if (R > 1) acc /= (float)(R * R);
+    store_ray<T>(L, V.a, u, v, acc);
+}
+
+// Columns layout (cell of slice s, texels (k1, k2) at L.vol + s st0 + k1 st1
+// + k2), used for x- and y-major views: a warp traces
+// 32 consecutive detector rows of one column, a CTA VCOLS columns for VPC
+// consecutive views.  For a detector whose v axis is parallel to the
+// volume's z axis (circular orbits, parallel or cone) the rays of one column
+// lie in one plane containing z, so at every slice they share the in-plane
+// texel k1 and their k2 run along the contiguous axis: a warp's 16-byte
+// loads fall on three or four 128-byte lines instead of the seven to nine a
+// detector row needs when its rays cross several k2 rows.  Four loads in
+// flight per thread (40 registers, three CTAs per SM) cover the L2 latency.
+// The ray set-up is the rows tracer's, written out here: the shared form
+// spilled at 40 registers.
+template <typename T, int VPC, int VCOLS>
+__global__ void __launch_bounds__(32 * VCOLS * VPC, 3) fp3d_col_kernel(const __grid_constant__ FPLaunch L)
+{
+    using C = typename CellT<T>::type;
+    const int vi = blockIdx.x * VPC + threadIdx.z;
+    if (vi >= L.nviews) return;
+    const FPView &V = L.views[vi];
+    const int v = blockIdx.z * 32 + threadIdx.x;
+    const int u = blockIdx.y * VCOLS + threadIdx.y;
+    if (u >= L.nu || v >= L.nv) return;
     const C *__restrict__ cells = static_cast<const C *>(L.vol);
-    const long long st0 = L.st0, st2 = L.st2;
+    const long long st0 = L.st0, st1 = L.st1;  // slice and k1 strides; k2 stride 1
     const int R = L.rays;
     const float n0 = (float)L.n0;
     float acc = 0.0f;
@@ -221,7 +391,6 @@ __global__ void __launch_bounds__(32 * VROWS * VPC, 2048 / (32 * VROWS * VPC)) f
             clip_slices_c(A2, B2, -1.6f, (float)L.n2 - 0.4f, smin, smax);
             int s_lo = max(0, (int)ceilf(fmaxf(smin, -1.0f)));
             int s_hi = min(L.n0 - 1, (int)floorf(fminf(smax, n0)));
-            // sample positions plus one half: texel floor(), weight frac()
             const float B1h = B1 + 0.5f, B2h = B2 + 0.5f;
             for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
                 if (texel_ok_f(A1, B1h, s_lo, L.n1) && texel_ok_f(A2, B2h, s_lo, L.n2)) break;
@@ -234,40 +403,36 @@ __global__ void __launch_bounds__(32 * VROWS * VPC, 2048 / (32 * VROWS * VPC)) f
             if (!(texel_ok_f(A1, B1h, s_lo, L.n1) && texel_ok_f(A2, B2h, s_lo, L.n2) &&
                   texel_ok_f(A1, B1h, s_hi, L.n1) && texel_ok_f(A2, B2h, s_hi, L.n2)))
                 s_hi = s_lo - 1;
-            // the base texels are monotone in s, so the checks at both ends
-            // keep every access inside the cell grid.  Cell address of slice
-            // s, texels (k1, k2): cells + s st0 + k2 st2 + k1, formed from the
-            // bits of the rounded-down sums (k + 0x4B400000) with 32 x 32 ->
-            // 64-bit multiply-adds; the constant offset wraps around in 64 bits
-            const uint32_t cb = (uint32_t)sizeof(C), st0b = (uint32_t)(st0 * cb), st2b = (uint32_t)(st2 * cb);
+            constexpr uint32_t cb = (uint32_t)sizeof(C);
+            const uint32_t st0b = (uint32_t)(st0 * cb), st1b = (uint32_t)(st1 * cb);
             const unsigned long long base0 = reinterpret_cast<unsigned long long>(cells) -
-                                             0x4B400000ull * ((unsigned long long)st2b + cb);
+                                             0x4B400000ull * ((unsigned long long)st1b + cb);
             auto sample = [&](int sl) -> float {
                 const float q1 = fmaf(A1, (float)sl, B1h), q2 = fmaf(A2, (float)sl, B2h);
                 const float t1 = __fadd_rd(q1, SPLIT_M), t2 = __fadd_rd(q2, SPLIT_M);
                 const float f1 = q1 - (t1 - SPLIT_M), f2 = q2 - (t2 - SPLIT_M);
                 const unsigned long long a = base0 + (unsigned long long)(uint32_t)sl * st0b +
-                                             (unsigned long long)(uint32_t)__float_as_int(t2) * st2b +
-                                             (unsigned long long)(uint32_t)__float_as_int(t1) * cb;
+                                             (unsigned long long)(uint32_t)__float_as_int(t1) * st1b +
+                                             (unsigned long long)(uint32_t)__float_as_int(t2) * cb;
                 return cell_value<T>(reinterpret_cast<const C *>(a), f1, f2);
             };
-            // two independent accumulators keep two loads in flight per thread
-            float sum0 = 0.0f, sum1 = 0.0f;
+            float sum0 = 0.0f, sum1 = 0.0f, sum2 = 0.0f, sum3 = 0.0f;
             int s = s_lo;
-            for (; s + 1 <= s_hi; s += 2) {
+            for (; s + 3 <= s_hi; s += 4) {
                 sum0 += sample(s);
                 sum1 += sample(s + 1);
+                sum2 += sample(s + 2);
+                sum3 += sample(s + 3);
             }
-            if (s <= s_hi) sum0 += sample(s);
+            for (; s <= s_hi; ++s) sum0 += sample(s);
+            sum0 += sum2;
+            sum1 += sum3;
             const float sc = sqrtf(fmaf(A1 * A1, L.f1, fmaf(A2 * A2, L.f2, 1.0f))) * L.mul;
             acc = fmaf(sum0 + sum1, sc, acc);
         }
     }
     if (R > 1) acc /= (float)(R * R);
-    T *out = static_cast<T *>(L.proj) + ((size_t)v * L.na + V.a) * L.proj_pitch + u;
-    float r = acc;
-    if (L.accumulate) r += (float)(*out);
-    *out = vstore<T>(r);
+    store_ray<T>(L, V.a, u, v, acc);
 }
 
 // Launch shape of the cell forward projector: views per CTA.
@@ -327,6 +492,28 @@ static b2t_status launch_cells(const FPLaunch &P, int nviews, const b2t_dims3d &
     }
 }
 
+template <typename T, int VPC, int VCOLS>
+static b2t_status launch_cols_shape(const FPLaunch &P, int nviews, const b2t_dims3d &d, cudaStream_t s)
+{
+    dim3 grid((unsigned)((nviews + VPC - 1) / VPC), (d.det_u + VCOLS - 1) / VCOLS, (d.det_v + 31) / 32);
+    fp3d_col_kernel<T, VPC, VCOLS><<<grid, dim3(32, VCOLS, VPC), 0, s>>>(P);
+    count_launches(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "fp3d_col_kernel launch");
+    return B2T_OK;
+}
+
+template <typename T>
+static b2t_status launch_cols(const FPLaunch &P, int nviews, const b2t_dims3d &d, const CellShape &shape,
+                              cudaStream_t s)
+{
+    switch (shape.vpc) {
+    case 1: return launch_cols_shape<T, 1, 16>(P, nviews, d, s);
+    case 2: return launch_cols_shape<T, 2, 8>(P, nviews, d, s);
+    case 8: return launch_cols_shape<T, 8, 2>(P, nviews, d, s);
+    default: return launch_cols_shape<T, 4, 4>(P, nviews, d, s);
+    }
+}
+
 template <typename T>
 b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch, void *proj,
                      size_t proj_pitch, int32_t mode, const std::vector<int> &dirs, cudaStream_t s)
@@ -338,7 +525,7 @@ b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
     const int nx = d.vol_x, ny = d.vol_y, nz = d.vol_z;
     Scratch cs[3];
     const C *base[3] = {nullptr, nullptr, nullptr};
-    long long st0[3], st2[3];
+    long long st0[3], st1[3], st2[3];
     for (int dir = 0; dir < 3; ++dir) {
         if (!need[dir]) continue;
         int n0, n1, n2;
@@ -348,18 +535,26 @@ b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
         const long long m1 = n1 + 4, m2 = n2 + 4;
         const size_t count = (size_t)m1 * m2 * n0;
         B2T_TRY(cs[dir].alloc(count * sizeof(C), s, "b2t_fp3d scratch (cells)"));
-        dim3 grid((unsigned)((m1 + 127) / 128), (unsigned)m2, (unsigned)n0);
-        build_cells<T><<<grid, 128, 0, s>>>(static_cast<const T *>(vol), vol_pitch, nx, ny, nz, dir, cs[dir].as<C>());
-        count_launches(1);
-        B2T_CUDA_TRY(cudaGetLastError(), "build_cells launch");
         if (dir == 2) {
+            // rows layout: cell (s, j2, j1) at (s m2 + j2) m1 + j1
+            dim3 grid((unsigned)((m1 + 127) / 128), (unsigned)m2, (unsigned)n0);
+            build_cells<T><<<grid, 128, 0, s>>>(static_cast<const T *>(vol), vol_pitch, nx, ny, nz, dir, cs[dir].as<C>());
             st0[dir] = m1 * m2;
+            st1[dir] = 1;
             st2[dir] = m1;
         } else {
-            st0[dir] = m1;
-            st2[dir] = m1 * n0;
+            // columns layout: cell (j1, s, j2) at (j1 n0 + s) m2 + j2
+            dim3 grid((unsigned)((m2 + 31) / 32), (unsigned)((dir == 0 ? n0 : m1) + 31) / 32,
+                      (unsigned)(dir == 0 ? m1 : n0));
+            build_cells_cols<T><<<grid, 256, 0, s>>>(static_cast<const T *>(vol), vol_pitch, nx, ny, nz, dir,
+                                                     cs[dir].as<C>());
+            st0[dir] = m2;
+            st1[dir] = (long long)n0 * m2;
+            st2[dir] = 1;
         }
-        base[dir] = cs[dir].as<C>() + 2 * st2[dir] + 2;
+        count_launches(1);
+        B2T_CUDA_TRY(cudaGetLastError(), "cell layout launch");
+        base[dir] = cs[dir].as<C>() + 2 * st1[dir] + 2 * st2[dir];
     }
     const CellShape shape = choose_shape(shape_key(g, p, CellDtype<T>::value));
     FPLaunch *Lp = new FPLaunch;
@@ -380,6 +575,7 @@ b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
         else if (dir == 1) { P.n0 = ny; P.n1 = nx; P.n2 = nz; }
         else { P.n0 = nz; P.n1 = nx; P.n2 = ny; }
         P.st0 = st0[dir];
+        P.st1 = st1[dir];
         P.st2 = st2[dir];
         P.vol = base[dir];
         std::vector<int> views;
@@ -393,7 +589,7 @@ b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
                 fp_view_coeffs(g->kind, g->views[a], d, dir, P.views[i]);
                 P.views[i].a = a;
             }
-            st = launch_cells<T>(P, (int)cn, d, shape, s);
+            st = (dir == 2) ? launch_cells<T>(P, (int)cn, d, shape, s) : launch_cols<T>(P, (int)cn, d, shape, s);
             if (st != B2T_OK) break;
         }
     }

@@ -29,7 +29,8 @@ struct FPLaunch {
     const void *vol;        // padded volume, pointing at texel (s=0, k1=0, k2=0)
     void *proj;             // output projections [v][angle][u]
     long long proj_pitch;   // elements
-    long long st0, st2;     // element strides of the marching axis and axis 2 (axis 1 stride is 1)
+    long long st0, st1, st2; // element strides of the marching axis, axis 1 and axis 2 (the direct
+                             // kernel's padded volume has st1 = 1)
     int n0, n1, n2;         // extents along marching axis, axis 1, axis 2
     int nu, nv, na;
     int rays;               // detector supersampling per dimension
