@@ -515,18 +515,18 @@ static b2t_status launch_cols(const FPLaunch &P, int nviews, const b2t_dims3d &d
 }
 
 template <typename T>
-b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch, void *proj,
-                     size_t proj_pitch, int32_t mode, const std::vector<int> &dirs, cudaStream_t s)
+b2t_status build_cells_t(const b2t_geom3d *g, const void *vol, size_t vol_pitch, const bool need[3], cudaStream_t s,
+                         FPCells &c)
 {
     using C = typename CellT<T>::type;
     const b2t_dims3d &d = g->dims;
-    bool need[3] = {false, false, false};
-    for (int dd : dirs) need[dd] = true;
     const int nx = d.vol_x, ny = d.vol_y, nz = d.vol_z;
-    Scratch cs[3];
-    const C *base[3] = {nullptr, nullptr, nullptr};
-    long long st0[3], st1[3], st2[3];
+    c.dtype = CellDtype<T>::value;
+    c.vol_x = d.vol_x;
+    c.vol_y = d.vol_y;
+    c.vol_z = d.vol_z;
     for (int dir = 0; dir < 3; ++dir) {
+        c.base[dir] = nullptr;
         if (!need[dir]) continue;
         int n0, n1, n2;
         if (dir == 0) { n0 = nx; n1 = ny; n2 = nz; }
@@ -534,28 +534,40 @@ b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
         else { n0 = nz; n1 = nx; n2 = ny; }
         const long long m1 = n1 + 4, m2 = n2 + 4;
         const size_t count = (size_t)m1 * m2 * n0;
-        B2T_TRY(cs[dir].alloc(count * sizeof(C), s, "b2t_fp3d scratch (cells)"));
+        if (!c.mem[dir]) c.mem[dir].reset(new Scratch);
+        B2T_TRY(c.mem[dir]->alloc(count * sizeof(C), s, "b2t_fp3d scratch (cells)"));
+        C *cells = c.mem[dir]->as<C>();
         if (dir == 2) {
             // rows layout: cell (s, j2, j1) at (s m2 + j2) m1 + j1
             dim3 grid((unsigned)((m1 + 127) / 128), (unsigned)m2, (unsigned)n0);
-            build_cells<T><<<grid, 128, 0, s>>>(static_cast<const T *>(vol), vol_pitch, nx, ny, nz, dir, cs[dir].as<C>());
-            st0[dir] = m1 * m2;
-            st1[dir] = 1;
-            st2[dir] = m1;
+            build_cells<T><<<grid, 128, 0, s>>>(static_cast<const T *>(vol), vol_pitch, nx, ny, nz, dir, cells);
+            c.st0[dir] = m1 * m2;
+            c.st1[dir] = 1;
+            c.st2[dir] = m1;
         } else {
             // columns layout: cell (j1, s, j2) at (j1 n0 + s) m2 + j2
             dim3 grid((unsigned)((m2 + 31) / 32), (unsigned)((dir == 0 ? n0 : m1) + 31) / 32,
                       (unsigned)(dir == 0 ? m1 : n0));
-            build_cells_cols<T><<<grid, 256, 0, s>>>(static_cast<const T *>(vol), vol_pitch, nx, ny, nz, dir,
-                                                     cs[dir].as<C>());
-            st0[dir] = m2;
-            st1[dir] = (long long)n0 * m2;
-            st2[dir] = 1;
+            build_cells_cols<T><<<grid, 256, 0, s>>>(static_cast<const T *>(vol), vol_pitch, nx, ny, nz, dir, cells);
+            c.st0[dir] = m2;
+            c.st1[dir] = (long long)n0 * m2;
+            c.st2[dir] = 1;
         }
         count_launches(1);
         B2T_CUDA_TRY(cudaGetLastError(), "cell layout launch");
-        base[dir] = cs[dir].as<C>() + 2 * st1[dir] + 2 * st2[dir];
+        c.base[dir] = cells + 2 * c.st1[dir] + 2 * c.st2[dir];
     }
+    return B2T_OK;
+}
+
+template <typename T>
+b2t_status project_cells_t(const b2t_geom3d *g, const b2t_params3d *p, const FPCells &c, void *proj,
+                           size_t proj_pitch, int32_t mode, const std::vector<int> &dirs, cudaStream_t s)
+{
+    const b2t_dims3d &d = g->dims;
+    const int nx = d.vol_x, ny = d.vol_y, nz = d.vol_z;
+    bool need[3] = {false, false, false};
+    for (int dd : dirs) need[dd] = true;
     const CellShape shape = choose_shape(shape_key(g, p, CellDtype<T>::value));
     FPLaunch *Lp = new FPLaunch;
     FPLaunch &P = *Lp;
@@ -574,10 +586,10 @@ b2t_status run_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
         if (dir == 0) { P.n0 = nx; P.n1 = ny; P.n2 = nz; }
         else if (dir == 1) { P.n0 = ny; P.n1 = nx; P.n2 = nz; }
         else { P.n0 = nz; P.n1 = nx; P.n2 = ny; }
-        P.st0 = st0[dir];
-        P.st1 = st1[dir];
-        P.st2 = st2[dir];
-        P.vol = base[dir];
+        P.st0 = c.st0[dir];
+        P.st1 = c.st1[dir];
+        P.st2 = c.st2[dir];
+        P.vol = c.base[dir];
         std::vector<int> views;
         for (uint32_t a = 0; a < d.angles; ++a)
             if (dirs[a] == dir) views.push_back((int)a);
@@ -652,12 +664,45 @@ b2t_status fp3d_autotune_impl(const b2t_geom3d *g, const b2t_params3d *p, const 
     return B2T_OK;
 }
 
+FPCells::FPCells() = default;
+FPCells::~FPCells() = default;
+
+b2t_status fp3d_cells_build(const b2t_geom3d *g, const void *vol, size_t vol_pitch, int32_t dtype, const bool need[3],
+                            cudaStream_t s, FPCells &c)
+{
+    if (vol_pitch == 0) vol_pitch = g->dims.vol_x;
+    if (dtype == B2T_F32) return build_cells_t<float>(g, vol, vol_pitch, need, s, c);
+    if (dtype == B2T_F16) return build_cells_t<__half>(g, vol, vol_pitch, need, s, c);
+    return build_cells_t<__nv_bfloat16>(g, vol, vol_pitch, need, s, c);
+}
+
+b2t_status fp3d_cells_project(const b2t_geom3d *g, const b2t_params3d *p, const FPCells &c, void *proj,
+                              size_t proj_pitch, int32_t mode, cudaStream_t s)
+{
+    const b2t_dims3d &d = g->dims;
+    if (d.vol_x != c.vol_x || d.vol_y != c.vol_y || d.vol_z != c.vol_z)
+        return fail(B2T_ERR_INVALID_ARG, "fp3d_cells_project: the cells were built for another volume");
+    if (proj_pitch == 0) proj_pitch = d.det_u;
+    std::vector<int> dirs(d.angles);
+    for (uint32_t a = 0; a < d.angles; ++a) {
+        dirs[a] = dominant_axis(g->kind, g->views[a], d);
+        if (!c.base[dirs[a]]) return fail(B2T_ERR_INVALID_ARG, "fp3d_cells_project: no cells for view %u", a);
+    }
+    if (c.dtype == B2T_F32) return project_cells_t<float>(g, p, c, proj, proj_pitch, mode, dirs, s);
+    if (c.dtype == B2T_F16) return project_cells_t<__half>(g, p, c, proj, proj_pitch, mode, dirs, s);
+    return project_cells_t<__nv_bfloat16>(g, p, c, proj, proj_pitch, mode, dirs, s);
+}
+
 b2t_status fp3d_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch, void *proj,
                       size_t proj_pitch, int32_t dtype, int32_t mode, const std::vector<int> &dirs, cudaStream_t s)
 {
-    if (dtype == B2T_F32) return run_cells<float>(g, p, vol, vol_pitch, proj, proj_pitch, mode, dirs, s);
-    if (dtype == B2T_F16) return run_cells<__half>(g, p, vol, vol_pitch, proj, proj_pitch, mode, dirs, s);
-    return run_cells<__nv_bfloat16>(g, p, vol, vol_pitch, proj, proj_pitch, mode, dirs, s);
+    bool need[3] = {false, false, false};
+    for (int dd : dirs) need[dd] = true;
+    FPCells c;
+    B2T_TRY(fp3d_cells_build(g, vol, vol_pitch, dtype, need, s, c));
+    if (dtype == B2T_F32) return project_cells_t<float>(g, p, c, proj, proj_pitch, mode, dirs, s);
+    if (dtype == B2T_F16) return project_cells_t<__half>(g, p, c, proj, proj_pitch, mode, dirs, s);
+    return project_cells_t<__nv_bfloat16>(g, p, c, proj, proj_pitch, mode, dirs, s);
 }
 
 }  // namespace b2t

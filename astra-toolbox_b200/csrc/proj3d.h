@@ -5,6 +5,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <vector>
 
 #include "b2tomo.h"
@@ -106,6 +107,29 @@ bool force_simple_bp();
 bool force_simple_fp();
 b2t_status fp3d_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch, void *proj,
                       size_t proj_pitch, int32_t dtype, int32_t mode, const std::vector<int> &dirs, cudaStream_t s);
+
+// The cell copies of one volume for the cell forward projector
+// (fp3d_cells.cu), built once and projected by any number of calls over
+// subsets of the views (the streamed executor's angle blocks).
+class Scratch;
+struct FPCells {
+    FPCells();
+    ~FPCells();
+    FPCells(const FPCells &) = delete;
+    FPCells &operator=(const FPCells &) = delete;
+    std::unique_ptr<Scratch> mem[3];
+    const void *base[3] = {nullptr, nullptr, nullptr};  // cell of texels (0, 0), slice 0, per marching axis
+    long long st0[3] = {0, 0, 0}, st1[3] = {0, 0, 0}, st2[3] = {0, 0, 0};
+    int32_t dtype = B2T_F32;
+    uint32_t vol_x = 0, vol_y = 0, vol_z = 0;
+};
+// Builds the cells of the marching axes marked in need[] (x, y, z).
+b2t_status fp3d_cells_build(const b2t_geom3d *g, const void *vol, size_t vol_pitch, int32_t dtype, const bool need[3],
+                            cudaStream_t s, FPCells &c);
+// proj (=|+=) FP of the volume the cells hold, for the views of g (same
+// volume dimensions as at build time; every view's marching axis built).
+b2t_status fp3d_cells_project(const b2t_geom3d *g, const b2t_params3d *p, const FPCells &c, void *proj,
+                              size_t proj_pitch, int32_t mode, cudaStream_t s);
 
 // Zero-padded FP32 volume copies (2-voxel border): xyz = [z+2][y+2][x+2],
 // zxy = [z+2][x+2][y+2] (either may be null).

@@ -55,20 +55,27 @@ struct Req {
     uint32_t slab, block;  // z-slab thickness and angle block size
 };
 
+// A device buffer of a streamed call, from the library's stream-ordered
+// memory pool (cached between calls, so repeated calls map no memory),
+// allocated and released on the worker's compute stream.
 struct DevBuf {
     void *p = nullptr;
+    cudaStream_t s = nullptr;
     ~DevBuf()
     {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, s);
     }
-    b2t_status alloc(size_t bytes, const char *what)
+    b2t_status alloc(size_t bytes, cudaStream_t st, const char *what)
     {
-        const cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+        cudaError_t e = cudaSuccess;
+        cudaMemPool_t pool = scratch_pool(e);
+        if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, pool, st);
         if (e != cudaSuccess) {
             p = nullptr;
             (void)cudaGetLastError();
             return cuda_fail(e, what);
         }
+        s = st;
         return B2T_OK;
     }
     float *f() const { return static_cast<float *>(p); }
@@ -86,6 +93,16 @@ struct Event {
     ~Event()
     {
         if (e) cudaEventDestroy(e);
+    }
+};
+// Drains a worker's three streams when it leaves, on every path, before its
+// buffers go back to the pool (declared after the buffers, so destroyed first).
+struct Drain {
+    Stream *st[3];
+    ~Drain()
+    {
+        for (Stream *x : st)
+            if (x->s) cudaStreamSynchronize(x->s);
     }
 };
 
@@ -159,19 +176,27 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
     for (Stream *st : {&cs, &hs, &os})
         B2T_CUDA_TRY(cudaStreamCreateWithFlags(&st->s, cudaStreamNonBlocking), "stream create");
     DevBuf inb[2], outb[2], padded;
-    Event in_ready[2], in_free[2], out_done[2], out_copied[2];
+    Drain drain{{&cs, &hs, &os}};
+    Event in_ready[2], in_free[2], out_done[2], out_copied[2], allocated;
     for (int k = 0; k < 2; ++k) {
-        if (k == 0 || !resident) B2T_TRY(inb[k].alloc(in_elems * sizeof(float), "streamed input buffer"));
-        B2T_TRY(outb[k].alloc(out_elems * sizeof(float), "streamed output buffer"));
-        for (Event *e : {&in_ready[k], &in_free[k], &out_done[k], &out_copied[k]})
-            B2T_CUDA_TRY(cudaEventCreateWithFlags(&e->e, cudaEventDisableTiming), "event create");
-        B2T_CUDA_TRY(cudaEventRecord(in_free[k].e, cs.s), "event record");
-        B2T_CUDA_TRY(cudaEventRecord(out_copied[k].e, os.s), "event record");
+        if (k == 0 || !resident) B2T_TRY(inb[k].alloc(in_elems * sizeof(float), cs.s, "streamed input buffer"));
+        B2T_TRY(outb[k].alloc(out_elems * sizeof(float), cs.s, "streamed output buffer"));
     }
     if (R.op == Op::fdk) {
         b2t_dims3d db = d;
         db.angles = R.block;
-        B2T_TRY(padded.alloc(padded_proj_bytes(db, B2T_F32), "streamed FDK filtered block"));
+        B2T_TRY(padded.alloc(padded_proj_bytes(db, B2T_F32), cs.s, "streamed FDK filtered block"));
+    }
+    // the copy streams touch the buffers only after their allocation
+    B2T_CUDA_TRY(cudaEventCreateWithFlags(&allocated.e, cudaEventDisableTiming), "event create");
+    B2T_CUDA_TRY(cudaEventRecord(allocated.e, cs.s), "event record");
+    B2T_CUDA_TRY(cudaStreamWaitEvent(hs.s, allocated.e, 0), "wait");
+    B2T_CUDA_TRY(cudaStreamWaitEvent(os.s, allocated.e, 0), "wait");
+    for (int k = 0; k < 2; ++k) {
+        for (Event *e : {&in_ready[k], &in_free[k], &out_done[k], &out_copied[k]})
+            B2T_CUDA_TRY(cudaEventCreateWithFlags(&e->e, cudaEventDisableTiming), "event create");
+        B2T_CUDA_TRY(cudaEventRecord(in_free[k].e, cs.s), "event record");
+        B2T_CUDA_TRY(cudaEventRecord(out_copied[k].e, os.s), "event record");
     }
     auto upload = [&](uint32_t c, int buf) -> b2t_status {
         const uint32_t c0 = c * in_step, cn = std::min(in_step, in_n - c0);
@@ -182,6 +207,19 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
         return B2T_OK;
     };
     if (resident) B2T_TRY(upload(0, 0));
+    // a resident FP input (the whole volume in one slab) is laid out in
+    // cells once; every angle block projects from them
+    FPCells cells;
+    bool have_cells = false;
+    if (fp && resident && R.params.kernel == B2T_KER_DEFAULT && !force_simple_fp()) {
+        bool need[3] = {false, false, false};
+        for (uint32_t a = 0; a < d.angles; ++a) need[dominant_axis(G.kind, G.views[a], d)] = true;
+        B2T_CUDA_TRY(cudaStreamWaitEvent(cs.s, in_ready[0].e, 0), "wait");
+        const b2t_status bs = fp3d_cells_build(&G, inb[0].f(), 0, B2T_F32, need, cs.s, cells);
+        if (bs == B2T_OK) have_cells = true;
+        else if (bs == B2T_ERR_NO_MEMORY) clear_error();  // project block by block instead
+        else return bs;
+    }
 
     SubGeom sub;
     for (size_t jn = 0; jn < jobs.size(); ++jn) {
@@ -211,7 +249,8 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
             first = false;
             if (fp) {
                 sub.set(G, o0, on, c0, cn);
-                B2T_TRY(fp3d_impl(&sub.g, &R.params, inb[ib].f(), 0, obuf, 0, B2T_F32, mode, cs.s));
+                if (have_cells) B2T_TRY(fp3d_cells_project(&sub.g, &R.params, cells, obuf, 0, mode, cs.s));
+                else B2T_TRY(fp3d_impl(&sub.g, &R.params, inb[ib].f(), 0, obuf, 0, B2T_F32, mode, cs.s));
             } else if (R.op == Op::bp) {
                 sub.set(G, c0, cn, o0, on);
                 B2T_TRY(bp3d_impl(&sub.g, &R.params, inb[ib].f(), 0, obuf, 0, B2T_F32, mode, cs.s));
@@ -289,6 +328,12 @@ b2t_status stream3d_plan_impl(int32_t op, const b2t_geom3d *g, const b2t_stream_
         z = std::min((double)d.vol_z, std::floor((B - a * view * pix_in) / (plane * vox_out)));
         if (z < 1) return fail(B2T_ERR_NO_MEMORY, "%s: one volume slice does not fit %zu bytes", who, budget);
     }
+    // angle blocks of at most an eighth of the views (and at least 16 views):
+    // the FP downloads one block while it computes the next, the BP and FDK
+    // upload the next block while they compute one, so transfers overlap
+    // compute even when everything would fit at once
+    const double overlap_block = std::max(16.0, std::ceil(d.angles / 8.0));
+    a = std::min(a, overlap_block);
     slab = (uint32_t)z;
     block = (uint32_t)a;
     return B2T_OK;

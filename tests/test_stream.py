@@ -34,13 +34,15 @@ def _plan(lib, geom, op, budget):
 
 
 def test_stream_plan_splits_by_budget(astra, geo):
-    """The split follows the budget: everything in one piece when it fits,
-    slabs and blocks when it does not, and an error below one slice/view."""
+    """The split follows the budget: the whole volume in one slab when it
+    fits, with angle blocks of at most an eighth of the views (at least 16)
+    so that transfers overlap compute; thinner slabs and smaller blocks when
+    it does not fit, and an error below one slice/view."""
     lib = importlib.import_module("astra-toolbox_b200._lib").load()
     vg, pg = _geom(astra)
     g = geo.Geometry3D(vg, pg)
     st, z, a = _plan(lib, g, 0, 1 << 40)
-    assert st == 0 and (z, a) == (96, 96)
+    assert st == 0 and (z, a) == (96, 16)
     st, z, a = _plan(lib, g, 0, 8_000_000)
     assert st == 0 and 1 <= z < 96 and 1 <= a < 96
     for op in (1, 2):
