@@ -250,7 +250,27 @@ __device__ __forceinline__ float sample_det(const CylBPLaunch &L, int a, float q
     return fmaf(tv, a1 - a0, a0);
 }
 
-constexpr int CYL_BP_Z = 8;
+// sample_det with the u split done once for a column of voxels: ku, tu and
+// the validity of columns ku, ku + 1 (cu0, cu1) from sample_det's rules
+__device__ __forceinline__ float sample_det_col(const CylBPLaunch &L, const float *row, int ku, float tu, bool cu0,
+                                                bool cu1, float qv)
+{
+    if (!(fabsf(qv) < 1.0e7f)) return 0.0f;  // also NaN
+    const float fv = floorf(qv);
+    const int kv = (int)fv;
+    const float tv = qv - fv;
+    if (kv < -1 || kv >= L.nv) return 0.0f;
+    const long long pv = (long long)L.na * L.proj_pitch;
+    const bool r0 = kv >= 0, r1 = kv + 1 < L.nv;
+    const float *p0 = row + (long long)kv * pv + ku;
+    const float v00 = (cu0 && r0) ? __ldg(p0) : 0.0f, v10 = (cu1 && r0) ? __ldg(p0 + 1) : 0.0f;
+    const float v01 = (cu0 && r1) ? __ldg(p0 + pv) : 0.0f, v11 = (cu1 && r1) ? __ldg(p0 + pv + 1) : 0.0f;
+    const float a0 = fmaf(tu, v10 - v00, v00);
+    const float a1 = fmaf(tu, v11 - v01, v01);
+    return fmaf(tv, a1 - a0, a0);
+}
+
+constexpr int CYL_BP_Z = 16;
 
 __global__ void __launch_bounds__(256) bp3d_cyl_kernel(const __grid_constant__ CylBPLaunch L)
 {
@@ -270,6 +290,33 @@ __global__ void __launch_bounds__(256) bp3d_cyl_kernel(const __grid_constant__ C
         float rb = fmaf(fz0, C.cb.z, fmaf(fy, C.cb.y, fmaf(fx, C.cb.x, C.cb.w)));
         float rc = fmaf(fz0, C.cc.z, fmaf(fy, C.cc.y, fmaf(fx, C.cc.x, C.cc.w)));
         const float cq = fmaf(C.sa, C.sa, fmaf(C.sb, C.sb, -C.r * C.r));
+        if (C.ca.z == 0.0f && C.cb.z == 0.0f) {
+            // cylinder axis along z: the ray's in-plane part does not change
+            // along the voxel column, so t and the hit angle are the
+            // column's (the same values the general loop computes per voxel)
+            const float qa = fmaf(ra, ra, rb * rb);
+            const float qb = fmaf(ra, C.sa, rb * C.sb);
+            const float disc = fmaf(qb, qb, -qa * cq);
+            if (!(disc >= 0.0f && qa > 0.0f)) continue;
+            const float t = (sqrtf(disc) - qb) / qa;
+            const float th = asinf(fmaf(t, rb, C.sb) / C.r) / C.ut;
+            const float qu = th + 0.5f * (float)L.nu - 0.5f;
+            if (!(fabsf(qu) < 1.0e7f)) continue;
+            const float fu = floorf(qu);
+            const int ku = (int)fu;
+            const float tu = qu - fu;
+            if (ku < -1 || ku >= L.nu) continue;
+            const bool cu0 = ku >= 0, cu1 = ku + 1 < L.nu;
+            const float *row = L.proj + (size_t)(L.a0 + i) * L.proj_pitch;
+            const float w = t * t;
+#pragma unroll
+            for (int j = 0; j < CYL_BP_Z; ++j) {
+                const float vv = fmaf(t, rc, C.sc) * C.inv_norm_v;
+                acc[j] = fmaf(sample_det_col(L, row, ku, tu, cu0, cu1, vv + 0.5f * (float)L.nv - 0.5f), w, acc[j]);
+                rc = fmaf(L.vsz, C.cc.z, rc);
+            }
+            continue;
+        }
 #pragma unroll
         for (int j = 0; j < CYL_BP_Z; ++j) {
             // |smc_ab + t r_ab| = R, larger root
