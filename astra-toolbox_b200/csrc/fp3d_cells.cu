@@ -357,8 +357,8 @@ __global__ void __launch_bounds__(32 * VROWS * VPC, 2048 / (32 * VROWS * VPC)) f
 // flight per thread (40 registers, three CTAs per SM) cover the L2 latency.
 // The ray set-up is the rows tracer's, written out here: the shared form
 // spilled at 40 registers.
-template <typename T, int VPC, int VCOLS>
-__global__ void __launch_bounds__(32 * VCOLS * VPC, 3) fp3d_col_kernel(const __grid_constant__ FPLaunch L)
+template <typename T, int VPC, int VCOLS, bool IDX32>
+__global__ void __launch_bounds__(32 * VCOLS * VPC, IDX32 ? 4 : 3) fp3d_col_kernel(const __grid_constant__ FPLaunch L)
 {
     using C = typename CellT<T>::type;
     const int vi = blockIdx.x * VPC + threadIdx.z;
@@ -407,14 +407,27 @@ __global__ void __launch_bounds__(32 * VCOLS * VPC, 3) fp3d_col_kernel(const __g
             const uint32_t st0b = (uint32_t)(st0 * cb), st1b = (uint32_t)(st1 * cb);
             const unsigned long long base0 = reinterpret_cast<unsigned long long>(cells) -
                                              0x4B400000ull * ((unsigned long long)st1b + cb);
+            // IDX32 (a cell array of fewer than 2^32 cells): the cell index
+            // from the array's first cell, k + 2 >= 0 on both plane axes, in
+            // 32-bit arithmetic (the constant offset wraps around), then one
+            // wide multiply-add for the address; 32 registers, four CTAs per SM
+            const C *arr = cells - 2 * st1 - 2;
+            const uint32_t s0 = (uint32_t)st0, s1 = (uint32_t)st1;
+            const uint32_t ibase = 2u * s1 + 2u - 0x4B400000u * (s1 + 1u);
             auto sample = [&](int sl) -> float {
                 const float q1 = fmaf(A1, (float)sl, B1h), q2 = fmaf(A2, (float)sl, B2h);
                 const float t1 = __fadd_rd(q1, SPLIT_M), t2 = __fadd_rd(q2, SPLIT_M);
                 const float f1 = q1 - (t1 - SPLIT_M), f2 = q2 - (t2 - SPLIT_M);
-                const unsigned long long a = base0 + (unsigned long long)(uint32_t)sl * st0b +
-                                             (unsigned long long)(uint32_t)__float_as_int(t1) * st1b +
-                                             (unsigned long long)(uint32_t)__float_as_int(t2) * cb;
-                return cell_value<T>(reinterpret_cast<const C *>(a), f1, f2);
+                if constexpr (IDX32) {
+                    const uint32_t idx = (uint32_t)sl * s0 + (uint32_t)__float_as_int(t1) * s1 +
+                                         (uint32_t)__float_as_int(t2) + ibase;
+                    return cell_value<T>(arr + idx, f1, f2);
+                } else {
+                    const unsigned long long a = base0 + (unsigned long long)(uint32_t)sl * st0b +
+                                                 (unsigned long long)(uint32_t)__float_as_int(t1) * st1b +
+                                                 (unsigned long long)(uint32_t)__float_as_int(t2) * cb;
+                    return cell_value<T>(reinterpret_cast<const C *>(a), f1, f2);
+                }
             };
             float sum0 = 0.0f, sum1 = 0.0f, sum2 = 0.0f, sum3 = 0.0f;
             int s = s_lo;
@@ -496,7 +509,12 @@ template <typename T, int VPC, int VCOLS>
 static b2t_status launch_cols_shape(const FPLaunch &P, int nviews, const b2t_dims3d &d, cudaStream_t s)
 {
     dim3 grid((unsigned)((nviews + VPC - 1) / VPC), (d.det_u + VCOLS - 1) / VCOLS, (d.det_v + 31) / 32);
-    fp3d_col_kernel<T, VPC, VCOLS><<<grid, dim3(32, VCOLS, VPC), 0, s>>>(P);
+    // the cell count of the columns layout, (n1 + 4) n0 (n2 + 4)
+    const unsigned long long cells = (unsigned long long)(P.n1 + 4) * (unsigned long long)P.st1;
+    if (cells < (1ull << 32))
+        fp3d_col_kernel<T, VPC, VCOLS, true><<<grid, dim3(32, VCOLS, VPC), 0, s>>>(P);
+    else
+        fp3d_col_kernel<T, VPC, VCOLS, false><<<grid, dim3(32, VCOLS, VPC), 0, s>>>(P);
     count_launches(1);
     B2T_CUDA_TRY(cudaGetLastError(), "fp3d_col_kernel launch");
     return B2T_OK;
