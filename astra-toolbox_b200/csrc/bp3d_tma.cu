@@ -31,6 +31,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 
 #include "b2t_internal.h"
@@ -81,24 +82,20 @@ __device__ __forceinline__ void split_texel_t(float qm, int &k, float &f)
 }
 
 // shared-memory texel at 32-bit shared-window address a
-template <typename T> __device__ __forceinline__ float lds_sh(uint32_t a);
-template <> __device__ __forceinline__ float lds_sh<float>(uint32_t a)
+// Shared-memory load at 32-bit shared address a + OFF (OFF an immediate of
+// the instruction, so the four texels of a sample share one address register).
+template <typename T, int OFF> __device__ __forceinline__ float lds_sh(uint32_t a)
 {
-    float v;
-    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
-    return v;
-}
-template <> __device__ __forceinline__ float lds_sh<__half>(uint32_t a)
-{
-    unsigned short v;
-    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
-    return __half2float(__ushort_as_half(v));
-}
-template <> __device__ __forceinline__ float lds_sh<__nv_bfloat16>(uint32_t a)
-{
-    unsigned short v;
-    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
-    return __bfloat162float(__ushort_as_bfloat16(v));
+    if constexpr (sizeof(T) == 4) {
+        float v;
+        asm volatile("ld.shared.f32 %0, [%1+%2];" : "=f"(v) : "r"(a), "n"(OFF));
+        return v;
+    } else {
+        unsigned short v;
+        asm volatile("ld.shared.u16 %0, [%1+%2];" : "=h"(v) : "r"(a), "n"(OFF));
+        if constexpr (std::is_same<T, __half>::value) return __half2float(__ushort_as_half(v));
+        else return __bfloat162float(__ushort_as_bfloat16(v));
+    }
 }
 
 // Tile width and ring row pitch in texels: a TMA box row must be a multiple
@@ -407,8 +404,8 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
                     const float t = __fadd_rd(q, M);
                     const float fv = q - (t - M);
                     const uint32_t a = (uint32_t)__float_as_int(t) * ROWB + abase;
-                    const float v00 = lds_sh<T>(a), v10 = lds_sh<T>(a + sizeof(T));
-                    const float v01 = lds_sh<T>(a + ROWB), v11 = lds_sh<T>(a + ROWB + sizeof(T));
+                    const float v00 = lds_sh<T, 0>(a), v10 = lds_sh<T, (int)sizeof(T)>(a);
+                    const float v01 = lds_sh<T, (int)ROWB>(a), v11 = lds_sh<T, (int)(ROWB + sizeof(T))>(a);
                     const float av = fmaf(fu, v10 - v00, v00);
                     const float bv = fmaf(fu, v11 - v01, v01);
                     acc[j] = fmaf(fmaf(fv, bv - av, av), w, acc[j]);
