@@ -105,3 +105,35 @@ def test_memory_budget_keeps_results(astra):
     finally:
         astra.set_gpu_index(0, memory=0)
     assert rel_l2(got, want) < 1e-5
+
+
+@pytest.mark.gpu
+def test_host_entry_points_whole_volume(astra):
+    """With no budget the whole volume fits: the streamed FP lays the volume
+    out in cells once and projects it in angle blocks (an eighth of the views
+    each), the streamed BP uploads angle blocks while it computes.  The FP
+    equals the device FP exactly (every ray is computed by the same kernel);
+    the BP equals it up to the order in which the blocks are summed."""
+    import torch
+    P = importlib.import_module("astra-toolbox_b200.projector")
+    phantom = importlib.import_module("astra-toolbox_b200.phantom")
+    vg, pg = _geom(astra)
+    pr = P.Projector3D(pg, vg)
+    astra.set_gpu_index(0, memory=0)
+    z, a = P.stream_plan(pr, 'fp')
+    assert z == pr.vol_shape[0] and a == 16  # one slab, 96 views in blocks of 16
+    vol = phantom.ellipsoids(pr.vol_shape, 8, seed=2, axes=(5.0, 30.0), device='cuda')
+    dproj = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(vol, dproj)
+    hvol = vol.cpu().pin_memory()
+    hproj = torch.zeros(pr.proj_shape).pin_memory()
+    P.fp3d_host(pr, hvol, hproj)
+    assert torch.equal(hproj, dproj.cpu())
+    drec = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(dproj, drec)
+    hrec = torch.zeros(pr.vol_shape).pin_memory()
+    P.bp3d_host(pr, hproj, hrec)
+    assert rel_l2(hrec.numpy(), drec.cpu().numpy()) < 1e-6
+    # accumulate onto the host arrays
+    P.fp3d_host(pr, hvol, hproj, mode=0)
+    assert rel_l2(hproj.numpy(), 2 * dproj.cpu().numpy()) < 1e-6
