@@ -766,12 +766,22 @@ def main():
         peak_on = onchip["smem"]
     alg_bytes = units * 4 * esz
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
+    # DRAM bytes (read + write) of the dominant call's launches, from one ncu
+    # capture of this exact workload (dram__bytes_read.sum + write.sum, one
+    # pass; profiles/dram_traffic_cone_fpbp_512cube_720views.md); null for
+    # other workloads, which were not captured
+    traffic = None
+    if (args.n, args.views, args.det, args.dtype) == (N_VOX, N_ANG, N_DET, "float32"):
+        traffic = {"fp": (79.36 + 1.15 + 76.48 + 1.14) * 1e9, "bp": (15.92 + 0.533 + 0.948 + 0.502) * 1e9}[dom]
     hbm_achieved = hbm_bytes / (dom_ms * 1e-3) / 1e9
     roofline = {"bound": "l1" if dom == "fp" else "smem",
                 "kernel": "b2t_fp3d" if dom == "fp" else "b2t_bp3d",
                 "achieved": achieved, "peak": peak_on, "unit": "GB/s",
                 "frac": (achieved / peak_on) if peak_on else None,
-                "traffic": None, "units_per_launch": units, "bytes_per_unit": 4 * esz,
+                "traffic": traffic, "units_per_launch": units, "bytes_per_unit": 4 * esz,
+                "traffic_note": "DRAM bytes of one whole call (the FP's x- and y-major launches, or the BP's "
+                                "640- and 80-view launches) from one ncu capture of this workload; the "
+                                "cell / tile traffic stays on chip, DRAM moves ~1/26 of the algorithmic bytes",
                 "peak_source": "measured on this GPU by b2t_onchip_peak (16-byte streaming loads)",
                 "onchip_peaks_gbs": onchip,
                 "hbm": {"achieved": hbm_achieved, "peak": peak_hbm, "frac": hbm_achieved / peak_hbm,
