@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(32 * VROWS * VPC, 2048 / (32 * VROWS * VPC)) f
 // The ray set-up is the rows tracer's, written out here: the shared form
 // spilled at 40 registers.
 template <typename T, int VPC, int VCOLS, bool IDX32>
-__global__ void __launch_bounds__(32 * VCOLS * VPC, IDX32 ? 4 : 3) fp3d_col_kernel(const __grid_constant__ FPLaunch L)
+__global__ void __launch_bounds__(32 * VCOLS * VPC, (IDX32 ? 2048 : 1536) / (32 * VCOLS * VPC)) fp3d_col_kernel(const __grid_constant__ FPLaunch L)
 {
     using C = typename CellT<T>::type;
     const int vi = blockIdx.x * VPC + threadIdx.z;
