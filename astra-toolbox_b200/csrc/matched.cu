@@ -144,6 +144,111 @@ __global__ void __launch_bounds__(256) fp3d_transpose_kernel(const __grid_consta
     }
 }
 
+__device__ __forceinline__ void red_add_v4(float4 *p, float a, float b, float c, float d)
+{
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+
+// Transpose of the forward projector for x- and y-major views, in the cell
+// space of its columns layout: a sample with base texel (k1, k2) at slice s
+// adds its four bilinear taps (weights of corners (k1, k2), (k1 + 1, k2),
+// (k1, k2 + 1), (k1 + 1, k2 + 1)) to the 16-byte accumulator of cell
+// (k1, s, k2), one vector reduction per sample instead of four scalar
+// atomics; fold_cells then gathers each voxel's taps from the four cells
+// around it.  A warp takes 32 rows of one detector column, so its
+// reductions fall on a few contiguous lines.  L.vol is the accumulator's
+// first cell (j1 = j2 = 0), index (j1 n0 + s) (n2 + 4) + j2, j = k + 2.
+template <typename T>
+__global__ void __launch_bounds__(256) fp3d_transpose_cols_kernel(const __grid_constant__ FPLaunch L)
+{
+    const FPView &V = L.views[blockIdx.x];
+    const int v = blockIdx.z * 32 + threadIdx.x;
+    const int u = blockIdx.y * 8 + threadIdx.y;
+    if (u >= L.nu || v >= L.nv) return;
+    float4 *cacc = static_cast<float4 *>(const_cast<void *>(L.vol));
+    const T *pin = static_cast<const T *>(L.proj) + ((size_t)v * L.na + V.a) * L.proj_pitch + u;
+    float val = ldm(pin);
+    if (val == 0.0f) return;
+    const int R = L.rays;
+    if (R > 1) val /= (float)(R * R);
+    const float n0 = (float)L.n0;
+    const long long m2 = L.n2 + 4;
+    for (int iu = 0; iu < R; ++iu) {
+        for (int iv = 0; iv < R; ++iv) {
+            float uu = (float)u + 0.5f - 0.5f * (float)L.nu;
+            float vv = (float)v + 0.5f - 0.5f * (float)L.nv;
+            if (R > 1) {
+                uu += -0.5f + (0.5f + (float)iu) / (float)R;
+                vv += -0.5f + (0.5f + (float)iv) / (float)R;
+            }
+            const float den = fmaf(vv, V.e[2], fmaf(uu, V.e[1], V.e[0]));
+            const float inv = 1.0f / den;
+            const float A1 = fmaf(vv, V.m1[2], fmaf(uu, V.m1[1], V.m1[0])) * inv;
+            const float A2 = fmaf(vv, V.m2[2], fmaf(uu, V.m2[1], V.m2[0])) * inv;
+            const float B1 = fmaf(vv, V.n1[2], fmaf(uu, V.n1[1], V.n1[0])) * inv;
+            const float B2 = fmaf(vv, V.n2[2], fmaf(uu, V.n2[1], V.n2[0])) * inv;
+            float smin = 0.0f, smax = n0 - 1.0f;
+            clip_slices_m(A1, B1, -1.6f, (float)L.n1 - 0.4f, smin, smax);
+            clip_slices_m(A2, B2, -1.6f, (float)L.n2 - 0.4f, smin, smax);
+            int s_lo = max(0, (int)ceilf(fmaxf(smin, -1.0f)));
+            int s_hi = min(L.n0 - 1, (int)floorf(fminf(smax, n0)));
+            const float B1h = B1 + 0.5f, B2h = B2 + 0.5f;
+            for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
+                if (texel_ok_m(A1, B1h, s_lo, L.n1) && texel_ok_m(A2, B2h, s_lo, L.n2)) break;
+                ++s_lo;
+            }
+            for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
+                if (texel_ok_m(A1, B1h, s_hi, L.n1) && texel_ok_m(A2, B2h, s_hi, L.n2)) break;
+                --s_hi;
+            }
+            if (!(texel_ok_m(A1, B1h, s_lo, L.n1) && texel_ok_m(A2, B2h, s_lo, L.n2) &&
+                  texel_ok_m(A1, B1h, s_hi, L.n1) && texel_ok_m(A2, B2h, s_hi, L.n2)))
+                s_hi = s_lo - 1;
+            const float sc = sqrtf(fmaf(A1 * A1, L.f1, fmaf(A2 * A2, L.f2, 1.0f))) * L.mul;
+            const float w = val * sc;
+            for (int s = s_lo; s <= s_hi; ++s) {
+                int k1, k2;
+                float f1, f2;
+                split_floor_m(fmaf(A1, (float)s, B1h), k1, f1);
+                split_floor_m(fmaf(A2, (float)s, B2h), k2, f2);
+                const float g1 = 1.0f - f1, g2 = 1.0f - f2;
+                red_add_v4(cacc + ((long long)(k1 + 2) * L.n0 + s) * m2 + (k2 + 2), g1 * g2 * w, f1 * g2 * w,
+                           g1 * f2 * w, f1 * f2 * w);
+            }
+        }
+    }
+}
+
+// out[z][y][x] (=|+=) the x-major cell taps C0 (k1 = y, s = x, k2 = z), the
+// y-major cell taps C1 (k1 = x, s = y, k2 = z) and the z-major padded
+// accumulator accA[z+2][y+2][x+2]; a voxel's taps are .x of its own cell,
+// .y of the cell before it along k1, .z before it along k2, .w before both.
+// Threads run along z, the cells' contiguous axis.
+template <typename T>
+__global__ void fold_cells(const float4 *__restrict__ c0, const float4 *__restrict__ c1,
+                           const float *__restrict__ accA, int nx, int ny, int nz, T *__restrict__ out,
+                           size_t pitch, int accumulate)
+{
+    const int z = blockIdx.x * blockDim.x + threadIdx.x;
+    const int x = blockIdx.y;
+    const int y = blockIdx.z;
+    if (z >= nz) return;
+    const long long m2 = nz + 4;
+    float r = 0.0f;
+    auto taps = [&](const float4 *c, long long j1, long long n0, long long sl) {
+        const float4 *p = c + (j1 * n0 + sl) * m2 + (z + 2);  // cell (k1, s, k2 = z)
+        const float4 *q = p - n0 * m2;                        // k1 - 1
+        r += p->x + q->y + (p - 1)->z + (q - 1)->w;
+    };
+    if (c0) taps(c0, y + 2, nx, x);
+    if (c1) taps(c1, x + 2, ny, y);
+    if (accA) r += accA[((size_t)(z + 2) * (ny + 4) + (y + 2)) * (nx + 4) + (x + 2)];
+    T *o = out + ((size_t)z * ny + y) * pitch + x;
+    if (accumulate) r += ldm_plain(o);
+    *o = tom<T>(r);
+}
+
 // out[z][y][x] (=|+=) accA[z+2][y+2][x+2] + accB[z+2][x+2][y+2]
 template <typename T>
 __global__ void fold_accumulators(const float *__restrict__ accA, const float *__restrict__ accB, int nx,
@@ -203,6 +308,105 @@ b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const v
     }
     const size_t px = d.vol_x + 4, py = d.vol_y + 4, pz = d.vol_z + 4;
     const size_t padded = px * py * pz;
+    {
+        // cell-space accumulators for x- and y-major views (one vector
+        // reduction per sample); the scalar path below when they do not fit
+        Scratch cacc[2], sz;
+        bool ok = true;
+        for (int dir = 0; dir < 2 && ok; ++dir) {
+            if (!need[dir]) continue;
+            const size_t count = (dir == 0 ? py : px) * (size_t)(dir == 0 ? d.vol_x : d.vol_y) * pz;
+            const b2t_status st = cacc[dir].alloc(count * sizeof(float4), s, "matched bp cell accumulator");
+            if (st == B2T_ERR_NO_MEMORY) {
+                clear_error();
+                ok = false;
+                break;
+            }
+            B2T_TRY(st);
+            B2T_CUDA_TRY(cudaMemsetAsync(cacc[dir].as<void>(), 0, count * sizeof(float4), s), "matched bp memset");
+        }
+        if (ok && need[2]) {
+            const b2t_status st = sz.alloc(padded * sizeof(float), s, "matched bp accumulator (xyz)");
+            if (st == B2T_ERR_NO_MEMORY) {
+                clear_error();
+                ok = false;
+            } else {
+                B2T_TRY(st);
+                B2T_CUDA_TRY(cudaMemsetAsync(sz.as<void>(), 0, padded * sizeof(float), s), "matched bp memset");
+            }
+        }
+        if (ok) {
+            FPLaunch *Lp = new FPLaunch;
+            FPLaunch &P = *Lp;
+            const bool force_noncube = p->det_supersample > 1;
+            b2t_status st = B2T_OK;
+            for (int dir = 0; dir < 3 && st == B2T_OK; ++dir) {
+                if (!need[dir]) continue;
+                P.proj = const_cast<void *>(proj);
+                P.proj_pitch = (long long)proj_pitch;
+                P.nu = d.det_u;
+                P.nv = d.det_v;
+                P.na = d.angles;
+                P.rays = p->det_supersample;
+                P.accumulate = 0;
+                fp_scale(g->kind, dir, g->vol_scale, force_noncube, p->output_scale, P.f1, P.f2, P.mul);
+                if (dir == 0) { P.n0 = d.vol_x; P.n1 = d.vol_y; P.n2 = d.vol_z; }
+                else if (dir == 1) { P.n0 = d.vol_y; P.n1 = d.vol_x; P.n2 = d.vol_z; }
+                else {
+                    P.n0 = d.vol_z; P.n1 = d.vol_x; P.n2 = d.vol_y;
+                    P.st0 = (long long)(px * py);
+                    P.st2 = (long long)px;
+                }
+                P.vol = (dir == 2) ? static_cast<void *>(sz.as<float>() + 2 * P.st0 + 2 * P.st2 + 2)
+                                   : cacc[dir].as<void>();
+                std::vector<int> views;
+                for (uint32_t a = 0; a < d.angles; ++a)
+                    if (dirs[a] == dir) views.push_back((int)a);
+                for (size_t c0 = 0; c0 < views.size() && st == B2T_OK; c0 += FP_MAX_VIEWS) {
+                    const size_t cn = std::min(views.size() - c0, (size_t)FP_MAX_VIEWS);
+                    P.nviews = (int)cn;
+                    for (size_t i = 0; i < cn; ++i) {
+                        const int a = views[c0 + i];
+                        fp_view_coeffs(g->kind, g->views[a], d, dir, P.views[i]);
+                        P.views[i].a = a;
+                    }
+                    if (dir == 2) {
+                        dim3 grid((unsigned)cn, (d.det_u + 31) / 32, (d.det_v + 7) / 8);
+                        if (dtype == B2T_F32) st = launch_T<float>(P, grid, s);
+                        else if (dtype == B2T_F16) st = launch_T<__half>(P, grid, s);
+                        else st = launch_T<__nv_bfloat16>(P, grid, s);
+                    } else {
+                        dim3 grid((unsigned)cn, (d.det_u + 7) / 8, (d.det_v + 31) / 32);
+                        if (dtype == B2T_F32) fp3d_transpose_cols_kernel<float><<<grid, dim3(32, 8), 0, s>>>(P);
+                        else if (dtype == B2T_F16) fp3d_transpose_cols_kernel<__half><<<grid, dim3(32, 8), 0, s>>>(P);
+                        else fp3d_transpose_cols_kernel<__nv_bfloat16><<<grid, dim3(32, 8), 0, s>>>(P);
+                        count_launches(1);
+                        if (cudaGetLastError() != cudaSuccess) st = fail(B2T_ERR_CUDA, "matched bp (cells) launch");
+                    }
+                }
+            }
+            delete Lp;
+            B2T_TRY(st);
+            const int accumulate = (mode == B2T_MODE_ADD) ? 1 : 0;
+            dim3 grid((d.vol_z + 127) / 128, d.vol_x, d.vol_y);
+            const float4 *c0 = need[0] ? cacc[0].as<float4>() : nullptr;
+            const float4 *c1 = need[1] ? cacc[1].as<float4>() : nullptr;
+            const float *az = need[2] ? sz.as<float>() : nullptr;
+            if (dtype == B2T_F32)
+                fold_cells<float><<<grid, 128, 0, s>>>(c0, c1, az, d.vol_x, d.vol_y, d.vol_z,
+                                                       static_cast<float *>(vol), vol_pitch, accumulate);
+            else if (dtype == B2T_F16)
+                fold_cells<__half><<<grid, 128, 0, s>>>(c0, c1, az, d.vol_x, d.vol_y, d.vol_z,
+                                                        static_cast<__half *>(vol), vol_pitch, accumulate);
+            else
+                fold_cells<__nv_bfloat16><<<grid, 128, 0, s>>>(c0, c1, az, d.vol_x, d.vol_y, d.vol_z,
+                                                               static_cast<__nv_bfloat16 *>(vol), vol_pitch,
+                                                               accumulate);
+            count_launches(1);
+            B2T_CUDA_TRY(cudaGetLastError(), "matched bp fold launch");
+            return B2T_OK;
+        }
+    }
     Scratch sa, sb;
     if (need[1] || need[2]) {
         B2T_TRY(sa.alloc(padded * sizeof(float), s, "matched bp accumulator (xyz)"));
