@@ -157,6 +157,31 @@ b2t_status copy_slab(float *dst, const float *src, const b2t_dims3d &d, uint32_t
 
 // One GPU's share of the jobs (job j = angle block j for FP, slab j for
 // BP / FDK).
+// The angle blocks of a streamed call, (first view, count): blocks of at
+// most `step` views, balanced, and, when the views are split at all, one
+// block of at most 16 views at the end of the pipeline whose transfer no
+// compute hides: last for the FP (its final download), first for the BP and
+// FDK (their first upload).
+std::vector<std::pair<uint32_t, uint32_t>> angle_blocks(uint32_t n, uint32_t step, bool small_last)
+{
+    std::vector<std::pair<uint32_t, uint32_t>> r;
+    const uint32_t edge = n > step ? std::min<uint32_t>(16, step) : 0;
+    const uint32_t rest = n - edge;
+    const uint32_t nb = (rest + step - 1) / step;
+    uint32_t a = 0;
+    if (!small_last && edge) {
+        r.push_back({0, edge});
+        a = edge;
+    }
+    for (uint32_t b = 0; b < nb; ++b) {
+        const uint32_t len = rest / nb + (b < rest % nb ? 1u : 0u);
+        r.push_back({a, len});
+        a += len;
+    }
+    if (small_last && edge) r.push_back({a, edge});
+    return r;
+}
+
 b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &jobs)
 {
     B2T_CUDA_TRY(cudaSetDevice(device), "stream worker device");
@@ -167,7 +192,8 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
     const uint32_t in_n = fp ? d.vol_z : d.angles, in_step = fp ? R.slab : R.block;
     const uint32_t out_step = fp ? R.block : R.slab;
     const uint32_t out_n = fp ? d.angles : d.vol_z;
-    const uint32_t nin = (in_n + in_step - 1) / in_step;
+    const std::vector<std::pair<uint32_t, uint32_t>> ablocks = angle_blocks(d.angles, R.block, fp);
+    const uint32_t nin = fp ? (in_n + in_step - 1) / in_step : (uint32_t)ablocks.size();
     const size_t in_elems = fp ? (size_t)d.vol_x * d.vol_y * in_step : (size_t)d.det_u * d.det_v * in_step;
     const size_t out_elems = fp ? (size_t)d.det_u * d.det_v * out_step : (size_t)d.vol_x * d.vol_y * out_step;
     const bool resident = nin == 1;  // the whole input fits: copy it once
@@ -198,8 +224,19 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
         B2T_CUDA_TRY(cudaEventRecord(in_free[k].e, cs.s), "event record");
         B2T_CUDA_TRY(cudaEventRecord(out_copied[k].e, os.s), "event record");
     }
+    // input chunk c: a z-slab of the FP, an angle block of the BP / FDK
+    auto in_chunk = [&](uint32_t c, uint32_t &c0, uint32_t &cn) {
+        if (fp) {
+            c0 = c * in_step;
+            cn = std::min(in_step, in_n - c0);
+        } else {
+            c0 = ablocks[c].first;
+            cn = ablocks[c].second;
+        }
+    };
     auto upload = [&](uint32_t c, int buf) -> b2t_status {
-        const uint32_t c0 = c * in_step, cn = std::min(in_step, in_n - c0);
+        uint32_t c0, cn;
+        in_chunk(c, c0, cn);
         B2T_CUDA_TRY(cudaStreamWaitEvent(hs.s, in_free[buf].e, 0), "wait");
         if (fp) B2T_TRY(copy_slab(inb[buf].f(), R.in, d, c0, cn, true, hs.s));
         else B2T_TRY(copy_block(inb[buf].f(), R.in, d, c0, cn, true, hs.s));
@@ -224,7 +261,11 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
     SubGeom sub;
     for (size_t jn = 0; jn < jobs.size(); ++jn) {
         const uint32_t j = jobs[jn];
-        const uint32_t o0 = j * out_step, on = std::min(out_step, out_n - o0);
+        uint32_t o0 = j * out_step, on = std::min(out_step, out_n - std::min(o0, out_n));
+        if (fp) {
+            o0 = ablocks[j].first;
+            on = ablocks[j].second;
+        }
         const int ob = (int)(jn & 1);
         float *obuf = outb[ob].f();
         // the output buffer's previous download must be complete
@@ -244,7 +285,8 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
             const int ib = resident ? 0 : (int)(c & 1);
             if (!resident && c + 1 < nin) B2T_TRY(upload(c + 1, (int)((c + 1) & 1)));
             B2T_CUDA_TRY(cudaStreamWaitEvent(cs.s, in_ready[ib].e, 0), "wait");
-            const uint32_t c0 = c * in_step, cn = std::min(in_step, in_n - c0);
+            uint32_t c0, cn;
+            in_chunk(c, c0, cn);
             const int32_t mode = first ? B2T_MODE_SET : B2T_MODE_ADD;
             first = false;
             if (fp) {
@@ -367,7 +409,8 @@ b2t_status stream3d_run(int32_t op, const b2t_geom3d *g, const b2t_params3d *par
     std::vector<int> devs;
     B2T_TRY(stream3d_plan_impl(op, g, cfg, who, devs, R.slab, R.block));
     const b2t_dims3d &d = g->dims;
-    const uint32_t njobs = op == 0 ? (d.angles + R.block - 1) / R.block : (d.vol_z + R.slab - 1) / R.slab;
+    const uint32_t njobs = op == 0 ? (uint32_t)angle_blocks(d.angles, R.block, true).size()
+                                   : (d.vol_z + R.slab - 1) / R.slab;
     const size_t nw = std::min<size_t>(devs.size(), njobs);
     std::vector<std::vector<uint32_t>> share(nw);
     for (uint32_t j = 0; j < njobs; ++j) share[j % nw].push_back(j);
