@@ -18,7 +18,13 @@
 //                      (no re-rounding of the stored data).
 // Cells cover padded texel indices -2..n+1 in both plane axes (the texture
 // border is zero), so every ray's clipped slice range stays inside the grid
-// exactly as in fp3d_kernel.
+// exactly as in fp3d_kernel.  Two cell layouts: the columns layout (cells
+// contiguous along z, build_cells_cols, fp3d_col_kernel) for x- and y-major
+// views, whose warps follow detector columns; the rows layout (contiguous
+// along the first plane axis, build_cells, fp3d_cell_kernel) for z-major
+// views.  fp3d_cells_build / fp3d_cells_project split the layout pass from
+// the projection, so that a streamed call lays a volume out once for all of
+// its angle blocks.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -354,7 +360,9 @@ __global__ void __launch_bounds__(32 * VROWS * VPC, 2048 / (32 * VROWS * VPC)) f
 // texel k1 and their k2 run along the contiguous axis: a warp's 16-byte
 // loads fall on three or four 128-byte lines instead of the seven to nine a
 // detector row needs when its rays cross several k2 rows.  Four loads in
-// flight per thread (40 registers, three CTAs per SM) cover the L2 latency.
+// flight per thread cover the L2 latency: 32 registers and four CTAs per SM
+// with 32-bit cell indices (IDX32, a cell array of fewer than 2^32 cells),
+// else 64-bit addresses at 40 registers and three CTAs.
 // The ray set-up is the rows tracer's, written out here: the shared form
 // spilled at 40 registers.
 template <typename T, int VPC, int VCOLS, bool IDX32>

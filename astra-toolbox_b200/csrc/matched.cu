@@ -58,7 +58,7 @@ __device__ __forceinline__ void clip_slices_m(float A, float B, float lo, float 
     smax = fminf(smax, fmaxf(s1, s2));
 }
 
-// The forward projectors' split (fp3d_cell_kernel, fp3d_kernel): sample
+// The forward projectors' split (fp3d_col_kernel, fp3d_cell_kernel, fp3d_kernel): sample
 // position plus one half qh = A s + (B + 1/2); texel floor(qh) by rounding
 // down, weight qh - floor(qh).  Identical arithmetic keeps the transpose exact.
 constexpr float SPLIT_M = 12582912.0f;  // 1.5 * 2^23

@@ -166,7 +166,7 @@ __device__ __forceinline__ void clip_slices(float A, float B, float lo, float hi
     smax = fminf(smax, fmaxf(s1, s2));
 }
 
-// The FP's split (shared with fp3d_cell_kernel and the matched BP): sample
+// The FP's split (shared with the cell kernels and the matched BP): sample
 // position plus one half qh = A s + (B + 1/2); texel floor(qh) by rounding
 // down, weight qh - floor(qh).
 constexpr float SPLIT_M = 12582912.0f;  // 1.5 * 2^23
