@@ -159,17 +159,20 @@ __device__ __forceinline__ void red_add_v4(float4 *p, float a, float b, float c,
 // around it.  A warp takes 32 rows of one detector column, so its
 // reductions fall on a few contiguous lines.  L.vol is the accumulator's
 // first cell (j1 = j2 = 0), index (j1 n0 + s) (n2 + 4) + j2, j = k + 2.
-template <typename T>
+template <typename T, bool AGG>
 __global__ void __launch_bounds__(256) fp3d_transpose_cols_kernel(const __grid_constant__ FPLaunch L)
 {
     const FPView &V = L.views[blockIdx.x];
     const int v = blockIdx.z * 32 + threadIdx.x;
     const int u = blockIdx.y * 8 + threadIdx.y;
-    if (u >= L.nu || v >= L.nv) return;
+    const int lane = threadIdx.x;
+    const bool inside = u < L.nu && v < L.nv;
+    if (!AGG && !inside) return;
     float4 *cacc = static_cast<float4 *>(const_cast<void *>(L.vol));
-    const T *pin = static_cast<const T *>(L.proj) + ((size_t)v * L.na + V.a) * L.proj_pitch + u;
-    float val = ldm(pin);
-    if (val == 0.0f) return;
+    float val = 0.0f;
+    if (inside) val = ldm(static_cast<const T *>(L.proj) + ((size_t)v * L.na + V.a) * L.proj_pitch + u);
+    if (!AGG && val == 0.0f) return;
+    const bool live = inside && val != 0.0f;
     const int R = L.rays;
     if (R > 1) val /= (float)(R * R);
     const float n0 = (float)L.n0;
@@ -207,14 +210,65 @@ __global__ void __launch_bounds__(256) fp3d_transpose_cols_kernel(const __grid_c
                 s_hi = s_lo - 1;
             const float sc = sqrtf(fmaf(A1 * A1, L.f1, fmaf(A2 * A2, L.f2, 1.0f))) * L.mul;
             const float w = val * sc;
-            for (int s = s_lo; s <= s_hi; ++s) {
-                int k1, k2;
-                float f1, f2;
-                split_floor_m(fmaf(A1, (float)s, B1h), k1, f1);
-                split_floor_m(fmaf(A2, (float)s, B2h), k2, f2);
-                const float g1 = 1.0f - f1, g2 = 1.0f - f2;
-                red_add_v4(cacc + ((long long)(k1 + 2) * L.n0 + s) * m2 + (k2 + 2), g1 * g2 * w, f1 * g2 * w,
-                           g1 * f2 * w, f1 * f2 * w);
+            if constexpr (!AGG) {
+                for (int s = s_lo; s <= s_hi; ++s) {
+                    int k1, k2;
+                    float f1, f2;
+                    split_floor_m(fmaf(A1, (float)s, B1h), k1, f1);
+                    split_floor_m(fmaf(A2, (float)s, B2h), k2, f2);
+                    const float g1 = 1.0f - f1, g2 = 1.0f - f2;
+                    red_add_v4(cacc + ((long long)(k1 + 2) * L.n0 + s) * m2 + (k2 + 2), g1 * g2 * w,
+                               f1 * g2 * w, g1 * f2 * w, f1 * f2 * w);
+                }
+            } else {
+                // The warp's rays (consecutive rows of one column) walk one
+                // common slice range; at each slice, neighbouring lanes whose
+                // samples share a cell (about 1.5 rays per cell) merge: the
+                // head of a run of equal cells adds the taps of the lane after
+                // it, which then skips its reduction; later lanes of longer
+                // runs reduce on their own.  Lanes without a sample carry
+                // distinct keys that match nothing.
+                if (!live) {
+                    s_lo = 1;
+                    s_hi = 0;
+                }
+                const int S0 = __reduce_min_sync(0xffffffffu, s_lo <= s_hi ? s_lo : 0x7fffffff);
+                const int S1 = __reduce_max_sync(0xffffffffu, s_lo <= s_hi ? s_hi : -1);
+                for (int s = S0; s <= S1; ++s) {
+                    const bool in = s >= s_lo && s <= s_hi;
+                    uint32_t key = 0xffffffffu - (uint32_t)lane;
+                    float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f, t3 = 0.0f;
+                    if (in) {
+                        int k1, k2;
+                        float f1, f2;
+                        split_floor_m(fmaf(A1, (float)s, B1h), k1, f1);
+                        split_floor_m(fmaf(A2, (float)s, B2h), k2, f2);
+                        const float g1 = 1.0f - f1, g2 = 1.0f - f2;
+                        key = ((uint32_t)(k1 + 2) * (uint32_t)L.n0 + (uint32_t)s) * (uint32_t)m2 + (uint32_t)(k2 + 2);
+                        t0 = g1 * g2 * w;
+                        t1 = f1 * g2 * w;
+                        t2 = g1 * f2 * w;
+                        t3 = f1 * f2 * w;
+                    }
+                    const uint32_t kp = __shfl_up_sync(0xffffffffu, key, 1);
+                    const uint32_t kp2 = __shfl_up_sync(0xffffffffu, key, 2);
+                    const uint32_t kn = __shfl_down_sync(0xffffffffu, key, 1);
+                    const float n0v = __shfl_down_sync(0xffffffffu, t0, 1);
+                    const float n1v = __shfl_down_sync(0xffffffffu, t1, 1);
+                    const float n2v = __shfl_down_sync(0xffffffffu, t2, 1);
+                    const float n3v = __shfl_down_sync(0xffffffffu, t3, 1);
+                    const bool head = lane == 0 || kp != key;
+                    const bool second = !head && (lane == 1 || kp2 != key);
+                    if (in && !second) {
+                        if (head && lane < 31 && kn == key) {
+                            t0 += n0v;
+                            t1 += n1v;
+                            t2 += n2v;
+                            t3 += n3v;
+                        }
+                        red_add_v4(cacc + key, t0, t1, t2, t3);
+                    }
+                }
             }
         }
     }
@@ -377,9 +431,21 @@ b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const v
                         else st = launch_T<__nv_bfloat16>(P, grid, s);
                     } else {
                         dim3 grid((unsigned)cn, (d.det_u + 7) / 8, (d.det_v + 31) / 32);
-                        if (dtype == B2T_F32) fp3d_transpose_cols_kernel<float><<<grid, dim3(32, 8), 0, s>>>(P);
-                        else if (dtype == B2T_F16) fp3d_transpose_cols_kernel<__half><<<grid, dim3(32, 8), 0, s>>>(P);
-                        else fp3d_transpose_cols_kernel<__nv_bfloat16><<<grid, dim3(32, 8), 0, s>>>(P);
+                        // merged reductions key cells by 32-bit index (with
+                        // the lanes' sentinels above the cell count)
+                        const unsigned long long cells =
+                            (unsigned long long)(P.n1 + 4) * P.n0 * (unsigned long long)(P.n2 + 4);
+                        const bool agg = cells < (1ull << 32) - 64;
+                        if (dtype == B2T_F32) {
+                            if (agg) fp3d_transpose_cols_kernel<float, true><<<grid, dim3(32, 8), 0, s>>>(P);
+                            else fp3d_transpose_cols_kernel<float, false><<<grid, dim3(32, 8), 0, s>>>(P);
+                        } else if (dtype == B2T_F16) {
+                            if (agg) fp3d_transpose_cols_kernel<__half, true><<<grid, dim3(32, 8), 0, s>>>(P);
+                            else fp3d_transpose_cols_kernel<__half, false><<<grid, dim3(32, 8), 0, s>>>(P);
+                        } else {
+                            if (agg) fp3d_transpose_cols_kernel<__nv_bfloat16, true><<<grid, dim3(32, 8), 0, s>>>(P);
+                            else fp3d_transpose_cols_kernel<__nv_bfloat16, false><<<grid, dim3(32, 8), 0, s>>>(P);
+                        }
                         count_launches(1);
                         if (cudaGetLastError() != cudaSuccess) st = fail(B2T_ERR_CUDA, "matched bp (cells) launch");
                     }
