@@ -286,17 +286,22 @@ struct DevBuf {
     void *p = nullptr;
     ~DevBuf()
     {
-        if (p) cudaFree(p);
+        if (p) {
+            cudaFree(p);
+            alloc_live(-1);
+        }
     }
     b2t_status alloc(size_t bytes, const char *what)
     {
         if (bytes == 0) bytes = 16;
+        if (alloc_injected_failure()) return fail(B2T_ERR_NO_MEMORY, "%s: injected allocation failure", what);
         cudaError_t e = cudaMalloc(&p, bytes);
         if (e != cudaSuccess) {
             p = nullptr;
             (void)cudaGetLastError();
             return cuda_fail(e, what);
         }
+        alloc_live(1);
         // zero: element-wise passes also run over the gaps between the
         // problems of a packed batch, which no projector writes
         e = cudaMemset(p, 0, bytes);

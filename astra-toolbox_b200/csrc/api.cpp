@@ -65,6 +65,22 @@ static std::atomic<unsigned long long> g_launches{0};
 
 void count_launches(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 
+// Allocations still to go before the armed one fails (0: none armed), and the
+// number of device allocations the library holds.
+static std::atomic<long long> g_alloc_countdown{0};
+static std::atomic<long long> g_live_allocs{0};
+
+bool alloc_injected_failure()
+{
+    long long c = g_alloc_countdown.load();
+    while (c > 0) {
+        if (g_alloc_countdown.compare_exchange_weak(c, c - 1)) return c == 1;
+    }
+    return false;
+}
+
+void alloc_live(long long delta) { g_live_allocs.fetch_add(delta); }
+
 b2t_status fail(b2t_status st, const char *fmt, ...)
 {
     char buf[1024];
@@ -109,6 +125,26 @@ b2t_status b2t_device_errors(uint32_t *flags)
     if (!flags) return fail(B2T_ERR_INVALID_ARG, "b2t_device_errors: null pointer");
     B2T_CUDA_TRY(cudaDeviceSynchronize(), "b2t_device_errors synchronize");
     return device_errors_impl(flags);
+}
+
+b2t_status b2t_debug_fail_alloc(int64_t nth, int64_t *pending)
+{
+    clear_error();
+    if (nth < 0) return fail(B2T_ERR_INVALID_ARG, "b2t_debug_fail_alloc: negative count %lld", (long long)nth);
+    const long long before = g_alloc_countdown.exchange(nth);
+    if (pending) *pending = before;
+    return B2T_OK;
+}
+
+int64_t b2t_debug_live_allocations(void) { return g_live_allocs.load(); }
+
+b2t_status b2t_selftest_bounded_wait(int32_t which, uint64_t limit_cycles, void *stream)
+{
+    clear_error();
+    if (which != 0 && which != 1) return fail(B2T_ERR_INVALID_ARG, "b2t_selftest_bounded_wait: which must be 0 or 1");
+    if (limit_cycles == 0 || limit_cycles > 4000000000ull)
+        return fail(B2T_ERR_INVALID_ARG, "b2t_selftest_bounded_wait: limit must be 1..4e9 cycles");
+    return selftest_wait_impl(which, (long long)limit_cycles, static_cast<cudaStream_t>(stream));
 }
 
 b2t_status b2t_bp_path_stats(uint64_t *stats)

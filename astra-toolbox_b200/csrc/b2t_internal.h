@@ -50,6 +50,14 @@ inline bool dtype_valid(int32_t dtype)
 cudaMemPool_t scratch_pool(cudaError_t &err);
 void trim_scratch_pools();
 
+// Device-allocation bookkeeping of the library (every allocation site calls
+// these): alloc_injected_failure() is true for the allocation that
+// b2t_debug_fail_alloc armed (its caller then fails with B2T_ERR_NO_MEMORY
+// without allocating); alloc_live() tracks the allocations the library holds,
+// read by b2t_debug_live_allocations.
+bool alloc_injected_failure();
+void alloc_live(long long delta);
+
 // Stream-ordered scratch allocation that is freed (stream-ordered) when the
 // object goes out of scope.
 class Scratch {
@@ -63,6 +71,7 @@ public:
         release();
         stream_ = s;
         if (bytes == 0) bytes = 16;
+        if (alloc_injected_failure()) return fail(B2T_ERR_NO_MEMORY, "%s: injected allocation failure", what);
         cudaError_t e = cudaSuccess;
         cudaMemPool_t pool = scratch_pool(e);
         if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&ptr_, bytes, pool, s);
@@ -71,12 +80,16 @@ public:
             (void)cudaGetLastError();  // allocation failures are not sticky: clear them
             return cuda_fail(e, what);
         }
+        alloc_live(1);
         bytes_ = bytes;
         return B2T_OK;
     }
     void release()
     {
-        if (ptr_) cudaFreeAsync(ptr_, stream_);
+        if (ptr_) {
+            cudaFreeAsync(ptr_, stream_);
+            alloc_live(-1);
+        }
         ptr_ = nullptr;
         bytes_ = 0;
     }

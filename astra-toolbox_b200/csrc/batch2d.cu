@@ -121,7 +121,10 @@ static b2t_status persistent_grid(K kern, int threads, int nitems, int &grid)
 
 Batch2D::~Batch2D()
 {
-    if (mem) cudaFree(mem);
+    if (mem) {
+        cudaFree(mem);
+        alloc_live(-1);
+    }
 }
 
 b2t_status batch2d_create_impl(const b2t_problem2d *problems, int32_t n, Batch2D **out)
@@ -243,12 +246,17 @@ b2t_status batch2d_create_impl(const b2t_problem2d *problems, int32_t n, Batch2D
     const size_t o_vfi = align(o_sch + sizeof(SegChunk) * sch.size());
     const size_t o_sfi = align(o_vfi + sizeof(int) * (n + 1));
     const size_t total = o_sfi + sizeof(int) * (n + 1);
+    if (alloc_injected_failure()) {
+        delete b;
+        return fail(B2T_ERR_NO_MEMORY, "b2t_batch2d_create: device tables: injected allocation failure");
+    }
     cudaError_t e = cudaMalloc(&b->mem, total);
     if (e != cudaSuccess) {
         b->mem = nullptr;
         delete b;
         return cuda_fail(e, "b2t_batch2d_create: device tables");
     }
+    alloc_live(1);
     char *base = static_cast<char *>(b->mem);
     b->d_probs = reinterpret_cast<BatchProb *>(base + o_probs);
     b->d_par = reinterpret_cast<ParFPView *>(base + o_par);

@@ -280,6 +280,11 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t 
                 if (!__all_sync(0xffffffffu, mbar_wait_bounded_sleep(&empty[j0 % BPT_SLOTS],
                                                                (uint32_t)((j0 / BPT_SLOTS) & 1), 2000000000LL))) {
                     if (lane == 0) atomicOr(&g_b2t_device_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
+                    // the copies already issued (views j0 .. vk - 1, one per
+                    // slot) land before the warp leaves
+                    for (int q = j0; q < vk; ++q)
+                        (void)mbar_wait_bounded_sleep(&full[q % BPT_SLOTS], (uint32_t)((q / BPT_SLOTS) & 1),
+                                                      2000000000LL);
                     return;
                 }
                 ++j0;
@@ -304,6 +309,11 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t 
             }
         }
     }
+    // the last views' copies land before the warp leaves: the CTA cannot end
+    // with bulk copies in flight, even when the compute warps give up on a
+    // wait (views j0 .. nviews - 1 hold one slot each)
+    for (int q = j0; q < L.nviews; ++q)
+        (void)mbar_wait_bounded_sleep(&full[q % BPT_SLOTS], (uint32_t)((q / BPT_SLOTS) & 1), 2000000000LL);
 }
 
 // 288 threads: warps 0-7 backproject a 32 x 8 x BPT_Z voxel block, warp 8
@@ -682,6 +692,57 @@ b2t_status bp_path_stats_impl(uint64_t *stats)
     const unsigned long long zero[4] = {0, 0, 0, 0};
     B2T_CUDA_TRY(cudaMemcpyToSymbol(g_bp_path_stats, zero, sizeof(zero)), "clear BP path statistics");
     for (int k = 0; k < 4; ++k) stats[k] = v[k];
+    return B2T_OK;
+}
+
+namespace {
+
+// Set by nothing: the flag the self-test waits for.
+static __device__ unsigned int g_selftest_flag = 0;
+
+// The bounded waits of the pipelined kernels, run where nothing can end them:
+// one warp waits for phase 0 of an mbarrier that expects one arrival and
+// never gets it (which 0), or polls a device flag that nothing sets
+// (which 1).  Either wait gives up after `limit` cycles, records
+// B2T_DEVERR_WAIT_TIMEOUT in the error word and returns, as bp3d_tma_kernel
+// and ramp_tc_kernel do on a timeout.  No copy is in flight.
+__global__ void __launch_bounds__(32) wait_selftest_kernel(int which, long long limit)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    bool ok;
+    if (which == 0) {
+        ok = mbar_wait_bounded(&bar, 0u, limit);
+    } else {
+        const long long t0 = clock64();
+        ok = true;
+        while (*reinterpret_cast<volatile unsigned int *>(&g_selftest_flag) == 0u) {
+            if (clock64() - t0 > limit) {
+                ok = false;
+                break;
+            }
+            __nanosleep(1000);
+        }
+    }
+    if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) atomicOr(&g_b2t_device_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
+}
+
+}  // namespace
+
+b2t_status selftest_wait_impl(int which, long long limit, cudaStream_t s)
+{
+    wait_selftest_kernel<<<1, 32, 0, s>>>(which, limit);
+    count_launches(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "wait self-test launch");
+    B2T_CUDA_TRY(cudaStreamSynchronize(s), "wait self-test synchronize");
+    uint32_t flags = 0;
+    B2T_TRY(device_errors_impl(&flags));
+    if (flags & B2T_DEVERR_WAIT_TIMEOUT)
+        return fail(B2T_ERR_TIMEOUT, "b2t_selftest_bounded_wait: the wait gave up after %lld cycles", limit);
     return B2T_OK;
 }
 

@@ -10,16 +10,18 @@
 // library instead.  The caller still provides the inputs and the result.
 //
 // The array (NOALLOC_PARTS doubles, 32 KB) exists on every GPU that loads the
-// library and stays there until the process exits.  Each block of the
-// reduction handles at most NOALLOC_CHUNK elements, so n is limited to
-// NOALLOC_PARTS * NOALLOC_CHUNK elements; larger n is rejected before any
-// device work.  Every call writes the partial sums it reads (nothing is
-// carried over from an earlier call), and all calls on one device share the
-// array: calls that overlap on the GPU race and must be serialised by the
-// caller.
+// library and stays there until the process exits.  The reduction runs with
+// the launch shape of b2t_dot_f64 (dot_num_blocks(n) blocks), so for every n
+// up to DOT_MAX_BLOCKS * NOALLOC_CHUNK elements both entry points sum in the
+// same order and return the same bits; above that, blocks of at most
+// NOALLOC_CHUNK elements, so n is limited to NOALLOC_PARTS * NOALLOC_CHUNK
+// elements and larger n is rejected before any device work.  Every call
+// writes the partial sums it reads (nothing is carried over from an earlier
+// call), and all calls on one device share the array: calls that overlap on
+// the GPU race and must be serialised by the caller.
 #include <cuda_runtime.h>
 
-#include <mutex>
+#include <algorithm>
 
 #include "arith.h"
 #include "b2t_internal.h"
@@ -30,29 +32,19 @@ namespace {
 
 constexpr size_t NOALLOC_PARTS = 4096;
 constexpr size_t NOALLOC_CHUNK = size_t(1) << 20;
-constexpr int NOALLOC_MAX_DEVICES = 64;
+static_assert(DOT_MAX_BLOCKS <= (int)NOALLOC_PARTS, "the fixed array must hold b2t_dot_f64's largest launch");
 
 static __device__ __align__(256) double g_noalloc_partials[NOALLOC_PARTS];
 
-std::mutex g_noalloc_mutex;
-double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
-
 // Device address of the array on the current device.  In host code the
-// symbol is only a host-side stand-in, so the address is looked up once per
-// device (with that device current) and cached.
+// symbol is only a host-side stand-in, so the address is looked up with the
+// device current, on every call: a cached address would not survive a
+// cudaDeviceReset or a new context on that device.
 b2t_status noalloc_partials(double **out)
 {
-    int dev = 0;
-    B2T_CUDA_TRY(cudaGetDevice(&dev), "b2t_dot_f64_noalloc: current device");
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
-        return fail(B2T_ERR_UNSUPPORTED, "b2t_dot_f64_noalloc: device index %d above %d", dev, NOALLOC_MAX_DEVICES);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
-        B2T_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_partials), "b2t_dot_f64_noalloc: scratch address");
-        g_noalloc_ptr[dev] = static_cast<double *>(p);
-    }
-    *out = g_noalloc_ptr[dev];
+    void *p = nullptr;
+    B2T_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_partials), "b2t_dot_f64_noalloc: scratch address");
+    *out = static_cast<double *>(p);
     return B2T_OK;
 }
 
@@ -69,8 +61,7 @@ b2t_status dot_noalloc_impl(const void *a, const void *b, size_t n, int32_t dtyp
                     n, NOALLOC_PARTS * NOALLOC_CHUNK, NOALLOC_PARTS, NOALLOC_CHUNK);
     double *partials = nullptr;
     B2T_TRY(noalloc_partials(&partials));
-    size_t nblocks = (n + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK;
-    if (nblocks < 1) nblocks = 1;
+    const size_t nblocks = std::max((size_t)dot_num_blocks(n), (n + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK);
     return dot_launch(a, b, n, dtype, partials, (int)nblocks, result, s);
 }
 

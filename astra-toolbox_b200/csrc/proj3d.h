@@ -96,6 +96,10 @@ b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *p
                     int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status device_errors_impl(uint32_t *flags);
 b2t_status bp_path_stats_impl(uint64_t *stats);
+// One warp waits, bounded by limit cycles, for an mbarrier phase (which 0) or
+// a device flag (which 1) that nothing completes; B2T_ERR_TIMEOUT when the
+// wait gave up and set the device error word.
+b2t_status selftest_wait_impl(int which, long long limit, cudaStream_t s);
 
 int dominant_axis(int kind, const b2t_view3d &w, const b2t_dims3d &d);
 void fp_view_coeffs(int kind, const b2t_view3d &w, const b2t_dims3d &d, int dir, FPView &o);

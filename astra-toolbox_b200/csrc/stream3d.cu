@@ -63,10 +63,14 @@ struct DevBuf {
     cudaStream_t s = nullptr;
     ~DevBuf()
     {
-        if (p) cudaFreeAsync(p, s);
+        if (p) {
+            cudaFreeAsync(p, s);
+            alloc_live(-1);
+        }
     }
     b2t_status alloc(size_t bytes, cudaStream_t st, const char *what)
     {
+        if (alloc_injected_failure()) return fail(B2T_ERR_NO_MEMORY, "%s: injected allocation failure", what);
         cudaError_t e = cudaSuccess;
         cudaMemPool_t pool = scratch_pool(e);
         if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, pool, st);
@@ -75,6 +79,7 @@ struct DevBuf {
             (void)cudaGetLastError();
             return cuda_fail(e, what);
         }
+        alloc_live(1);
         s = st;
         return B2T_OK;
     }

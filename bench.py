@@ -12,8 +12,15 @@ the total updates of all ranks divided by the slowest rank's time.
 
 --impl reference times the reference's CPU path for this workload on the host
 cores: the reference has no CPU 3D projector, so this is the FP64 port of its
-model (oracle/), multi-threaded over all host threads, on a bounded sample of
-views per step.
+model (oracle/), multi-threaded over all host threads, on a bounded sample per
+step (FP of a few views, BP of a few z-slices over all views); it imports
+nothing of the library.
+
+The default arm also reports, after its timed region: `parity` (this run's
+FP output on sampled views and BP output on sampled z-slices against the FP64
+oracle on the same inputs, which is also the CPU baseline's sample) and
+`ref_cuda` (the reference's own CUDA build, oracle/_ref, timed on the same
+inputs and GPU, with the agreement of the outputs).
 """
 import argparse
 import ctypes
@@ -105,43 +112,102 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(vol_cpu, pr, n_views, nthreads):
-    """FP64 oracle FP of n_views views; returns (GUPS, seconds, threads)."""
+def astra_dicts(n, na, nd):
+    """The workload's volume and projection geometry as the reference's
+    geometry dictionaries (python/astra/creators.py), built without the
+    library."""
+    ang = np.linspace(0, 2 * np.pi, na, endpoint=False).astype(np.float32)
+    vg = {'GridRowCount': n, 'GridColCount': n, 'GridSliceCount': n,
+          'option': {'WindowMinX': -n / 2., 'WindowMaxX': n / 2., 'WindowMinY': -n / 2., 'WindowMaxY': n / 2.,
+                     'WindowMinZ': -n / 2., 'WindowMaxZ': n / 2.}}
+    pg = {'type': 'cone', 'DetectorSpacingX': 1.0, 'DetectorSpacingY': 1.0, 'DetectorRowCount': nd,
+          'DetectorColCount': nd, 'ProjectionAngles': ang, 'DistanceOriginSource': SOD,
+          'DistanceOriginDetector': ODD}
+    return ang, vg, pg
+
+
+def reference_geometry(n, na, nd):
+    """Per-view vectors of the workload from the reference's own
+    convertAstraGeometry (oracle/_ref, the reference built from its sources),
+    else from the oracle's numpy restatement; (views, voxel size, source)."""
     from oracle import oracle as orc
-    nv, na, nu = pr.proj_shape
-    views = pr.geom.views_array()
-    sel = np.linspace(0, na - 1, n_views).round().astype(int)
-    sub = views[sel]
+    from oracle import ref
+    ang, vg, pg = astra_dicts(n, na, nd)
+    if ref.available():
+        views, vs = ref.geom3d(vg, pg)
+        return views, vs, "reference convertAstraGeometry (oracle/_ref)"
+    return orc.cone_views(ang, nd, nd, SOD, ODD), np.ones(3, np.float32), "oracle cone_views (numpy)"
+
+
+def phantom_module():
+    """The seeded ellipsoid generator (pure numpy / torch), loaded from its
+    file so that the reference arm imports nothing of the library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_b2t_phantom", os.path.join(ROOT, "astra-toolbox_b200",
+                                                                               "phantom.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def sample_views(na, k):
+    return [int(v) for v in np.linspace(0, na - 1, k).round().astype(int)]
+
+
+def sample_slices(nz, k):
+    return [int(z) for z in np.linspace(0, nz - 1, k).round().astype(int)]
+
+
+def oracle_sample(vol_np, proj_np, views, vs, nu, nv, fp_sel, bp_slices, nthreads):
+    """The FP64 oracle (the CPU restatement of the reference's ray / voxel
+    model) on a bounded sample of the workload: the forward projection of the
+    views fp_sel (all rays of each) and the backprojection of the z-slices
+    bp_slices over all views.  Returns the outputs, the seconds of each and
+    the voxel-view updates they stand for (n^3 per FP view, n^2 x views per
+    BP slice, the GUPS unit of the GPU arm)."""
+    from oracle import oracle as orc
+    nz, ny, nx = vol_np.shape
+    na = views.shape[0]
     t0 = time.perf_counter()
-    orc.fp3d(2, sub, vol_cpu, nu, nv, pr.geom.vol_scale, nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    n = vol_cpu.size
-    return n * n_views / dt / 1e9, dt
+    fp = orc.fp3d(orc.CONE, views[fp_sel], vol_np, nu, nv, vs, nthreads=nthreads)
+    t1 = time.perf_counter()
+    bp = orc.bp3d_slices(orc.CONE, views, proj_np, (nz, ny, nx), bp_slices, vs, nthreads=nthreads)
+    t2 = time.perf_counter()
+    units = float(nx * ny * nz) * len(fp_sel) + float(nx * ny) * len(bp_slices) * na
+    return {"fp": fp, "bp": bp, "fp_s": t1 - t0, "bp_s": t2 - t1, "units": units}
 
 
 def run_reference(args):
-    """--impl reference: the CPU path (FP64 port of the model) on host cores."""
+    """--impl reference: the reference's CPU path for this workload on the
+    host cores.  The reference has no CPU 3D projector (its cone FP/BP exist
+    only as CUDA kernels), so this is the FP64 port of its model (oracle/),
+    over all host threads, on a bounded sample per step: the FP of
+    --ref-views views and the BP of --ref-slices z-slices over all views.
+    Imports nothing of the library (geometry from the reference build or the
+    oracle, phantom from its file)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import torch
-    astra, vg, pg = workload(args.n, args.views, args.det)
-    proj_mod = importlib.import_module("astra-toolbox_b200.projector")
-    pr = proj_mod.Projector3D.__new__(proj_mod.Projector3D)
-    pr.geom = importlib.import_module("astra-toolbox_b200.geometry").Geometry3D(vg, pg)
-    pr.proj_shape = pr.geom.proj_shape
-    ph = importlib.import_module("astra-toolbox_b200.phantom")
+    views, vs, geom_src = reference_geometry(args.n, args.views, args.det)
+    ph = phantom_module()
     vol = ph.ellipsoids((args.n, args.n, args.n), N_ELL, seed=0, device="cpu").numpy()
+    # BP input: the oracle's time does not depend on the values, and the
+    # full projections of the phantom cannot be computed on the host in a
+    # bench step; a constant array of the full projection shape stands in
+    proj = np.ones((args.det, args.views, args.det), dtype=np.float32)
     threads = os.cpu_count() or 1
+    fp_sel = sample_views(args.views, args.ref_views)
+    bp_sl = sample_slices(args.n, args.ref_slices)
     samples = []
     for i in range(args.warmup + args.steps):
-        g, dt = cpu_sample(vol, pr, args.ref_views, threads)
+        r = oracle_sample(vol, proj, views, vs, args.det, args.det, fp_sel, bp_sl, threads)
         if i >= args.warmup:
-            samples.append((g, dt))
+            samples.append((r["units"] / (r["fp_s"] + r["bp_s"]) / 1e9, r["fp_s"] + r["bp_s"]))
     gups = float(np.median([s[0] for s in samples]))
     ms = float(np.median([s[1] for s in samples])) * 1e3
-    sample = ("FP64 oracle forward projection of %d of the %d views per step (all %d^2 rays of each view), "
-              "GUPS extrapolated per view" % (args.ref_views, args.views, args.det))
+    sample = ("FP64 oracle (CPU port of the reference's cone model) per step: forward projection of views %s "
+              "(all %d^2 rays) and backprojection of z-slices %s over all %d views; GUPS = their voxel-view "
+              "updates / time; geometry from %s" % (fp_sel, args.det, bp_sl, args.views, geom_src))
     line = {"metric": "cone FP/BP GUPS at 512^3x720", "value": gups, "unit": "GUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -150,6 +216,66 @@ def run_reference(args):
             "e2e": {"value": gups, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def ref_cuda_block(torch, dev, vol, proj_ours, back_ours, args, reps=3):
+    """The reference's own CUDA build (oracle/_ref: astraCUDA3d::ConeFP /
+    ConeBP, cuda/3d/cone_fp.cu:444-504, cone_bp.cu:380-401, unchanged) on the
+    same inputs and GPU: CUDA-event time per call (median of reps after one
+    warm-up call; every reference call allocates its texture array and
+    synchronises, as inside ASTRA), clocks during those calls, speed-ups of
+    this library's calls, and the relative L2 difference of the outputs."""
+    from oracle import ref
+    if not ref.available():
+        return {"unavailable": "oracle/_ref/libastra_ref.so is not built"}
+    if vol.dtype != torch.float32:
+        return {"unavailable": "the reference projects float32 data only"}
+    views, vs, _ = reference_geometry(args.n, args.views, args.det)
+    views = np.ascontiguousarray(views)
+    vsc = np.ascontiguousarray(vs, dtype=np.float32)
+    n, na, nd = args.n, args.views, args.det
+    L = ref.lib()
+    out_p = torch.zeros_like(proj_ours)
+    out_v = torch.zeros_like(back_ours)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, out):
+        ts = []
+        for i in range(reps + 1):
+            out.zero_()
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = fn()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            assert rc == 0, "reference call failed"
+            if i > 0:
+                ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    sampler = ClockSampler(dev.index or 0)
+    sampler.start()
+    time.sleep(0.3)
+    t_fp = timed(lambda: L.ref_cuda_fp3d(2, views.ctypes.data, n, n, n, na, nd, nd, vsc.ctypes.data, 1.0, 1,
+                                         vol.data_ptr(), out_p.data_ptr()), out_p)
+    # both BPs read the same projections: this library's FP output
+    t_bp = timed(lambda: L.ref_cuda_bp3d(2, 0, views.ctypes.data, n, n, n, na, nd, nd, vsc.ctypes.data, 1.0, 1,
+                                         proj_ours.data_ptr(), out_v.data_ptr()), out_v)
+    clocks = sampler.stop()
+
+    def rl2(a, b):
+        return float(torch.linalg.vector_norm((a - b).double()) / torch.linalg.vector_norm(b.double()))
+
+    upd = float(n) ** 3 * na
+    res = {"what": "reference ConeFP / ConeBP built from its sources (oracle/ref.mk), same inputs, same GPU",
+           "fp_ms": t_fp, "bp_ms": t_bp, "fp_gups": upd / t_fp / 1e6, "bp_gups": upd / t_bp / 1e6,
+           "fpbp_gups": 2 * upd / (t_fp + t_bp) / 1e6,
+           "fp_rel_l2_ours_vs_ref": rl2(proj_ours, out_p), "bp_rel_l2_ours_vs_ref": rl2(back_ours, out_v),
+           "clocks": clocks}
+    del out_p, out_v
+    return res
 
 
 def _timed_region(torch, stream, fn, steps):
@@ -559,9 +685,13 @@ def main():
     ap.add_argument("--views", type=int, default=N_ANG)
     ap.add_argument("--det", type=int, default=N_DET)
     ap.add_argument("--dtype", default="float32", choices=["float32", "float16", "bfloat16"])
-    ap.add_argument("--ref-views", type=int, default=2)
+    ap.add_argument("--ref-views", type=int, default=2, help="FP views per step of --impl reference")
+    ap.add_argument("--ref-slices", type=int, default=1, help="BP z-slices per step of --impl reference")
+    ap.add_argument("--parity-views", type=int, default=4, help="FP views of the CPU baseline / parity sample")
+    ap.add_argument("--parity-slices", type=int, default=3, help="BP z-slices of the CPU baseline / parity sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA build")
     ap.add_argument("--workload", default="fpbp",
                     choices=["fpbp", "fdk", "sirt3d", "cgls3d", "batch2d", "stream", "sart2d", "cyl"])
     ap.add_argument("--budget-gb", type=float, default=4.0, help="device budget of --workload stream")
@@ -722,14 +852,48 @@ def main():
                    "device_data_path": dpath}
         del dvol, dproj, dback
 
+    # CPU baseline and parity: the FP64 oracle on a sample of this workload
+    # (views of the FP, z-slices of the BP), run once after the timed region
+    # on the same inputs; its outputs are compared with this run's GPU
+    # outputs on the same views and slices (the full-size accuracy of the
+    # timed configuration)
     cpu = None
+    parity = None
     if rank == 0 and not args.no_cpu:
         vcpu = vol.float().cpu().numpy()
+        pcpu = proj.float().cpu().numpy()
         threads = os.cpu_count() or 1
-        g, dt = cpu_sample(vcpu, pr, args.ref_views, threads)
-        cpu = {"value": g, "unit": "GUPS", "cores": threads, "kind": "port",
-               "sample": "FP64 oracle forward projection of %d views of this workload on %d host threads "
-                         "(%.1f s), GUPS per view" % (args.ref_views, threads, dt)}
+        fp_sel = sample_views(args.views, args.parity_views)
+        bp_sl = sample_slices(args.n, args.parity_slices)
+        nv_, na_, nu_ = pr.proj_shape
+        r = oracle_sample(vcpu, pcpu, pr.geom.views_array(), pr.geom.vol_scale, nu_, nv_, fp_sel, bp_sl, threads)
+        dt = r["fp_s"] + r["bp_s"]
+        cpu = {"value": r["units"] / dt / 1e9, "unit": "GUPS", "cores": threads, "kind": "port",
+               "sample": "FP64 oracle (CPU port of the reference's cone model) on %d host threads: forward "
+                         "projection of views %s (all %d^2 rays, %.1f s) and backprojection of z-slices %s over "
+                         "all %d views (%.1f s); GUPS = their voxel-view updates / time"
+                         % (threads, fp_sel, args.det, r["fp_s"], bp_sl, args.views, r["bp_s"])}
+        del pcpu
+
+        def rl2(a, b):
+            return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+        got_fp = proj[:, fp_sel, :].double().cpu().numpy()
+        got_bp = back[bp_sl].double().cpu().numpy()
+        parity = {"fp_rel_l2_vs_oracle": rl2(got_fp, r["fp"]), "fp_views": fp_sel,
+                  "bp_rel_l2_vs_oracle": rl2(got_bp, r["bp"]), "bp_slices": bp_sl,
+                  "fp_rel_l2_worst_view": max(rl2(got_fp[:, i], r["fp"][:, i]) for i in range(len(fp_sel))),
+                  "bp_rel_l2_worst_slice": max(rl2(got_bp[i], r["bp"][i]) for i in range(len(bp_sl))),
+                  "tolerance": 1e-5 if args.dtype == "float32" else None,
+                  "oracle": "FP64 restatement of cone_fp.cu:154-231 / cone_bp.cu:55-133 (oracle/b2t_oracle.c) on "
+                            "this run's inputs: FP of the phantom, BP of this run's FP output"}
+    ref_cuda = None
+    if rank == 0 and not args.no_ref_cuda:
+        ref_cuda = ref_cuda_block(torch, dev, vol, proj, back, args)
+        if "fp_ms" in ref_cuda:
+            ref_cuda["fp_speedup"] = ref_cuda["fp_ms"] / fp_ms
+            ref_cuda["bp_speedup"] = ref_cuda["bp_ms"] / bp_ms
+            ref_cuda["fpbp_speedup"] = (ref_cuda["fp_ms"] + ref_cuda["bp_ms"]) / ms_step
 
     # roofline of the dominant call (the larger of FP and BP).  The projectors
     # are bound by on-chip interpolation reads, not by HBM: the forward
@@ -799,7 +963,7 @@ def main():
                 "fp_ms": fp_ms, "bp_ms": bp_ms,
                 "fp_gups": updates / (fp_ms * 1e-3) / 1e9, "bp_gups": updates / (bp_ms * 1e-3) / 1e9,
                 "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu}
+                "cpu_baseline": cpu, "parity": parity, "ref_cuda": ref_cuda}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

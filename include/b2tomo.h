@@ -75,6 +75,26 @@ b2t_status b2t_device_errors(uint32_t *flags);
  * warps.  Synchronises the device.  A performance diagnostic; the reference
  * has no counterpart. */
 b2t_status b2t_bp_path_stats(uint64_t stats[4]);
+
+/* Failure-handling test hooks; the reference has no counterpart.
+ * b2t_debug_fail_alloc(n), n >= 1: the n-th device allocation the library
+ * makes from now on (any thread) fails with B2T_ERR_NO_MEMORY without
+ * allocating, as a real out-of-memory would; n = 0 disarms it.  *pending (if
+ * not null) receives the allocations that were still to go before the
+ * previously armed failure (0: it fired, or none was armed).
+ * b2t_debug_live_allocations: the device allocations the library holds now
+ * (scratch, algorithm buffers, batch tables), to check that a failed call
+ * released what it had taken.
+ * b2t_selftest_bounded_wait: one warp waits for something nothing completes,
+ * an mbarrier phase (which = 0) or a device flag (which = 1), with the
+ * bounded wait the pipelined kernels use, limited to limit_cycles (at most
+ * 4e9, about two seconds); the wait gives up, records bit 0 of the device
+ * error word and returns.  Synchronises the stream, reads and clears the
+ * error word and returns B2T_ERR_TIMEOUT when the bit was set. */
+b2t_status b2t_debug_fail_alloc(int64_t nth, int64_t *pending);
+int64_t b2t_debug_live_allocations(void);
+b2t_status b2t_selftest_bounded_wait(int32_t which, uint64_t limit_cycles, void *stream);
+
 /* Scratch buffers (padded copies, cell copies, filter operands) come from a
  * stream-ordered memory pool of the library, one per device, that keeps freed
  * blocks cached so repeated calls do not map device memory again.  This
@@ -455,10 +475,12 @@ b2t_status b2t_dot_f64(const void *a, const void *b, size_t n, int32_t dtype, do
  * hands out all device memory from its own fixed pool): the partial sums live
  * in a fixed 32 KB array built into the library, present on every GPU that
  * loads it until the process exits.  Limit: n <= 4096 * 2^20 elements; larger
- * n returns B2T_ERR_INVALID_ARG before any device work.  All calls on one
- * device share the array, so calls that overlap on the GPU race: serialise
- * them.  The first call on each device looks up the array's device address
- * with that device current. */
+ * n returns B2T_ERR_INVALID_ARG before any device work.  Up to 1184 * 2^20
+ * elements it launches exactly as b2t_dot_f64 does and returns the same
+ * bits.  All calls on one device share the array, so calls that overlap on
+ * the GPU race: serialise them.  Every call looks up the array's device
+ * address on the current device (a cheap host lookup that stays valid after
+ * a cudaDeviceReset). */
 b2t_status b2t_dot_f64_noalloc(const void *a, const void *b, size_t n, int32_t dtype, double *result,
                                void *stream);
 

@@ -552,8 +552,11 @@ static void orc_bp3d_range(void *vctx, long begin, long end)
     else
         outs = c->out_scale * c->vs[0] * c->vs[1] * c->vs[2];
     outs /= (double)(R * R * R);
-    for (long Z = begin; Z < end; ++Z) {
-        for (long Y = 0; Y < c->ny; ++Y) {
+    /* [begin, end) are volume rows Z * ny + Y */
+    for (long row = begin; row < end; ++row) {
+        const long Z = row / c->ny;
+        {
+            const long Y = row % c->ny;
             for (long X = 0; X < c->nx; ++X) {
                 double x = X - 0.5 * c->nx + 0.5;
                 double y = Y - 0.5 * c->ny + 0.5;
@@ -600,10 +603,10 @@ int orc_bp3d(int kind, int kernel, const double *views, long nx, long ny, long n
     c.co = (orc_bpview *)malloc(sizeof(orc_bpview) * (size_t)na);
     if (!c.co) return 2;
     for (long a = 0; a < na; ++a) orc_bp_coeffs(kind, kernel, views + 12 * a, vs, &c.co[a]);
-    long n = z_end - z_begin;
-    /* slices are split across threads in absolute z coordinates */
+    /* rows Z * ny + Y of slices [z_begin, z_end) are split across threads */
+    long n = (z_end - z_begin) * ny;
     if (nthreads <= 1 || n <= 1) {
-        orc_bp3d_range(&c, z_begin, z_end);
+        orc_bp3d_range(&c, z_begin * ny, z_end * ny);
     } else {
         if (nthreads > 256) nthreads = 256;
         if (nthreads > n) nthreads = (int)n;
@@ -612,8 +615,8 @@ int orc_bp3d(int kind, int kernel, const double *views, long nx, long ny, long n
         for (int t = 0; t < nthreads; ++t) {
             jobs[t].fn = orc_bp3d_range;
             jobs[t].ctx = &c;
-            jobs[t].begin = z_begin + n * t / nthreads;
-            jobs[t].end = z_begin + n * (t + 1) / nthreads;
+            jobs[t].begin = z_begin * ny + n * t / nthreads;
+            jobs[t].end = z_begin * ny + n * (t + 1) / nthreads;
             pthread_create(&th[t], NULL, orc_thread_main, &jobs[t]);
         }
         for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);

@@ -430,3 +430,50 @@ def cylcone_bp(views, proj, vol_shape, vol_scale, out_scale=1.0, tex8=False):
                               proj.ctypes.data, vol.ctypes.data)
     assert rc == 0
     return vol
+
+
+def bp3d_slices(kind, views, proj, vol_shape, slices, vol_scale=(1.0, 1.0, 1.0), out_scale=1.0,
+                kernel=KER_DEFAULT, nthreads=None):
+    """Backprojection of single z-slices of a (nz, ny, nx) volume; returns
+    float64 [len(slices)][y][x].  Each slice is backprojected as a one-slice
+    volume centred on the origin, with the views moved along z by the slice
+    centre's offset from the volume centre (the source point of a cone view
+    and the detector origin; a parallel view's ray direction stays), so a
+    full-size check holds one slice instead of the whole volume in memory."""
+    views = _c(views, np.float64)
+    nz, ny, nx = vol_shape
+    out = np.zeros((len(slices), ny, nx), dtype=np.float64)
+    for i, z in enumerate(slices):
+        zc = float(z) + 0.5 - 0.5 * nz
+        w = views.copy()
+        if kind == CONE:
+            w[:, 2] -= zc
+        w[:, 5] -= zc
+        out[i] = bp3d(kind, w, proj, (1, ny, nx), vol_scale, out_scale, kernel, nthreads=nthreads)[0]
+    return out
+
+
+def cone_views(angles, det_cols, det_rows, src_origin, origin_det, det_spacing_x=1.0, det_spacing_y=1.0):
+    """Per-view vectors of a circular cone geometry for a volume of unit voxels
+    centred on the origin (genConeProjections, src/GeometryUtil3D.cpp:42-83;
+    convertAstraGeometry is then the identity): (n, 12) float64, the float32
+    angles promoted to double as the reference does.  numpy's cos / sin may
+    differ from the C library's in the last bit, so this is for workloads
+    that need the geometry without the reference build, not for bit-exact
+    checks."""
+    a = np.asarray(angles, dtype=np.float32).astype(np.float64)
+    c, s = np.cos(a), np.sin(a)
+    sod, odd = float(src_origin), float(origin_det)
+    du, dv = float(det_spacing_x), float(det_spacing_y)
+    out = np.zeros((a.size, 12), dtype=np.float64)
+
+    def rot(k, bx, by, bz):
+        out[:, k] = bx * c - by * s
+        out[:, k + 1] = bx * s + by * c
+        out[:, k + 2] = bz
+
+    rot(0, 0.0, -sod, 0.0)
+    rot(3, det_cols * du * -0.5, odd, det_rows * dv * -0.5)
+    rot(6, du, 0.0, 0.0)
+    rot(9, 0.0, 0.0, dv)
+    return out

@@ -3,7 +3,9 @@
 # Test infrastructure only: the product never links it.  Outputs go to _ref/
 # (git-ignored; the built .so travels with the repository snapshot).
 #   make -f ref.mk REF=/path/to/astra-toolbox -j8
-REF ?= /root/reference
+ifeq ($(REF),)
+$(error REF=<reference source tree> is required)
+endif
 OUT = _ref
 SRCS = $(wildcard $(REF)/src/*.cpp)
 CUS = $(wildcard $(REF)/cuda/*.cu) $(wildcard $(REF)/cuda/2d/*.cu) $(wildcard $(REF)/cuda/3d/*.cu)

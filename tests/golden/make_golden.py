@@ -241,5 +241,6 @@ def main(outdir, only=None):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"),
-         sys.argv[2] if len(sys.argv) > 2 else None)
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py OUTDIR [NAME_SUBSTRING]")
+    main(sys.argv[1], sys.argv[2] if len(sys.argv) > 2 else None)

@@ -120,3 +120,22 @@ def test_dominant_axis_matches_rule(astra, geo, orc):
     g = geo.Geometry3D(vg, astra.create_proj_geom('cone', 1.0, 1.0, 8, 8, ang, 40.0, 20.0))
     dirs = [orc.dominant_axis3d(orc.CONE, v, 8, 8) for v in g.views_array()]
     assert dirs[0] == 1 and dirs[1] == 0
+
+
+def test_bp3d_slices_match_z_range(orc):
+    """The single-slice BP used by the full-size checks equals the slices of a
+    whole-volume BP (cone and parallel)."""
+    rng = np.random.default_rng(4)
+    ang = np.linspace(0, 2 * np.pi, 9, endpoint=False).astype(np.float32)
+    for kind in (orc.CONE, orc.PAR3D):
+        if kind == orc.CONE:
+            views = orc.cone_views(ang, 20, 18, 60.0, 30.0)
+        else:
+            views = orc.cone_views(ang, 20, 18, 60.0, 30.0)
+            d = views[:, 3:6] + 10 * views[:, 6:9] + 9 * views[:, 9:12] - views[:, 0:3]
+            views[:, 0:3] = d / np.linalg.norm(d, axis=1, keepdims=True)
+        proj = rng.random((18, 9, 20), dtype=np.float32)
+        full = orc.bp3d(kind, views, proj, (12, 14, 16))
+        sl = orc.bp3d_slices(kind, views, proj, (12, 14, 16), [0, 5, 11])
+        for i, z in enumerate([0, 5, 11]):
+            assert np.allclose(sl[i], full[z], rtol=1e-12, atol=1e-12)
