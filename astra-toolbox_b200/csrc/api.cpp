@@ -147,6 +147,14 @@ b2t_status b2t_selftest_bounded_wait(int32_t which, uint64_t limit_cycles, void 
     return selftest_wait_impl(which, (long long)limit_cycles, static_cast<cudaStream_t>(stream));
 }
 
+b2t_status b2t_fp_path_stats(uint64_t *stats)
+{
+    clear_error();
+    if (!stats) return fail(B2T_ERR_INVALID_ARG, "b2t_fp_path_stats: null pointer");
+    B2T_CUDA_TRY(cudaDeviceSynchronize(), "b2t_fp_path_stats synchronize");
+    return fp_path_stats_impl(stats);
+}
+
 b2t_status b2t_bp_path_stats(uint64_t *stats)
 {
     clear_error();

@@ -752,9 +752,10 @@ b2t_status device_errors_impl(uint32_t *flags)
     B2T_CUDA_TRY(cudaMemcpyFromSymbol(&v, g_b2t_device_errors, sizeof(v)), "read device error word");
     const unsigned int zero = 0;
     B2T_CUDA_TRY(cudaMemcpyToSymbol(g_b2t_device_errors, &zero, sizeof(zero)), "clear device error word");
-    uint32_t w = 0;
+    uint32_t w = 0, f = 0;
     B2T_TRY(ramp_tc_errors(&w));
-    *flags = v | w;
+    B2T_TRY(fp_slab_errors(&f));
+    *flags = v | w | f;
     return B2T_OK;
 }
 

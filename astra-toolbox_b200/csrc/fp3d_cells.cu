@@ -30,6 +30,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -456,6 +457,9 @@ __global__ void __launch_bounds__(32 * VCOLS * VPC, (IDX32 ? 2048 : 1536) / (32 
     store_ray<T>(L, V.a, u, v, acc);
 }
 
+// Launches of the cell kernels since the last b2t_fp_path_stats.
+static std::atomic<unsigned long long> g_cell_launches{0};
+
 // Launch shape of the cell forward projector: views per CTA.
 struct CellShape {
     int vpc;
@@ -497,6 +501,7 @@ static b2t_status launch_cells_shape(const FPLaunch &P, int nviews, const b2t_di
     dim3 grid((unsigned)((nviews + VPC - 1) / VPC), (d.det_u + 31) / 32, (d.det_v + VROWS - 1) / VROWS);
     fp3d_cell_kernel<T, VPC, VROWS><<<grid, dim3(32, VROWS, VPC), 0, s>>>(P);
     count_launches(1);
+    g_cell_launches.fetch_add(1);
     B2T_CUDA_TRY(cudaGetLastError(), "fp3d_cell_kernel launch");
     return B2T_OK;
 }
@@ -524,6 +529,7 @@ static b2t_status launch_cols_shape(const FPLaunch &P, int nviews, const b2t_dim
     else
         fp3d_col_kernel<T, VPC, VCOLS, false><<<grid, dim3(32, VCOLS, VPC), 0, s>>>(P);
     count_launches(1);
+    g_cell_launches.fetch_add(1);
     B2T_CUDA_TRY(cudaGetLastError(), "fp3d_col_kernel launch");
     return B2T_OK;
 }
@@ -541,8 +547,8 @@ static b2t_status launch_cols(const FPLaunch &P, int nviews, const b2t_dims3d &d
 }
 
 template <typename T>
-b2t_status build_cells_t(const b2t_geom3d *g, const void *vol, size_t vol_pitch, const bool need[3], cudaStream_t s,
-                         FPCells &c)
+b2t_status build_cells_t(const b2t_geom3d *g, const void *vol, size_t vol_pitch, const bool need[3],
+                         const bool slab[3], cudaStream_t s, FPCells &c)
 {
     using C = typename CellT<T>::type;
     const b2t_dims3d &d = g->dims;
@@ -553,7 +559,17 @@ b2t_status build_cells_t(const b2t_geom3d *g, const void *vol, size_t vol_pitch,
     c.vol_z = d.vol_z;
     for (int dir = 0; dir < 3; ++dir) {
         c.base[dir] = nullptr;
+        c.slab[dir] = false;
         if (!need[dir]) continue;
+        if (slab[dir]) {
+            // slab copy for the TMA-staged kernel (fp3d_slab.cu)
+            if (!c.mem[dir]) c.mem[dir].reset(new Scratch);
+            B2T_TRY(c.mem[dir]->alloc(fp_slab_copy_bytes(d, dir), s, "b2t_fp3d scratch (slab copy)"));
+            B2T_TRY(fp_slab_build(d, static_cast<const float *>(vol), vol_pitch, dir, c.mem[dir]->as<void>(), s));
+            c.slab[dir] = true;
+            c.base[dir] = c.mem[dir]->as<void>();
+            continue;
+        }
         int n0, n1, n2;
         if (dir == 0) { n0 = nx; n1 = ny; n2 = nz; }
         else if (dir == 1) { n0 = ny; n1 = nx; n2 = nz; }
@@ -601,6 +617,15 @@ b2t_status project_cells_t(const b2t_geom3d *g, const b2t_params3d *p, const FPC
     b2t_status st = B2T_OK;
     for (int dir = 0; dir < 3 && st == B2T_OK; ++dir) {
         if (!need[dir]) continue;
+        if (c.slab[dir]) {
+            if (!fp_slab_eligible(g, p, c.dtype, dir, dirs)) {
+                st = fail(B2T_ERR_UNSUPPORTED, "b2t_fp3d: views or parameters differ from those the slab copy was "
+                                               "built for");
+                break;
+            }
+            st = fp_slab_project(g, p, c.base[dir], dir, proj, proj_pitch, mode, dirs, s);
+            continue;
+        }
         P.proj = proj;
         P.proj_pitch = (long long)proj_pitch;
         P.nu = d.det_u;
@@ -690,16 +715,22 @@ b2t_status fp3d_autotune_impl(const b2t_geom3d *g, const b2t_params3d *p, const 
     return B2T_OK;
 }
 
+unsigned long long fp_cell_launches_take() { return g_cell_launches.exchange(0); }
+
 FPCells::FPCells() = default;
 FPCells::~FPCells() = default;
 
-b2t_status fp3d_cells_build(const b2t_geom3d *g, const void *vol, size_t vol_pitch, int32_t dtype, const bool need[3],
-                            cudaStream_t s, FPCells &c)
+b2t_status fp3d_cells_build(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch,
+                            int32_t dtype, const bool need[3], cudaStream_t s, FPCells &c)
 {
     if (vol_pitch == 0) vol_pitch = g->dims.vol_x;
-    if (dtype == B2T_F32) return build_cells_t<float>(g, vol, vol_pitch, need, s, c);
-    if (dtype == B2T_F16) return build_cells_t<__half>(g, vol, vol_pitch, need, s, c);
-    return build_cells_t<__nv_bfloat16>(g, vol, vol_pitch, need, s, c);
+    std::vector<int> dirs(g->dims.angles);
+    for (uint32_t a = 0; a < g->dims.angles; ++a) dirs[a] = dominant_axis(g->kind, g->views[a], g->dims);
+    bool slab[3] = {false, false, false};
+    for (int dir = 0; dir < 2; ++dir) slab[dir] = need[dir] && fp_slab_eligible(g, p, dtype, dir, dirs);
+    if (dtype == B2T_F32) return build_cells_t<float>(g, vol, vol_pitch, need, slab, s, c);
+    if (dtype == B2T_F16) return build_cells_t<__half>(g, vol, vol_pitch, need, slab, s, c);
+    return build_cells_t<__nv_bfloat16>(g, vol, vol_pitch, need, slab, s, c);
 }
 
 b2t_status fp3d_cells_project(const b2t_geom3d *g, const b2t_params3d *p, const FPCells &c, void *proj,
@@ -725,7 +756,7 @@ b2t_status fp3d_cells(const b2t_geom3d *g, const b2t_params3d *p, const void *vo
     bool need[3] = {false, false, false};
     for (int dd : dirs) need[dd] = true;
     FPCells c;
-    B2T_TRY(fp3d_cells_build(g, vol, vol_pitch, dtype, need, s, c));
+    B2T_TRY(fp3d_cells_build(g, p, vol, vol_pitch, dtype, need, s, c));
     if (dtype == B2T_F32) return project_cells_t<float>(g, p, c, proj, proj_pitch, mode, dirs, s);
     if (dtype == B2T_F16) return project_cells_t<__half>(g, p, c, proj, proj_pitch, mode, dirs, s);
     return project_cells_t<__nv_bfloat16>(g, p, c, proj, proj_pitch, mode, dirs, s);

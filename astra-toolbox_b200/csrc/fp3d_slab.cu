@@ -1,0 +1,633 @@
+// Ray-driven 3D forward projection from TMA-staged volume slabs.
+//
+// Same model as fp3d_kernel / the cell kernels (the reference's cone_FP_t /
+// par3D_FP_t, cuda/3d/cone_fp.cu:154-231, cuda/3d/par3d_fp.cu:152-230): per
+// ray, the slices of the view's dominant axis are sampled bilinearly at unit
+// steps and the sum is scaled by the ray length factor.
+//
+// For views that march along x or y and whose detector v axis has no
+// component along the marching axis or the in-plane axis (every circular
+// orbit, parallel or cone), all rays of one detector column lie in a plane
+// that contains the z direction: at every slice they share the in-plane
+// texel and its weight, and only their z position differs.  The kernel is
+// built on that:
+//
+//   - the volume is copied once per call and marching axis into a slab copy
+//     of z-pairs [slice][in-plane texel + 2][z texel + 2] holding
+//     (v[z], v[z + 1] - v[z]) (z contiguous, a zero border of two texels), so
+//     a bilinear sample is two 8-byte loads and two FMAs along z;
+//   - a CTA traces SLAB_W consecutive views x SLAB_U consecutive detector
+//     columns x SLAB_ROWS detector rows; a compute warp owns one column, each
+//     lane SLAB_R rows of it (v, v + 32, ...) in both views, so the in-plane
+//     position, texel split and buffer row of a slice are computed once per
+//     view for SLAB_R rays and the slice's wait and release once for all
+//     SLAB_W x SLAB_R of them;
+//   - a producer warp works out the buffer box of 32 slices at a time (one
+//     slice per lane) from the tile's corner rays (the rays of a detector
+//     rectangle cross a slice in the convex hull of its corners' crossings),
+//     clamped to the zero border, and loads each slice's box with 4-row
+//     cp.async.bulk.tensor boxes of one of two widths (96 or 160 texels;
+//     plain tile loads, no multicast) into one of SLAB_STAGES slice buffers;
+//     a box lands densely, so its width is the buffer's row pitch;
+//   - compute warps interpolate from shared memory in FP32.  Samples outside
+//     the volume read the zero border (positions clamped to it on the slices
+//     where some ray of the warp leaves the volume);
+//   - a slice whose box does not fit a buffer (extreme magnification) is read
+//     from the slab copy in global memory instead.
+//
+// Every mbarrier wait is bounded (about a second); on a timeout the kernel
+// sets B2T_DEVERR_WAIT_TIMEOUT in its error word, lets its own copies land
+// and returns.  The reference has no such kernel; its FP samples a 3D
+// texture per slice (cone_fp.cu:154-231).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdlib>
+#include <vector>
+
+#include "b2t_internal.h"
+#include "proj3d.h"
+#include "tma.h"
+
+namespace b2t {
+
+// error word of this translation unit (read by b2t_device_errors)
+static __device__ unsigned int g_fp_slab_errors = 0;
+// slices staged in shared memory / read from global memory, summed over CTAs
+// (read and cleared by b2t_fp_path_stats)
+static __device__ unsigned long long g_fp_slab_slices[2] = {0, 0};
+
+namespace {
+
+constexpr int SLAB_W = 2;                   // views per CTA (every warp traces both)
+constexpr int SLAB_U = 14;                  // detector columns per CTA, one compute warp each
+constexpr int SLAB_R = 4;                   // rows per lane and view: v, v + 32, ...
+constexpr int SLAB_ROWS = 32 * SLAB_R;      // detector rows per CTA
+constexpr int SLAB_WARPS = SLAB_U;          // compute warps; one more produces
+constexpr int SLAB_THREADS = 32 * (SLAB_WARPS + 1);
+constexpr int SLAB_BY = 24;                 // buffer rows (in-plane texels) per slice
+constexpr int SLAB_WA = 96, SLAB_WB = 160;  // box widths (z-pairs): the buffer row pitch of a slice
+constexpr int SLAB_BOX_Y = 4;               // rows per TMA box
+constexpr int SLAB_STAGES = 3;              // slices in flight
+constexpr int SLAB_SLOT = SLAB_BY * SLAB_WB;  // z-pairs per slice buffer
+constexpr int SLAB_MAX_VIEWS = 448;
+constexpr long long SLAB_WAIT = 2000000000LL;  // cycles (about a second)
+constexpr float SPLIT_M = 12582912.0f;      // 1.5 * 2^23
+constexpr int SPLIT_BITS = 0x4B400000;      // bits of SPLIT_M
+
+static_assert(SLAB_BY % SLAB_BOX_Y == 0, "buffer made of whole boxes");
+static_assert(4 * SLAB_W <= 32, "the producer projects the corner rays one per lane");
+
+struct alignas(64) SlabLaunch {
+    CUtensorMap tmap[2];   // slab copy as 8-byte z-pairs, dims (n2 + 4, n1 + 4, n0); box widths WA, WB
+    const float2 *copy;    // z-pair (s, k1, k2) at (s * py + k1 + 2) * pz + k2 + 2
+    long long py, pz;
+    void *proj;            // output projections [v][angle][u]
+    long long proj_pitch;
+    int n0, n1, n2, nu, nv, na;
+    int accumulate;
+    float f1, f2, mul;     // ray length factors and output scale
+    int nviews;
+    FPView views[SLAB_MAX_VIEWS];
+};
+
+// A slice's buffer: sel 0 / 1 the box width WA / WB, -1 read global memory;
+// rbase folds the box origin and the texel split's offset into the byte
+// address: texel (k1, k2) at slot + rbase + bits1 * 8 pitch + bits2 * 8
+struct SlabInfo {
+    int sel, rbase, pad0, pad1;
+};
+
+__device__ __forceinline__ float ray_setup(const FPView &V, float uu, float vv, float &A1, float &B1h, float &A2,
+                                           float &B2h)
+{
+    const float den = fmaf(vv, V.e[2], fmaf(uu, V.e[1], V.e[0]));
+    const float inv = 1.0f / den;
+    A1 = fmaf(vv, V.m1[2], fmaf(uu, V.m1[1], V.m1[0])) * inv;
+    A2 = fmaf(vv, V.m2[2], fmaf(uu, V.m2[1], V.m2[0])) * inv;
+    B1h = fmaf(vv, V.n1[2], fmaf(uu, V.n1[1], V.n1[0])) * inv + 0.5f;
+    B2h = fmaf(vv, V.n2[2], fmaf(uu, V.n2[1], V.n2[0])) * inv + 0.5f;
+    return den;
+}
+
+// Base texel of position qh (floor), by rounding down qh + 1.5 * 2^23.
+__device__ __forceinline__ int floor_texel(float qh) { return __float_as_int(__fadd_rd(qh, SPLIT_M)) - SPLIT_BITS; }
+
+// Slices s of [0, n0) at which a ray's base texel along one axis stays in
+// [-2, n] (the copy's zero border), intersected into [lo, hi].
+__device__ __forceinline__ void clip_axis(float A, float Bh, int n, int n0, int &lo, int &hi)
+{
+    // qh = A s + Bh in [-2, n + 1) up to rounding (a nearly constant qh: the
+    // whole range); then step inwards until the texel of the end slices is
+    // inside.  fmaf(A, s, Bh) is monotone in s, so texels inside at both end
+    // slices are inside at every slice between them; ends that stay outside
+    // leave the range empty.
+    float a = -1.0f, b = (float)n0;
+    if (fabsf(A) >= 1e-12f) {
+        const float s1 = (-2.0f - Bh) / A, s2 = ((float)n + 1.0f - Bh) / A;
+        a = fminf(s1, s2);
+        b = fmaxf(s1, s2);
+    }
+    int l = max(lo, (int)ceilf(fmaxf(a, -1.0f)));
+    int h = min(hi, (int)floorf(fminf(b, (float)n0)));
+    for (int it = 0; it < 4 && l <= h; ++it) {
+        const int k = floor_texel(fmaf(A, (float)l, Bh));
+        if (k >= -2 && k <= n) break;
+        ++l;
+    }
+    for (int it = 0; it < 4 && l <= h; ++it) {
+        const int k = floor_texel(fmaf(A, (float)h, Bh));
+        if (k >= -2 && k <= n) break;
+        --h;
+    }
+    if (l <= h) {
+        const int kl = floor_texel(fmaf(A, (float)l, Bh)), kh = floor_texel(fmaf(A, (float)h, Bh));
+        if (kl < -2 || kl > n || kh < -2 || kh > n) h = l - 1;
+    }
+    lo = l;
+    hi = h;
+}
+
+// z-pair at a shared-memory byte address (plus an immediate offset)
+template <int OFF> __device__ __forceinline__ float2 lds_pair(uint32_t a)
+{
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2+%3];" : "=f"(v.x), "=f"(v.y) : "r"(a), "n"(OFF));
+    return v;
+}
+
+__device__ __forceinline__ int warp_min(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ int warp_max(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// The detector ray (column u, row v) of a tile, clamped into the detector:
+// lanes and corners outside the detector trace a copy of a real ray and
+// store nothing.
+__device__ __forceinline__ float det_uu(const SlabLaunch &L, int u) { return (float)min(u, L.nu - 1) + 0.5f - 0.5f * (float)L.nu; }
+__device__ __forceinline__ float det_vv(const SlabLaunch &L, int v) { return (float)min(v, L.nv - 1) + 0.5f - 0.5f * (float)L.nv; }
+
+// Producer warp: the buffer box of every slice of the CTA's range and its loads.
+__device__ __noinline__ void slab_produce(const SlabLaunch &L, float2 *buf, uint64_t *full, uint64_t *empty,
+                                          SlabInfo *info, int lane, int s_lo, int s_hi)
+{
+    // The tile's corner rays (view, column end, row end), set up once: lane
+    // c < 4 SLAB_W computes corner c, then every lane holds all of them.  The
+    // rays of a detector rectangle cross a slice inside the convex hull of the
+    // corners' crossings when their denominators share one sign.
+    constexpr int NC = 4 * SLAB_W;
+    float cA1[NC], cB1[NC], cA2[NC], cB2[NC];
+    bool hull;
+    {
+        const int c = lane % NC;
+        const int w = c >> 2, uc = c & 1, vc = (c >> 1) & 1;
+        const int vi = min((int)blockIdx.x * SLAB_W + w, L.nviews - 1);
+        const int u = (int)blockIdx.y * SLAB_U + (uc ? SLAB_U - 1 : 0);
+        const int v = (int)blockIdx.z * SLAB_ROWS + (vc ? SLAB_ROWS - 1 : 0);
+        float A1, B1h, A2, B2h;
+        const float den = ray_setup(L.views[vi], det_uu(L, u), det_vv(L, v), A1, B1h, A2, B2h);
+        hull = __all_sync(0xffffffffu, den > 1e-6f) || __all_sync(0xffffffffu, den < -1e-6f);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            cA1[k] = __shfl_sync(0xffffffffu, A1, k);
+            cB1[k] = __shfl_sync(0xffffffffu, B1h, k);
+            cA2[k] = __shfl_sync(0xffffffffu, A2, k);
+            cB2[k] = __shfl_sync(0xffffffffu, B2h, k);
+        }
+    }
+    const uint32_t sbuf = smem_u32(buf);
+    const int nst = s_hi - s_lo + 1;
+    unsigned long long n_staged = 0, n_global = 0;
+    for (int b0 = 0; b0 < nst; b0 += 32) {
+        // lane k: the buffer box of slice s_lo + b0 + k from the corners'
+        // texels, clamped to the zero border, one texel of margin for rounding
+        const float sf = (float)(s_lo + b0 + lane);
+        int k1lo = 0x7fffffff, k1hi = -0x7fffffff, k2lo = 0x7fffffff, k2hi = -0x7fffffff;
+        bool sane = true;
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            const float q1 = fmaf(cA1[k], sf, cB1[k]), q2 = fmaf(cA2[k], sf, cB2[k]);
+            sane = sane && fabsf(q1) < 1.0e7f && fabsf(q2) < 1.0e7f;
+            const int k1 = min(max(floor_texel(q1), -2), L.n1), k2 = min(max(floor_texel(q2), -2), L.n2);
+            k1lo = min(k1lo, k1);
+            k1hi = max(k1hi, k1);
+            k2lo = min(k2lo, k2);
+            k2hi = max(k2hi, k2);
+        }
+        const int y0 = max(k1lo - 1, -2), y1 = min(k1hi + 2, L.n1 + 1);
+        const int zlo = max(k2lo - 1, -2), z1 = min(k2hi + 2, L.n2 + 1);
+        const int z0 = ((zlo + 2) & ~1) - 2;  // TMA: (z0 + 2) * 8 bytes on a 16-byte boundary
+        const int ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+        const int sel = (!hull || !sane || ny > SLAB_BY || nz > SLAB_WB) ? -1 : (nz <= SLAB_WA ? 0 : 1);
+        const int pitch = sel == 0 ? SLAB_WA : SLAB_WB;
+        const int nby = (ny + SLAB_BOX_Y - 1) / SLAB_BOX_Y;
+        const int cnt = min(32, nst - b0);
+        if (lane < cnt) {
+            if (sel >= 0) ++n_staged;
+            else ++n_global;
+        }
+        // the slices in order: each waits for its buffer, then its own lane
+        // writes the record and issues the loads
+        for (int k = 0; k < cnt; ++k) {
+            const int st = b0 + k;
+            const int slot = st % SLAB_STAGES;
+            if (st >= SLAB_STAGES) {
+                const uint32_t par = (uint32_t)(((st / SLAB_STAGES) - 1) & 1);
+                if (!__all_sync(0xffffffffu, mbar_wait_bounded_sleep(&empty[slot], par, SLAB_WAIT))) {
+                    if (lane == 0) atomicOr(&g_fp_slab_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
+                    // the loads of the slices still in the buffers land first
+                    for (int q = max(0, st - SLAB_STAGES); q < st; ++q)
+                        (void)mbar_wait_bounded_sleep(&full[q % SLAB_STAGES], (uint32_t)((q / SLAB_STAGES) & 1),
+                                                      SLAB_WAIT);
+                    return;
+                }
+            }
+            if (lane == k) {
+                SlabInfo r;
+                r.sel = sel;
+                r.rbase = (int)(0u - (uint32_t)(SPLIT_BITS + y0) * (uint32_t)(8 * pitch) -
+                                (uint32_t)(SPLIT_BITS + z0) * 8u);
+                r.pad0 = r.pad1 = 0;
+                info[slot] = r;
+                if (sel >= 0) {
+                    // the loads go out after the arrival, whose transaction
+                    // count keeps the phase open until they land
+                    mbar_arrive_expect_tx(&full[slot], (uint32_t)(nby * SLAB_BOX_Y * pitch * sizeof(float2)));
+                    float2 *dst = buf + (size_t)slot * SLAB_SLOT;
+                    for (int by = 0; by < nby; ++by)
+                        tma_load_3d(dst + (size_t)(by * SLAB_BOX_Y) * pitch, &L.tmap[sel], z0 + 2,
+                                    y0 + 2 + by * SLAB_BOX_Y, s_lo + st, &full[slot]);
+                } else {
+                    mbar_arrive(&full[slot]);
+                }
+            }
+            __syncwarp();
+        }
+    }
+    (void)sbuf;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n_staged += __shfl_xor_sync(0xffffffffu, n_staged, o);
+        n_global += __shfl_xor_sync(0xffffffffu, n_global, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&g_fp_slab_slices[0], n_staged);
+        atomicAdd(&g_fp_slab_slices[1], n_global);
+    }
+    // the last slices' loads land before the warp leaves
+    for (int st = max(0, nst - SLAB_STAGES); st < nst; ++st)
+        (void)mbar_wait_bounded_sleep(&full[st % SLAB_STAGES], (uint32_t)((st / SLAB_STAGES) & 1), SLAB_WAIT);
+}
+
+// The lane's rays: both views, SLAB_R rows each.
+struct Rays {
+    float A1[SLAB_W], B1h[SLAB_W];
+    float A2[SLAB_W][SLAB_R], B2h[SLAB_W][SLAB_R];
+    float acc[SLAB_W][SLAB_R];
+};
+
+// One slice of the lane's rays from a shared-memory buffer of row pitch P
+// (z-pairs).  CLAMP: texels clamped to the zero border (slices where a ray of
+// the warp is outside the volume).  rb = the slot's byte address + rbase.
+template <int P, bool CLAMP>
+__device__ __forceinline__ void sample_smem(const SlabLaunch &L, uint32_t rb, float sf, Rays &R)
+{
+    constexpr uint32_t ROWB = 8u * P;
+#pragma unroll
+    for (int w = 0; w < SLAB_W; ++w) {
+        const float q1 = fmaf(R.A1[w], sf, R.B1h[w]);
+        const float t1 = __fadd_rd(q1, SPLIT_M);
+        const float f1 = q1 - (t1 - SPLIT_M);
+        const float g1 = 1.0f - f1;
+        int b1 = __float_as_int(t1);
+        if (CLAMP) b1 = min(max(b1, SPLIT_BITS - 2), SPLIT_BITS + L.n1);
+        const uint32_t row = (uint32_t)b1 * ROWB + rb;
+#pragma unroll
+        for (int r = 0; r < SLAB_R; ++r) {
+            const float q2 = fmaf(R.A2[w][r], sf, R.B2h[w][r]);
+            const float t2 = __fadd_rd(q2, SPLIT_M);
+            const float f2 = q2 - (t2 - SPLIT_M);
+            int b2 = __float_as_int(t2);
+            if (CLAMP) b2 = min(max(b2, SPLIT_BITS - 2), SPLIT_BITS + L.n2);
+            const uint32_t a = (uint32_t)b2 * 8u + row;
+            const float2 p0 = lds_pair<0>(a), p1 = lds_pair<(int)ROWB>(a);
+            // rows k1 and k1 + 1 interpolated along z, then blended by the
+            // shared in-plane weights straight into the sum
+            const float lo = fmaf(f2, p0.y, p0.x), hi = fmaf(f2, p1.y, p1.x);
+            R.acc[w][r] = fmaf(f1, hi, fmaf(g1, lo, R.acc[w][r]));
+        }
+    }
+}
+
+// The same from the slab copy in global memory (a slice whose box did not fit).
+__device__ __forceinline__ void sample_global(const SlabLaunch &L, int s, float sf, Rays &R)
+{
+#pragma unroll
+    for (int w = 0; w < SLAB_W; ++w) {
+        const float q1 = fmaf(R.A1[w], sf, R.B1h[w]);
+        const float t1 = __fadd_rd(q1, SPLIT_M);
+        const float f1 = q1 - (t1 - SPLIT_M);
+        const int k1 = min(max(__float_as_int(t1) - SPLIT_BITS, -2), L.n1);
+        const float2 *row = L.copy + ((long long)s * L.py + k1 + 2) * L.pz + 2;
+#pragma unroll
+        for (int r = 0; r < SLAB_R; ++r) {
+            const float q2 = fmaf(R.A2[w][r], sf, R.B2h[w][r]);
+            const float t2 = __fadd_rd(q2, SPLIT_M);
+            const float f2 = q2 - (t2 - SPLIT_M);
+            const int k2 = min(max(__float_as_int(t2) - SPLIT_BITS, -2), L.n2);
+            const float2 p0 = __ldg(row + k2), p1 = __ldg(row + L.pz + k2);
+            const float lo = fmaf(f2, p0.y, p0.x), hi = fmaf(f2, p1.y, p1.x);
+            R.acc[w][r] = fmaf(f1, hi - lo, R.acc[w][r] + lo);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(SLAB_THREADS, 2) fp3d_slab_kernel(const __grid_constant__ SlabLaunch L)
+{
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    float2 *buf = reinterpret_cast<float2 *>(smraw);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smraw + (size_t)SLAB_STAGES * SLAB_SLOT * sizeof(float2));
+    uint64_t *empty = full + SLAB_STAGES;
+    SlabInfo *info = reinterpret_cast<SlabInfo *>(empty + SLAB_STAGES);
+    int *range = reinterpret_cast<int *>(info + SLAB_STAGES);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (int k = 0; k < SLAB_STAGES; ++k) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], SLAB_WARPS);
+        }
+        range[0] = 0x7fffffff;
+        range[1] = -0x7fffffff;
+        mbar_fence_init();
+        tma_prefetch_map(&L.tmap[0]);
+        tma_prefetch_map(&L.tmap[1]);
+    }
+    __syncthreads();
+
+    // ---- ray set-up (compute warps): column `warp`, both views, SLAB_R rows per lane
+    const int u_raw = (int)blockIdx.y * SLAB_U + warp;
+    Rays R;
+    int wlo = 1, whi = 0, ilo = 1, ihi = 0;  // union and intersection of the warp's ray ranges
+    if (warp < SLAB_WARPS) {
+        const float uu = det_uu(L, u_raw);
+        int lo_u = 0x7fffffff, hi_u = -0x7fffffff, lo_i = -0x7fffffff, hi_i = 0x7fffffff;
+#pragma unroll
+        for (int w = 0; w < SLAB_W; ++w) {
+            const FPView &V = L.views[min((int)blockIdx.x * SLAB_W + w, L.nviews - 1)];
+#pragma unroll
+            for (int r = 0; r < SLAB_R; ++r) {
+                const int v = (int)blockIdx.z * SLAB_ROWS + lane + 32 * r;
+                float a1, b1;
+                ray_setup(V, uu, det_vv(L, v), a1, b1, R.A2[w][r], R.B2h[w][r]);
+                // the same for every row: a column's rays share the in-plane position
+                R.A1[w] = a1;
+                R.B1h[w] = b1;
+                R.acc[w][r] = 0.0f;
+                int lo = 0, hi = L.n0 - 1;
+                clip_axis(a1, b1, L.n1, L.n0, lo, hi);
+                clip_axis(R.A2[w][r], R.B2h[w][r], L.n2, L.n0, lo, hi);
+                if (lo <= hi) {
+                    lo_u = min(lo_u, lo);
+                    hi_u = max(hi_u, hi);
+                }
+                lo_i = max(lo_i, lo);
+                hi_i = min(hi_i, hi);
+            }
+        }
+        wlo = warp_min(lo_u);
+        whi = warp_max(hi_u);
+        ilo = warp_max(lo_i);
+        ihi = warp_min(hi_i);
+        if (lane == 0 && wlo <= whi) {
+            atomicMin(&range[0], wlo);
+            atomicMax(&range[1], whi);
+        }
+    }
+    __syncthreads();
+    const int s_lo = range[0], s_hi = range[1];
+
+    if (warp == SLAB_WARPS) {
+        if (s_lo <= s_hi) slab_produce(L, buf, full, empty, info, lane, s_lo, s_hi);
+        return;
+    }
+
+    // ---- compute warps
+    const uint32_t sbase = smem_u32(buf);
+    bool ok = true;
+    for (int s = s_lo; s <= s_hi; ++s) {
+        const int st = s - s_lo;
+        const int slot = st % SLAB_STAGES;
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[slot], (uint32_t)((st / SLAB_STAGES) & 1), SLAB_WAIT))) {
+            if (lane == 0) atomicOr(&g_fp_slab_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
+            ok = false;
+            break;
+        }
+        if (s >= wlo && s <= whi) {
+            const SlabInfo I = info[slot];
+            const float sf = (float)s;
+            const uint32_t rb = sbase + (uint32_t)slot * (SLAB_SLOT * 8u) + (uint32_t)I.rbase;
+            const bool fast = s >= ilo && s <= ihi;
+            if (I.sel == 0) {
+                if (fast) sample_smem<SLAB_WA, false>(L, rb, sf, R);
+                else sample_smem<SLAB_WA, true>(L, rb, sf, R);
+            } else if (I.sel == 1) {
+                if (fast) sample_smem<SLAB_WB, false>(L, rb, sf, R);
+                else sample_smem<SLAB_WB, true>(L, rb, sf, R);
+            } else {
+                sample_global(L, s, sf, R);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[slot]);
+    }
+    if (!ok || u_raw >= L.nu) return;
+    // ---- results
+#pragma unroll
+    for (int w = 0; w < SLAB_W; ++w) {
+        const int vi = (int)blockIdx.x * SLAB_W + w;
+        if (vi >= L.nviews) break;
+        const int a = L.views[vi].a;
+#pragma unroll
+        for (int r = 0; r < SLAB_R; ++r) {
+            const int v = (int)blockIdx.z * SLAB_ROWS + lane + 32 * r;
+            if (v >= L.nv) continue;
+            const float sc =
+                sqrtf(fmaf(R.A1[w] * R.A1[w], L.f1, fmaf(R.A2[w][r] * R.A2[w][r], L.f2, 1.0f))) * L.mul;
+            float *out = static_cast<float *>(L.proj) + ((size_t)v * L.na + a) * L.proj_pitch + u_raw;
+            float val = fmaf(R.acc[w][r], sc, 0.0f);
+            if (L.accumulate) val += *out;
+            *out = val;
+        }
+    }
+}
+
+// Slab copy of marching axis dir (0: slices along x, in-plane axis y; 1:
+// slices along y, in-plane axis x) as z-pairs: texel (s, k1, k2) holds
+// (v[k2], v[k2 + 1] - v[k2]) at (s * py + k1 + 2) * pz + k2 + 2, written for
+// k1 in [0, n1) and k2 in [-1, n2 - 1] (the pair below the volume carries
+// v[0] as its difference); everything else stays zero from a memset.  A CTA
+// transposes a (z, x) tile of one y plane through shared memory.
+__global__ void __launch_bounds__(256) build_slab_copy(const float *__restrict__ vol, size_t pitch, int nx, int ny,
+                                                       int nz, int dir, long long py, long long pz,
+                                                       float2 *__restrict__ out)
+{
+    __shared__ float t[34][33];  // t[i][xi] = v(z0 - 1 + i, y, x0 + xi), zero outside the volume
+    const int z0 = blockIdx.x * 32, x0 = blockIdx.y * 32, y = blockIdx.z;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int i = ty; i < 34; i += 8) {
+        const int z = z0 - 1 + i, x = x0 + tx;
+        t[i][tx] = (z >= 0 && z < nz && x < nx) ? __ldg(vol + ((size_t)z * ny + y) * pitch + x) : 0.0f;
+    }
+    __syncthreads();
+    for (int xi = ty; xi < 32; xi += 8) {
+        const int x = x0 + xi;
+        if (x >= nx) continue;
+        const long long s = (dir == 0) ? x : y, k1 = (dir == 0) ? y : x;
+        float2 *row = out + (s * py + k1 + 2) * pz + 2;
+        const int z = z0 + tx;
+        if (z < nz) row[z] = make_float2(t[tx + 1][xi], t[tx + 2][xi] - t[tx + 1][xi]);
+        if (z0 == 0 && tx == 0) row[-1] = make_float2(0.0f, t[1][xi]);
+    }
+}
+
+bool slab_enabled()
+{
+    const char *e = std::getenv("B2T_FP_PATH");
+    return !(e && e[0] == 'c');  // B2T_FP_PATH=cells keeps the cell kernels for every view
+}
+
+long long slab_pz(const b2t_dims3d &d) { return ((long long)d.vol_z + 4 + 1) & ~1ll; }
+
+}  // namespace
+
+static std::atomic<unsigned long long> g_slab_launches{0};
+
+b2t_status fp_path_stats_impl(uint64_t *stats)
+{
+    unsigned long long v[2] = {0, 0};
+    B2T_CUDA_TRY(cudaMemcpyFromSymbol(v, g_fp_slab_slices, sizeof(v)), "read FP path statistics");
+    const unsigned long long zero[2] = {0, 0};
+    B2T_CUDA_TRY(cudaMemcpyToSymbol(g_fp_slab_slices, zero, sizeof(zero)), "clear FP path statistics");
+    stats[0] = v[0];
+    stats[1] = v[1];
+    stats[2] = g_slab_launches.exchange(0);
+    stats[3] = fp_cell_launches_take();
+    return B2T_OK;
+}
+
+b2t_status fp_slab_errors(uint32_t *flags)
+{
+    unsigned int v = 0;
+    B2T_CUDA_TRY(cudaMemcpyFromSymbol(&v, g_fp_slab_errors, sizeof(v)), "read FP error word");
+    const unsigned int zero = 0;
+    B2T_CUDA_TRY(cudaMemcpyToSymbol(g_fp_slab_errors, &zero, sizeof(zero)), "clear FP error word");
+    *flags = v;
+    return B2T_OK;
+}
+
+bool fp_slab_eligible(const b2t_geom3d *g, const b2t_params3d *p, int32_t dtype, int dir, const std::vector<int> &dirs)
+{
+    if (!slab_enabled() || dtype != B2T_F32 || dir > 1 || p->det_supersample != 1) return false;
+    const b2t_dims3d &d = g->dims;
+    for (uint32_t a = 0; a < d.angles; ++a) {
+        if (dirs[a] != dir) continue;
+        FPView w;
+        fp_view_coeffs(g->kind, g->views[a], d, dir, w);
+        if (w.e[2] != 0.0f || w.m1[2] != 0.0f || w.n1[2] != 0.0f) return false;
+    }
+    return true;
+}
+
+size_t fp_slab_copy_bytes(const b2t_dims3d &d, int dir)
+{
+    const size_t n0 = dir == 0 ? d.vol_x : d.vol_y, n1 = dir == 0 ? d.vol_y : d.vol_x;
+    return n0 * (n1 + 4) * (size_t)slab_pz(d) * sizeof(float2);
+}
+
+b2t_status fp_slab_build(const b2t_dims3d &d, const float *vol, size_t vol_pitch, int dir, void *copy,
+                         cudaStream_t s)
+{
+    const long long n1 = dir == 0 ? d.vol_y : d.vol_x;
+    B2T_CUDA_TRY(cudaMemsetAsync(copy, 0, fp_slab_copy_bytes(d, dir), s), "slab copy clear");
+    dim3 grid((d.vol_z + 31) / 32, (d.vol_x + 31) / 32, d.vol_y);
+    build_slab_copy<<<grid, 256, 0, s>>>(vol, vol_pitch, d.vol_x, d.vol_y, d.vol_z, dir, n1 + 4, slab_pz(d),
+                                         static_cast<float2 *>(copy));
+    count_launches(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "slab copy launch");
+    return B2T_OK;
+}
+
+b2t_status fp_slab_project(const b2t_geom3d *g, const b2t_params3d *p, const void *copy, int dir, void *proj,
+                           size_t proj_pitch, int32_t mode, const std::vector<int> &dirs, cudaStream_t s)
+{
+    const b2t_dims3d &d = g->dims;
+    SlabLaunch *Lp = new SlabLaunch;
+    SlabLaunch &L = *Lp;
+    L.n0 = dir == 0 ? d.vol_x : d.vol_y;
+    L.n1 = dir == 0 ? d.vol_y : d.vol_x;
+    L.n2 = d.vol_z;
+    L.py = L.n1 + 4;
+    L.pz = slab_pz(d);
+    L.copy = static_cast<const float2 *>(copy);
+    // 8-byte elements (the z-pairs, copied bit for bit); zero fill outside
+    const uint64_t dims[3] = {(uint64_t)L.n2 + 4, (uint64_t)L.py, (uint64_t)L.n0};
+    const uint64_t strides[2] = {(uint64_t)L.pz * sizeof(float2), (uint64_t)(L.pz * L.py) * sizeof(float2)};
+    b2t_status st = B2T_OK;
+    for (int k = 0; k < 2 && st == B2T_OK; ++k) {
+        const uint32_t box[3] = {(uint32_t)(k == 0 ? SLAB_WA : SLAB_WB), SLAB_BOX_Y, 1};
+        st = encode_tensor_map(&L.tmap[k], CU_TENSOR_MAP_DATA_TYPE_INT64, 3, copy, dims, strides, box);
+    }
+    if (st != B2T_OK) {
+        delete Lp;
+        return st;
+    }
+    L.proj = proj;
+    L.proj_pitch = (long long)proj_pitch;
+    L.nu = d.det_u;
+    L.nv = d.det_v;
+    L.na = d.angles;
+    L.accumulate = (mode == B2T_MODE_ADD) ? 1 : 0;
+    fp_scale(g->kind, dir, g->vol_scale, false, p->output_scale, L.f1, L.f2, L.mul);
+    std::vector<int> views;
+    for (uint32_t a = 0; a < d.angles; ++a)
+        if (dirs[a] == dir) views.push_back((int)a);
+    const size_t smem = (size_t)SLAB_STAGES * SLAB_SLOT * sizeof(float2) +
+                        SLAB_STAGES * (2 * sizeof(uint64_t) + sizeof(SlabInfo)) + 2 * sizeof(int);
+    static bool attr_set = false;
+    if (!attr_set) {
+        B2T_CUDA_TRY(cudaFuncSetAttribute(fp3d_slab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                     "slab FP shared memory attribute");
+        attr_set = true;
+    }
+    for (size_t c0 = 0; c0 < views.size() && st == B2T_OK; c0 += SLAB_MAX_VIEWS) {
+        const size_t cn = std::min(views.size() - c0, (size_t)SLAB_MAX_VIEWS);
+        L.nviews = (int)cn;
+        for (size_t i = 0; i < cn; ++i) {
+            fp_view_coeffs(g->kind, g->views[views[c0 + i]], d, dir, L.views[i]);
+            L.views[i].a = views[c0 + i];
+        }
+        dim3 grid((unsigned)((cn + SLAB_W - 1) / SLAB_W), (d.det_u + SLAB_U - 1) / SLAB_U,
+                  (d.det_v + SLAB_ROWS - 1) / SLAB_ROWS);
+        fp3d_slab_kernel<<<grid, SLAB_THREADS, smem, s>>>(L);
+        count_launches(1);
+        g_slab_launches.fetch_add(1);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(e, "fp3d_slab_kernel launch");
+    }
+    delete Lp;
+    return st;
+}
+
+}  // namespace b2t

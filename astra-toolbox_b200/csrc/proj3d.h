@@ -124,12 +124,29 @@ struct FPCells {
     std::unique_ptr<Scratch> mem[3];
     const void *base[3] = {nullptr, nullptr, nullptr};  // cell of texels (0, 0), slice 0, per marching axis
     long long st0[3] = {0, 0, 0}, st1[3] = {0, 0, 0}, st2[3] = {0, 0, 0};
+    // marching axes held as a slab copy for the TMA-staged kernel
+    // (fp3d_slab.cu) instead of cells; base[] then points at the copy
+    bool slab[3] = {false, false, false};
     int32_t dtype = B2T_F32;
     uint32_t vol_x = 0, vol_y = 0, vol_z = 0;
 };
-// Builds the cells of the marching axes marked in need[] (x, y, z).
-b2t_status fp3d_cells_build(const b2t_geom3d *g, const void *vol, size_t vol_pitch, int32_t dtype, const bool need[3],
-                            cudaStream_t s, FPCells &c);
+// Builds the cells (or slab copies) of the marching axes marked in need[]
+// (x, y, z) for the views of g projected with parameters p.
+b2t_status fp3d_cells_build(const b2t_geom3d *g, const b2t_params3d *p, const void *vol, size_t vol_pitch,
+                            int32_t dtype, const bool need[3], cudaStream_t s, FPCells &c);
+
+// TMA-staged slab forward projector (fp3d_slab.cu) for x- and y-major views
+// whose rays share the in-plane position along a detector column: FP32,
+// no detector supersampling.
+bool fp_slab_eligible(const b2t_geom3d *g, const b2t_params3d *p, int32_t dtype, int dir, const std::vector<int> &dirs);
+size_t fp_slab_copy_bytes(const b2t_dims3d &d, int dir);
+b2t_status fp_slab_build(const b2t_dims3d &d, const float *vol, size_t vol_pitch, int dir, void *copy,
+                         cudaStream_t s);
+b2t_status fp_slab_project(const b2t_geom3d *g, const b2t_params3d *p, const void *copy, int dir, void *proj,
+                           size_t proj_pitch, int32_t mode, const std::vector<int> &dirs, cudaStream_t s);
+b2t_status fp_slab_errors(uint32_t *flags);
+b2t_status fp_path_stats_impl(uint64_t *stats);
+unsigned long long fp_cell_launches_take();
 // proj (=|+=) FP of the volume the cells hold, for the views of g (same
 // volume dimensions as at build time; every view's marching axis built).
 b2t_status fp3d_cells_project(const b2t_geom3d *g, const b2t_params3d *p, const FPCells &c, void *proj,

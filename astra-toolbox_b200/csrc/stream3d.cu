@@ -257,7 +257,7 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
         bool need[3] = {false, false, false};
         for (uint32_t a = 0; a < d.angles; ++a) need[dominant_axis(G.kind, G.views[a], d)] = true;
         B2T_CUDA_TRY(cudaStreamWaitEvent(cs.s, in_ready[0].e, 0), "wait");
-        const b2t_status bs = fp3d_cells_build(&G, inb[0].f(), 0, B2T_F32, need, cs.s, cells);
+        const b2t_status bs = fp3d_cells_build(&G, &R.params, inb[0].f(), 0, B2T_F32, need, cs.s, cells);
         if (bs == B2T_OK) have_cells = true;
         else if (bs == B2T_ERR_NO_MEMORY) clear_error();  // project block by block instead
         else return bs;

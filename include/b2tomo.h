@@ -75,6 +75,14 @@ b2t_status b2t_device_errors(uint32_t *flags);
  * warps.  Synchronises the device.  A performance diagnostic; the reference
  * has no counterpart. */
 b2t_status b2t_bp_path_stats(uint64_t stats[4]);
+/* Read and clear the path statistics of the cone/parallel forward projection
+ * since the last call: stats[0] slices that CTAs of the TMA-staged slab
+ * kernel read from shared memory, stats[1] slices they read from the slab
+ * copy in global memory (a box too large for a slice buffer), stats[2] slab
+ * kernel launches, stats[3] cell kernel launches (views the slab kernel does
+ * not take).  Synchronises the device.  A performance diagnostic; the
+ * reference has no counterpart. */
+b2t_status b2t_fp_path_stats(uint64_t stats[4]);
 
 /* Failure-handling test hooks; the reference has no counterpart.
  * b2t_debug_fail_alloc(n), n >= 1: the n-th device allocation the library

@@ -334,6 +334,75 @@ def test_cell_fp_matches_padded_fp(astra, idx, dtype, monkeypatch):
     assert rel_l2(a.float().cpu().numpy(), b.float().cpu().numpy()) < tol, name
 
 
+def _fp_stats():
+    import importlib
+    L = importlib.import_module("astra-toolbox_b200._lib")
+    out = (ctypes.c_uint64 * 4)()
+    assert L.load().b2t_fp_path_stats(out) == 0
+    return list(out)
+
+
+def _slab_cases(astra):
+    ang = np.linspace(0, 2 * np.pi, 30, endpoint=False).astype(np.float32)
+    near45 = np.linspace(np.pi / 4 - 0.2, np.pi / 4 + 0.2, 21).astype(np.float32)
+    return {
+        # staged slices, rays leaving through every face (clamped slices)
+        "cone": (astra.create_vol_geom(40, 44, 36), astra.create_proj_geom('cone', 1.0, 1.0, 48, 56, ang, 150.0, 80.0)),
+        "parallel3d": (astra.create_vol_geom(36, 40, 32),
+                       astra.create_proj_geom('parallel3d', 1.0, 1.0, 40, 48, ang[:24] / 2)),
+        # oblique views: x- and y-major views around 45 degrees, edge rays
+        # far outside the volume
+        "oblique": (astra.create_vol_geom(48, 40, 30), astra.create_proj_geom('cone', 1.0, 1.0, 40, 96, near45, 90.0, 60.0)),
+        # boxes larger than a slice buffer: read from global memory
+        "high_mag": (astra.create_vol_geom(40, 40, 40), astra.create_proj_geom('cone', 4.0, 4.0, 36, 20, ang, 60.0, 60.0)),
+        # more views than one launch takes, a detector taller than one CTA
+        "many_views": (astra.create_vol_geom(20, 18, 24),
+                       astra.create_proj_geom('cone', 1.0, 1.0, 150, 22, np.linspace(0, 2 * np.pi, 500, False).astype(np.float32), 80.0, 40.0)),
+        # odd sizes, anisotropic voxels
+        "odd": (astra.create_vol_geom(17, 23, 9, -9.0, 8.0, -11.0, 12.0, -3.0, 3.0),
+                astra.create_proj_geom('cone', 0.7, 1.3, 13, 21, ang + 0.1, 70.0, 30.0)),
+    }
+
+
+@pytest.mark.parametrize("case", ["cone", "parallel3d", "oblique", "high_mag", "many_views", "odd"])
+def test_slab_fp_vs_oracle_and_cells(astra, orc, case, monkeypatch):
+    """The TMA-staged slab FP (the default for x- and y-major views of
+    circular orbits) against the FP64 oracle and against the cell kernels:
+    slices staged in shared memory, slices where rays leave the volume
+    (clamped to the zero border), slices whose box is too large for a buffer
+    (read from global memory), ADD mode, more than one launch of views."""
+    vg, pg = _slab_cases(astra)[case]
+    pr = _proj(astra, vg, pg)
+    vol = _phantom(pr.vol_shape, 31)
+    tv = torch.from_numpy(vol).cuda()
+    _fp_stats()
+    a = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(tv, a)
+    staged, glob, slab_launches, cell_launches = _fp_stats()
+    assert slab_launches >= 1 and cell_launches == 0, (case, slab_launches, cell_launches)
+    if case == "high_mag":
+        assert glob > 0
+    else:
+        assert staged > 0, (staged, glob)
+    nv, na, nu = pr.proj_shape
+    ref = orc.fp3d(pr.geom.kind, pr.geom.views_array(), vol, nu, nv, pr.geom.vol_scale)
+    assert rel_l2(a.cpu().numpy(), ref) < TOL_F32, case
+    monkeypatch.setenv("B2T_FP_PATH", "cells")
+    b = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(tv, b)
+    assert _fp_stats()[2] == 0
+    monkeypatch.delenv("B2T_FP_PATH")
+    assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 2e-6, case
+    # ADD mode accumulates onto what is there
+    c = b.clone()
+    pr.fp(tv, c, mode=0)
+    assert rel_l2(c.cpu().numpy(), 2 * b.cpu().numpy()) < 2e-6
+    flags = ctypes.c_uint32(1)
+    import importlib
+    assert importlib.import_module("astra-toolbox_b200._lib").load().b2t_device_errors(ctypes.byref(flags)) == 0
+    assert flags.value == 0
+
+
 @pytest.mark.parametrize("idx", [0, 4])
 def test_autotune_fp3d_keeps_results(astra, orc, idx):
     """The autotuner times the views-per-CTA variants and keeps the fastest;
