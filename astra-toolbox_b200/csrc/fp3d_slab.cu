@@ -296,10 +296,11 @@ struct Rays {
     float acc[SLAB_W][SLAB_R];
 };
 
-// One slice of the lane's rays from a shared-memory buffer of row pitch P
-// (z-pairs).  CLAMP: texels clamped to the zero border (slices where a ray of
-// the warp is outside the volume).  rb = the slot's byte address + rbase.
-template <int P, bool CLAMP>
+// One slice of the lane's rays (rows r < RE of each view) from a
+// shared-memory buffer of row pitch P (z-pairs).  CLAMP: texels clamped to
+// the zero border (slices where a ray of the warp is outside the volume).
+// rb = the slot's byte address + rbase.
+template <int P, bool CLAMP, int RE>
 __device__ __forceinline__ void sample_smem(const SlabLaunch &L, uint32_t rb, float sf, Rays &R)
 {
     constexpr uint32_t ROWB = 8u * P;
@@ -313,7 +314,7 @@ __device__ __forceinline__ void sample_smem(const SlabLaunch &L, uint32_t rb, fl
         if (CLAMP) b1 = min(max(b1, SPLIT_BITS - 2), SPLIT_BITS + L.n1);
         const uint32_t row = (uint32_t)b1 * ROWB + rb;
 #pragma unroll
-        for (int r = 0; r < SLAB_R; ++r) {
+        for (int r = 0; r < RE; ++r) {
             const float q2 = fmaf(R.A2[w][r], sf, R.B2h[w][r]);
             const float t2 = __fadd_rd(q2, SPLIT_M);
             const float f2 = q2 - (t2 - SPLIT_M);
@@ -330,6 +331,7 @@ __device__ __forceinline__ void sample_smem(const SlabLaunch &L, uint32_t rb, fl
 }
 
 // The same from the slab copy in global memory (a slice whose box did not fit).
+template <int RE>
 __device__ __forceinline__ void sample_global(const SlabLaunch &L, int s, float sf, Rays &R)
 {
 #pragma unroll
@@ -340,7 +342,7 @@ __device__ __forceinline__ void sample_global(const SlabLaunch &L, int s, float 
         const int k1 = min(max(__float_as_int(t1) - SPLIT_BITS, -2), L.n1);
         const float2 *row = L.copy + ((long long)s * L.py + k1 + 2) * L.pz + 2;
 #pragma unroll
-        for (int r = 0; r < SLAB_R; ++r) {
+        for (int r = 0; r < RE; ++r) {
             const float q2 = fmaf(R.A2[w][r], sf, R.B2h[w][r]);
             const float t2 = __fadd_rd(q2, SPLIT_M);
             const float f2 = q2 - (t2 - SPLIT_M);
@@ -350,6 +352,51 @@ __device__ __forceinline__ void sample_global(const SlabLaunch &L, int s, float 
             R.acc[w][r] = fmaf(f1, hi - lo, R.acc[w][r] + lo);
         }
     }
+}
+
+// The CTA's slice range [s_lo, s_hi] and the warp's union [wlo, whi] and
+// intersection [ilo, ihi] of its rays' ranges.
+struct Range {
+    int s_lo, s_hi, wlo, whi, ilo, ihi;
+};
+
+// A compute warp's pass over the CTA's slices (rows r < RE of each view):
+// wait for the slice's buffer, sample, release it.  False when a wait gave up.
+template <int RE>
+__device__ __forceinline__ bool slab_consume(const SlabLaunch &L, const float2 *buf, uint64_t *full, uint64_t *empty,
+                                             const SlabInfo *info, int lane, const Range &rg, Rays &R)
+{
+    const uint32_t sbase = smem_u32(buf);
+    int slot = 0;
+    uint32_t par = 0;
+    float sf = (float)rg.s_lo;
+    for (int s = rg.s_lo; s <= rg.s_hi; ++s, sf += 1.0f) {
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[slot], par, SLAB_WAIT))) {
+            if (lane == 0) atomicOr(&g_fp_slab_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
+            return false;
+        }
+        if (s >= rg.wlo && s <= rg.whi) {
+            const SlabInfo I = info[slot];
+            const uint32_t rb = sbase + (uint32_t)slot * (SLAB_SLOT * 8u) + (uint32_t)I.rbase;
+            const bool fast = s >= rg.ilo && s <= rg.ihi;
+            if (I.sel == 0) {
+                if (fast) sample_smem<SLAB_WA, false, RE>(L, rb, sf, R);
+                else sample_smem<SLAB_WA, true, RE>(L, rb, sf, R);
+            } else if (I.sel == 1) {
+                if (fast) sample_smem<SLAB_WB, false, RE>(L, rb, sf, R);
+                else sample_smem<SLAB_WB, true, RE>(L, rb, sf, R);
+            } else {
+                sample_global<RE>(L, s, sf, R);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[slot]);
+        if (++slot == SLAB_STAGES) {
+            slot = 0;
+            par ^= 1u;
+        }
+    }
+    return true;
 }
 
 __global__ void __launch_bounds__(SLAB_THREADS, 2) fp3d_slab_kernel(const __grid_constant__ SlabLaunch L)
@@ -423,35 +470,15 @@ __global__ void __launch_bounds__(SLAB_THREADS, 2) fp3d_slab_kernel(const __grid
         return;
     }
 
-    // ---- compute warps
-    const uint32_t sbase = smem_u32(buf);
-    bool ok = true;
-    for (int s = s_lo; s <= s_hi; ++s) {
-        const int st = s - s_lo;
-        const int slot = st % SLAB_STAGES;
-        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[slot], (uint32_t)((st / SLAB_STAGES) & 1), SLAB_WAIT))) {
-            if (lane == 0) atomicOr(&g_fp_slab_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
-            ok = false;
-            break;
-        }
-        if (s >= wlo && s <= whi) {
-            const SlabInfo I = info[slot];
-            const float sf = (float)s;
-            const uint32_t rb = sbase + (uint32_t)slot * (SLAB_SLOT * 8u) + (uint32_t)I.rbase;
-            const bool fast = s >= ilo && s <= ihi;
-            if (I.sel == 0) {
-                if (fast) sample_smem<SLAB_WA, false>(L, rb, sf, R);
-                else sample_smem<SLAB_WA, true>(L, rb, sf, R);
-            } else if (I.sel == 1) {
-                if (fast) sample_smem<SLAB_WB, false>(L, rb, sf, R);
-                else sample_smem<SLAB_WB, true>(L, rb, sf, R);
-            } else {
-                sample_global(L, s, sf, R);
-            }
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[slot]);
-    }
+    // ---- compute warps: the rows in use (the last row block of the
+    // detector may hold fewer than SLAB_ROWS)
+    const int re = min(SLAB_R, (L.nv - (int)blockIdx.z * SLAB_ROWS + 31) >> 5);
+    const Range rg{s_lo, s_hi, wlo, whi, ilo, ihi};
+    bool ok;
+    if (re >= 4) ok = slab_consume<4>(L, buf, full, empty, info, lane, rg, R);
+    else if (re == 3) ok = slab_consume<3>(L, buf, full, empty, info, lane, rg, R);
+    else if (re == 2) ok = slab_consume<2>(L, buf, full, empty, info, lane, rg, R);
+    else ok = slab_consume<1>(L, buf, full, empty, info, lane, rg, R);
     if (!ok || u_raw >= L.nu) return;
     // ---- results
 #pragma unroll
