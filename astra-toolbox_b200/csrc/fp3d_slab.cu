@@ -339,6 +339,7 @@ __device__ __forceinline__ void sample_global(const SlabLaunch &L, int s, float 
         const float q1 = fmaf(R.A1[w], sf, R.B1h[w]);
         const float t1 = __fadd_rd(q1, SPLIT_M);
         const float f1 = q1 - (t1 - SPLIT_M);
+        const float g1 = 1.0f - f1;
         const int k1 = min(max(__float_as_int(t1) - SPLIT_BITS, -2), L.n1);
         const float2 *row = L.copy + ((long long)s * L.py + k1 + 2) * L.pz + 2;
 #pragma unroll
@@ -348,8 +349,10 @@ __device__ __forceinline__ void sample_global(const SlabLaunch &L, int s, float 
             const float f2 = q2 - (t2 - SPLIT_M);
             const int k2 = min(max(__float_as_int(t2) - SPLIT_BITS, -2), L.n2);
             const float2 p0 = __ldg(row + k2), p1 = __ldg(row + L.pz + k2);
+            // the arithmetic of sample_smem, so that a ray's sum does not
+            // depend on where its slices were read from
             const float lo = fmaf(f2, p0.y, p0.x), hi = fmaf(f2, p1.y, p1.x);
-            R.acc[w][r] = fmaf(f1, hi - lo, R.acc[w][r] + lo);
+            R.acc[w][r] = fmaf(f1, hi, fmaf(g1, lo, R.acc[w][r]));
         }
     }
 }

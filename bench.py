@@ -403,6 +403,384 @@ def run_batch2d(args):
     return 0
 
 
+def c1_phantom(n=256, seed=0):
+    """The C1 phantom: 10 seeded random ellipses (centres in the inner 80 %,
+    semi-axes 10-80 px, random rotation, additive intensities in [0, 1])."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    y, x = np.mgrid[0:n, 0:n] + 0.5 - n / 2
+    img = np.zeros((n, n), dtype=np.float64)
+    for _ in range(10):
+        cx, cy = rng.uniform(-0.4, 0.4, 2) * n
+        a, b = rng.uniform(10 * n / 256, 80 * n / 256, 2)
+        t = rng.uniform(0, np.pi)
+        xr = (x - cx) * np.cos(t) + (y - cy) * np.sin(t)
+        yr = -(x - cx) * np.sin(t) + (y - cy) * np.cos(t)
+        img[(xr / a) ** 2 + (yr / b) ** 2 <= 1] += rng.uniform(0, 1)
+    return img.astype(np.float32)
+
+
+def _c1_cpu_worker(core, kernel, iterations, sino, angles):
+    """One host process of the C1 CPU baseline: the reference's CPU SIRT
+    (its CPU-only build) pinned to one core; returns seconds."""
+    import os as _os
+    import time as _time
+    try:
+        _os.sched_setaffinity(0, {core})
+    except (AttributeError, OSError):
+        pass
+    from oracle import ref as _ref
+    t0 = _time.perf_counter()
+    _ref.cpu_sirt2d('parallel', kernel, sino, (256, 256), angles, iterations)
+    return _time.perf_counter() - t0
+
+
+def run_c1(args):
+    """--workload c1: 2D parallel beam, 256^2 volume of 10 seeded ellipses,
+    180 views over pi, 384 detectors of width 1.  GPU: one step = FP + BP
+    through Projector2D (metric GUPS = 2 x 256^2 x 180 / step time); SIRT_CUDA
+    100 iterations from zero on the exact sinogram (CUDA-graph iterations).
+    Beside it the reference's own CPU path (its CPU-only build,
+    oracle/_ref/libastra_ref_cpu.so): line and linear FP and BP, SIRT with the
+    line projector on one pinned core, and the aggregate over all host cores as
+    independent processes, one per core."""
+    import torch
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    from oracle import ref
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    astra = importlib.import_module("astra-toolbox_b200")
+    A = importlib.import_module("astra-toolbox_b200.algorithm")
+    D2 = importlib.import_module("astra-toolbox_b200.data2d")
+    lib = importlib.import_module("astra-toolbox_b200._lib").load()
+    lib.b2t_kernel_launches.restype = ctypes.c_uint64
+    n, na, nd = 256, 180, 384
+    ang = np.linspace(0, np.pi, na, endpoint=False).astype(np.float32)
+    vg = astra.create_vol_geom(n, n)
+    pg = astra.create_proj_geom('parallel', 1.0, nd, ang)
+    pr = astra.Projector2D(pg, vg)
+    img = c1_phantom(n)
+    x = torch.from_numpy(img).to(dev)
+    sino = torch.zeros(pr.proj_shape, device=dev)
+    back = torch.zeros(pr.vol_shape, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        pr.fp(x, sino)
+        pr.bp(sino, back)
+
+    for _ in range(args.warmup):
+        step()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = lib.b2t_kernel_launches()
+    ms = _timed_region(torch, stream, step, max(args.steps, 50))
+    launches = (lib.b2t_kernel_launches() - l0) / max(args.steps, 50) * args.steps
+    # SIRT 100 on the exact (CUDA) sinogram
+    sid = D2.link('-sino', pg, sino.clone())
+    rid = D2.create('-vol', vg, 0)
+    cfg = A.astra_dict('SIRT_CUDA')
+    cfg['ProjectionDataId'] = sid
+    cfg['ReconstructionDataId'] = rid
+    cfg['option'] = {'UseGraph': True}
+    aid = A.create(cfg)
+    A.run(aid, 100)
+    D2.store(rid, 0)
+    sirt_ms = _timed_region(torch, stream, lambda: (D2.store(rid, 0), A.run(aid, 100)), 3)
+    rec_gpu = D2.get(rid)
+    A.delete(aid)
+    D2.delete([sid, rid])
+    clocks = sampler.stop()
+    ups = 2.0 * n * n * na
+    extra = {"fp_bp_ms": ms, "sirt100_s": sirt_ms * 1e-3}
+    cpu = None
+    parity = None
+    if ref.cpu_available() and not args.no_cpu:
+        t0 = time.perf_counter()
+        s_line = ref.cpu_fp2d('parallel', 'line', img, ang, nd)
+        t_fp_line = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ref.cpu_bp2d('parallel', 'line', s_line, (n, n), ang)
+        t_bp_line = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        s_lin = ref.cpu_fp2d('parallel', 'linear', img, ang, nd)
+        t_fp_lin = time.perf_counter() - t0
+        sino_np = sino.cpu().numpy()
+        # SIRT: a bounded number of iterations per process, pinned
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        k1, kn = 20, 10
+        with ctx.Pool(1) as pool:
+            t_one = pool.apply(_c1_cpu_worker, (0, 'line', k1, sino_np, ang))
+        cores = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else list(range(os.cpu_count() or 1))
+        with ctx.Pool(len(cores)) as pool:
+            ts = pool.starmap(_c1_cpu_worker, [(c, 'line', kn, sino_np, ang) for c in cores])
+        it_per_s_all = sum(kn / t for t in ts)
+        cpu = {"value": ups / (t_fp_line + t_bp_line) / 1e9, "unit": "GUPS", "cores": 1, "kind": "reference",
+               "sample": "the reference's CPU 'line' projector (its CPU-only build), one FP + one BP of this "
+                         "workload on one core",
+               "fp_line_ms": t_fp_line * 1e3, "bp_line_ms": t_bp_line * 1e3, "fp_linear_ms": t_fp_lin * 1e3,
+               "sirt100_line_s_one_core": t_one * 100 / k1,
+               "sirt100_per_s_all_cores": it_per_s_all / 100, "all_cores": len(cores),
+               "sirt_sample": "SIRT (line projector) of %d iterations on core 0 (taskset-style affinity), "
+                              "extrapolated to 100; %d iterations in each of %d independent processes, one per "
+                              "core, aggregate" % (k1, kn, len(cores))}
+        rec_cpu = ref.cpu_sirt2d('parallel', 'linear', s_lin, (n, n), ang, 100)
+
+        def rl2(a, b):
+            return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+        parity = {"fp_vs_reference_cpu_linear": rl2(sino_np, s_lin),
+                  "fp_vs_reference_cpu_line": rl2(sino_np, s_line),
+                  "sirt100_vs_reference_cpu_linear_sirt100": rl2(rec_gpu, rec_cpu),
+                  "tolerances": {"linear": 1e-4, "line": 3e-2, "sirt100": 2e-2}}
+    line = {"metric": "2D parallel FP+BP GUPS at 256^2x180 (C1)", "value": ups / (ms * 1e-3) / 1e9,
+            "unit": "GUPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "2D parallel beam, 256^2 volume of 10 seeded ellipses, 180 views over pi, 384 "
+                                   "detectors; FP+BP per step, SIRT_CUDA 100 iterations", "workload_kind": "c1"},
+            "e2e": None, "gpu_launches": int(launches), "clocks": clocks, "roofline": None, "cpu_baseline": cpu,
+            "parity": parity}
+    line.update(extra)
+    print(json.dumps(line))
+    return 0
+
+
+def ref_algo_fdk(torch, args, proj, rec):
+    """The reference's FDK_CUDA object (oracle/_ref) on a copy of the same
+    projections: seconds for one run (host clock, the call synchronises) and
+    the relative L2 difference from this library's reconstruction."""
+    from oracle import ref
+    if not ref.available():
+        return {"unavailable": "oracle/_ref/libastra_ref.so is not built"}
+    ang = np.linspace(0, 2 * np.pi, args.views, endpoint=False).astype(np.float32)
+    out = torch.zeros_like(rec)
+    ts = []
+    for _ in range(2):
+        p = proj.clone()
+        out.zero_()
+        torch.cuda.synchronize()
+        alg = ref.Algo3D('FDK_CUDA', ang, SOD, ODD, p, out)
+        t0 = time.perf_counter()
+        alg.run(1)
+        ts.append(time.perf_counter() - t0)
+        alg.close()
+    d = float(torch.linalg.vector_norm((rec - out).double()) / torch.linalg.vector_norm(out.double()))
+    return {"what": "reference FDK_CUDA object (src/CudaFDKAlgorithm3D.cpp), same projections, same GPU",
+            "s": ts[-1], "volumes_per_s": 1.0 / ts[-1], "rel_l2_ours_vs_ref": d}
+
+
+def ref_algo_iterative(torch, args, kind, proj, our_run):
+    """Time to a fixed residual.  The reference's SIRT3D_CUDA / CGLS3D_CUDA
+    object runs --ref-iters iterations from zero on the same projections; its
+    relative residual |b - A x| / |b| is the target (the residual the
+    reference reaches at the configuration's iteration count).  our_run(k)
+    runs this library's algorithm k iterations from zero and returns (seconds,
+    relative residual); the smallest k reaching the target is searched and
+    timed.  Both sides host-clocked around synchronising calls."""
+    from oracle import ref
+    if not ref.available():
+        return {"unavailable": "oracle/_ref/libastra_ref.so is not built"}
+    K = args.ref_iters
+    ang = np.linspace(0, 2 * np.pi, args.views, endpoint=False).astype(np.float32)
+    nv, na, nu = proj.shape
+    bnorm = float(torch.linalg.vector_norm(proj.double()))
+
+    def ref_run(k):
+        vol = torch.zeros((args.n, args.n, args.n), device=proj.device)
+        torch.cuda.synchronize()
+        alg = ref.Algo3D(kind, ang, SOD, ODD, proj, vol)
+        t0 = time.perf_counter()
+        alg.run(k)
+        dt = time.perf_counter() - t0
+        res = alg.residual() / bnorm
+        alg.close()
+        return dt, res
+
+    t1, _ = ref_run(1)
+    tK, target = ref_run(K)
+    ref_per_iter = (tK - t1) / (K - 1)
+    # ours: the iteration count at which the residual reaches the target
+    lo, hi = 1, K
+    t_hi, r_hi = our_run(hi)
+    while r_hi > target and hi < 2 * K:
+        lo, hi = hi + 1, min(2 * K, hi + max(1, K // 4))
+        t_hi, r_hi = our_run(hi)
+    while lo < hi:
+        mid = (lo + hi) // 2
+        _, r = our_run(mid)
+        if r <= target:
+            hi = mid
+        else:
+            lo = mid + 1
+    t_ours, r_ours = our_run(hi)
+    return {"what": "reference %s object (src/Cuda%sAlgorithm3D.cpp), same projections, same GPU; it takes "
+                    "host-memory data only, so each run copies the projections in and the volume out"
+                    % (kind, "Sirt" if kind.startswith("SIRT") else "Cgls"),
+            "ref_iterations": K, "ref_s": tK, "ref_s_per_iter": ref_per_iter,
+            "target_relative_residual": target, "ours_iterations_to_target": hi,
+            "ours_relative_residual": r_ours, "ours_s_to_target": t_ours,
+            "time_to_residual_speedup": tK / t_ours if r_ours <= target else None}
+
+
+def c5_vectors(na=1500, cols=1280, rows=1024, sod=1500.0, odd=600.0, seed=0):
+    """The C5 cone_vec geometry: the circular orbit (source-origin 1500,
+    origin-detector 600, 1280 x 1024 pixels of size 1, na views over 2 pi)
+    with every view's detector jittered (seeded): its centre shifted by
+    N(0, 0.5 px) along u and v, and u / v tilted by N(0, 0.1 deg) about the
+    other detector axes."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = np.zeros((na, 12))
+    for i in range(na):
+        t = 2 * np.pi * i / na
+        src = np.array([np.sin(t) * sod, -np.cos(t) * sod, 0.0])
+        det = np.array([-np.sin(t) * odd, np.cos(t) * odd, 0.0])
+        u = np.array([np.cos(t), np.sin(t), 0.0])
+        v = np.array([0.0, 0.0, 1.0])
+        n = np.cross(u, v)
+        a, b = np.deg2rad(rng.normal(0.0, 0.1, 2))
+        u2 = u * np.cos(a) + n * np.sin(a)        # tilt u about v
+        v2 = v * np.cos(b) + n * np.sin(b)        # tilt v about u
+        det = det + rng.normal(0.0, 0.5) * u + rng.normal(0.0, 0.5) * v
+        out[i] = np.concatenate([src, det, u2, v2])
+    return out
+
+
+def run_c5(args):
+    """--workload c5: 1024^3 volume of 20 seeded ellipsoids, cone_vec geometry
+    of 1500 jittered views (c5_vectors), 1280 x 1024 detector.  For FP32,
+    FP16 and BF16 storage: FP and BP times (GUPS), the FP's error against the
+    FP64 oracle on sampled views (on the stored, rounded volume), and 30 CGLS
+    iterations from zero with FP64 inner products -- CGLS3D_CUDA for FP32; for
+    FP16 / BF16 the same recurrences with the iterates stored in the half
+    type, the library's half-storage projectors and b2t_dot_f64 -- with each
+    half-storage result's difference from the FP32 one.  Metric: FP + BP
+    GUPS with FP32 storage."""
+    import torch
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    from oracle import oracle as orc
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    astra = importlib.import_module("astra-toolbox_b200")
+    A = importlib.import_module("astra-toolbox_b200.algorithm")
+    D3 = importlib.import_module("astra-toolbox_b200.data3d")
+    ph = importlib.import_module("astra-toolbox_b200.phantom")
+    L = importlib.import_module("astra-toolbox_b200._lib")
+    lib = L.load()
+    lib.b2t_kernel_launches.restype = ctypes.c_uint64
+    n, na, cols, rows = args.n if args.n != N_VOX else 1024, args.c5_views, 1280, 1024
+    vecs = c5_vectors(na, cols, rows)
+    vg = astra.create_vol_geom(n, n, n)
+    pg = astra.create_proj_geom('cone_vec', rows, cols, vecs)
+    pr = astra.Projector3D(pg, vg)
+    stream = torch.cuda.current_stream(dev)
+    x32 = ph.ellipsoids(pr.vol_shape, 20, seed=0, axes=(0.04 * n, 0.4 * n), device=dev)
+    ups = float(n) ** 3 * na
+    sel = sample_views(na, 2)
+    out = {}
+    b32 = None
+    rec32 = None
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    for name, dt in (("f32", torch.float32), ("f16", torch.float16), ("bf16", torch.bfloat16)):
+        if name not in args.c5_types:
+            continue
+        code = {torch.float32: L.F32, torch.float16: L.F16, torch.bfloat16: L.BF16}[dt]
+        x = x32.to(dt)
+        b = torch.zeros(pr.proj_shape, device=dev, dtype=dt)
+        pr.fp(x, b)
+        ms_fp = _timed_region(torch, stream, lambda: pr.fp(x, b), 2)
+        back = torch.zeros(pr.vol_shape, device=dev, dtype=dt)
+        ms_bp = _timed_region(torch, stream, lambda: pr.bp(b, back), 2)
+        del back
+        ref = orc.fp3d(orc.CONE, pr.geom.views_array()[sel], x.float().cpu().numpy(), cols, rows, pr.geom.vol_scale)
+        got = b[:, sel, :].double().cpu().numpy()
+        err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        if dt == torch.float32:
+            b32 = b
+            pid = D3.link('-proj3d', pg, b)
+            rid = D3.create('-vol', vg, 0)
+            cfg = A.astra_dict('CGLS3D_CUDA')
+            cfg['ProjectionDataId'] = pid
+            cfg['ReconstructionDataId'] = rid
+            cfg['option'] = {'UseGraph': True}
+            aid = A.create(cfg)
+            t0 = time.perf_counter()
+            A.run(aid, args.c5_iters)
+            torch.cuda.synchronize()
+            t_cgls = time.perf_counter() - t0
+            res = A.get_res_norm(aid) / float(b.double().norm())
+            rec32 = D3.get_shared(rid).clone()
+            A.delete(aid)
+            D3.delete([pid, rid])
+            diff = None
+        else:
+            # CGLS with the iterates in the storage type (FP32 arithmetic per
+            # element), FP64 inner products
+            bh = b32.to(dt) if b32 is not None else b
+
+            def dot(a_, b_):
+                r_ = torch.zeros(1, dtype=torch.float64, device=dev)
+                L.check(lib.b2t_dot_f64(a_.data_ptr(), b_.data_ptr(), a_.numel(), code, r_.data_ptr(),
+                                        stream.cuda_stream))
+                return r_
+
+            # the operator scaled by 1 / c (c = sqrt(views x n), the projectors'
+            # output scale) keeps A^T r and A p inside the FP16 range; the
+            # iterate is then c x
+            c = float(np.sqrt(na * n))
+            sc = 1.0 / c
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            xr = torch.zeros(pr.vol_shape, device=dev, dtype=dt)
+            r = bh.clone()
+            p = torch.zeros(pr.vol_shape, device=dev, dtype=dt)
+            pr.bp(r, p, output_scale=sc)
+            q = torch.zeros(pr.proj_shape, device=dev, dtype=dt)
+            z = torch.zeros(pr.vol_shape, device=dev, dtype=dt)
+            gamma = dot(p, p)
+            for _ in range(args.c5_iters):
+                pr.fp(p, q, output_scale=sc)
+                alpha = (gamma / dot(q, q)).float()
+                xr.add_((p.float() * alpha).to(dt))
+                r.sub_((q.float() * alpha).to(dt))
+                pr.bp(r, z, output_scale=sc)
+                g2 = dot(z, z)
+                beta = (g2 / gamma).float()
+                p.copy_((z.float() + p.float() * beta).to(dt))
+                gamma = g2
+            torch.cuda.synchronize()
+            t_cgls = time.perf_counter() - t0
+            pr.fp(xr, q, output_scale=sc)
+            res = float((bh.double() - q.double()).norm() / bh.double().norm())
+            diff = (float(torch.linalg.vector_norm((xr.float() * sc - rec32).double()) /
+                          torch.linalg.vector_norm(rec32.double())) if rec32 is not None else None)
+            del xr, r, p, q, z
+        out[name] = {"fp_ms": ms_fp, "bp_ms": ms_bp, "fp_gups": ups / ms_fp / 1e6, "bp_gups": ups / ms_bp / 1e6,
+                     "fp_rel_l2_vs_oracle": err, "oracle_views": sel,
+                     "cgls_iterations": args.c5_iters, "cgls_s": t_cgls, "cgls_s_per_iter": t_cgls / args.c5_iters,
+                     "cgls_relative_residual": res, "cgls_rel_l2_vs_f32": diff}
+        if dt != torch.float32:
+            del b
+        torch.cuda.empty_cache()
+    clocks = sampler.stop()
+    f32 = out.get("f32", next(iter(out.values())))
+    value = 2 * ups / (f32["fp_ms"] + f32["bp_ms"]) / 1e6
+    line = {"metric": "cone_vec FP+BP GUPS at 1024^3x1500 (C5), f32 storage", "value": value, "unit": "GUPS",
+            "n_gpus": 1, "steps": 2, "warmup": 1, "ms_per_step": f32["fp_ms"] + f32["bp_ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f16/bf16 storage beside)",
+            "data": "synthetic",
+            "config": {"workload": "cone_vec %d^3 volume of 20 seeded ellipsoids, %d jittered views (0.5 px shift, "
+                                   "0.1 deg tilt), 1280x1024 detector, SOD 1500, ODD 600; CGLS %d iterations"
+                                   % (n, na, args.c5_iters), "workload_kind": "c5"},
+            "storage": out, "e2e": None, "clocks": clocks, "roofline": None, "cpu_baseline": None}
+    print(json.dumps(line))
+    return 0
+
+
 def run_workload(args):
     """--workload fdk | sirt3d | cgls3d on the same 512^3 x 720 cone geometry.
 
@@ -475,6 +853,11 @@ def run_workload(args):
         e2e = {"value": 1e3 / ems, "unit": unit, "h2d_bytes_per_step": proj.numel() * 4,
                "d2h_bytes_per_step": rec.numel() * 4, "ms_per_step": ems,
                "path": "astra-style fdk() with pinned host projections copied in and the volume copied out"}
+        if not args.no_ref_cuda:
+            P.fdk(pr, proj, rec)
+            extra["ref_cuda"] = ref_algo_fdk(torch, args, proj, rec)
+            if "s" in extra["ref_cuda"]:
+                extra["ref_cuda"]["speedup"] = extra["ref_cuda"]["s"] / (ms * 1e-3)
     else:
         D3 = importlib.import_module("astra-toolbox_b200.data3d")
         A = importlib.import_module("astra-toolbox_b200.algorithm")
@@ -505,6 +888,29 @@ def run_workload(args):
         bnorm = float(proj.double().norm())
         A.delete(aid)
         D3.delete([pid, rid])
+        ref_block = None
+        if not args.no_ref_cuda:
+            kind = 'SIRT3D_CUDA' if args.workload == "sirt3d" else 'CGLS3D_CUDA'
+
+            def our_run(k):
+                rid2 = D3.create('-vol', vg, 0)
+                pid2 = D3.link('-proj3d', pg, proj)
+                c2 = A.astra_dict(kind)
+                c2['ProjectionDataId'] = pid2
+                c2['ReconstructionDataId'] = rid2
+                c2['option'] = {'UseGraph': True}
+                a2 = A.create(c2)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                A.run(a2, k)
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t0
+                r = A.get_res_norm(a2) / bnorm
+                A.delete(a2)
+                D3.delete([pid2, rid2])
+                return dt, r
+
+            ref_block = ref_algo_iterative(torch, args, kind, proj, our_run)
         value, unit, hib = ms * 1e-3, "s/iter", False
         metric = ("SIRT3D" if args.workload == "sirt3d" else "CGLS3D") + " s/iter at 512^3x720"
         extra = {"iterations_before_residual": args.warmup + args.steps + (1 if restart is not None else 0),
@@ -513,6 +919,8 @@ def run_workload(args):
             extra["restart_ms_per_run"] = restart
             extra["timing"] = ("run(steps) and run(1) timed; s/iter = (T_steps - T_1) / (steps - 1), the "
                                "restart every run call does is reported apart")
+        if ref_block is not None:
+            extra["ref_cuda"] = ref_block
         roof = None
         e2e = None
     line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
@@ -692,8 +1100,13 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's CUDA build")
+    ap.add_argument("--ref-iters", type=int, default=30,
+                    help="iterations of the reference's SIRT3D / CGLS3D whose residual is the target")
     ap.add_argument("--workload", default="fpbp",
-                    choices=["fpbp", "fdk", "sirt3d", "cgls3d", "batch2d", "stream", "sart2d", "cyl"])
+                    choices=["fpbp", "fdk", "sirt3d", "cgls3d", "batch2d", "stream", "sart2d", "cyl", "c1", "c5"])
+    ap.add_argument("--c5-views", type=int, default=1500)
+    ap.add_argument("--c5-iters", type=int, default=30)
+    ap.add_argument("--c5-types", default="f32,f16,bf16")
     ap.add_argument("--budget-gb", type=float, default=4.0, help="device budget of --workload stream")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -702,6 +1115,10 @@ def main():
         return run_reference(args)
     if args.workload == "batch2d":
         return run_batch2d(args)
+    if args.workload == "c1":
+        return run_c1(args)
+    if args.workload == "c5":
+        return run_c5(args)
     if args.workload in ("stream", "sart2d", "cyl"):
         return run_extra(args)
     if args.workload != "fpbp":

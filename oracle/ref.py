@@ -241,6 +241,105 @@ def sart2d(vol_geom, proj_geom, sino, vol0, iterations, min_value=None, max_valu
     return vol
 
 
+class Algo3D:
+    """The reference's own 3D algorithm object -- 'SIRT3D_CUDA', 'CGLS3D_CUDA'
+    or 'FDK_CUDA' (Ram-Lak) -- for a circular cone geometry over float32 CUDA
+    tensors proj (v, angles, u) and vol (z, y, x), linked as the reference's
+    GPU data.  run() synchronises the device."""
+
+    TYPES = {'SIRT3D_CUDA': 0, 'CGLS3D_CUDA': 1, 'FDK_CUDA': 2}
+
+    def __init__(self, kind, angles, sod, odd, proj, vol, det_spacing=(1.0, 1.0)):
+        L = lib()
+        L.ref_algo3d_create.restype = _P
+        L.ref_algo3d_create.argtypes = [_I, _I, _I, _I, _I, _I, _I, _F, _F, _P, _F, _F, _P, _P]
+        L.ref_algo3d_run.argtypes = [_P, _I]
+        L.ref_algo3d_residual.argtypes = [_P, _P]
+        L.ref_algo3d_destroy.argtypes = [_P]
+        self._L = L
+        self._keep = (proj, vol)
+        self.angles = np.ascontiguousarray(angles, dtype=np.float32)
+        nv, na, nu = proj.shape
+        nz, ny, nx = vol.shape
+        self.h = L.ref_algo3d_create(self.TYPES[kind], nx, ny, nz, na, nu, nv, det_spacing[0], det_spacing[1],
+                                     self.angles.ctypes.data, sod, odd, proj.data_ptr(), vol.data_ptr())
+        assert self.h, "the reference refused the algorithm"
+
+    def run(self, iterations=1):
+        assert self._L.ref_algo3d_run(self.h, int(iterations)) == 0
+
+    def residual(self):
+        v = ctypes.c_float(0.0)
+        assert self._L.ref_algo3d_residual(self.h, ctypes.byref(v)) == 0
+        return float(v.value)
+
+    def close(self):
+        if self.h:
+            self._L.ref_algo3d_destroy(self.h)
+            self.h = None
+
+
+# ---------------------------------------------------------------------------
+# the reference's CPU 2D path (oracle/_ref/libastra_ref_cpu.so, built without
+# CUDA by oracle/ref_cpu.mk; single-threaded, runs without a GPU)
+# ---------------------------------------------------------------------------
+
+LIB_CPU = os.path.join(_HERE, "_ref", "libastra_ref_cpu.so")
+CPU_KERNELS = {'line': 0, 'linear': 1, 'strip': 2}
+_lib_cpu = None
+
+
+def cpu_available():
+    return os.path.exists(LIB_CPU)
+
+
+def lib_cpu():
+    global _lib_cpu
+    if _lib_cpu is None:
+        L = ctypes.CDLL(LIB_CPU)
+        for name in ("refcpu_fp2d", "refcpu_bp2d"):
+            getattr(L, name).argtypes = [_I, _I, _I, _I, _I, _I, _F, _P, _F, _F, _P, _P]
+        L.refcpu_sirt2d.argtypes = [_I, _I, _I, _I, _I, _I, _F, _P, _F, _F, _P, _P, _I]
+        _lib_cpu = L
+    return _lib_cpu
+
+
+def _cpu_args(kind, kernel, shape, angles, ndet, det_width, sod, odd):
+    rows, cols = shape
+    ang = np.ascontiguousarray(angles, dtype=np.float32)
+    geom = {'parallel': 0, 'fanflat': 1}[kind]
+    return [geom, CPU_KERNELS[kernel], cols, rows, ang.size, ndet, det_width, ang.ctypes.data, sod, odd], ang
+
+
+def cpu_fp2d(kind, kernel, vol, angles, ndet, det_width=1.0, sod=0.0, odd=0.0):
+    """Reference CPU forward projection ('parallel': line / linear / strip,
+    'fanflat': line / strip) of a (rows, cols) float32 volume of unit pixels
+    centred on the origin; returns the (angles, ndet) sinogram."""
+    vol = np.ascontiguousarray(vol, dtype=np.float32)
+    args, ang = _cpu_args(kind, kernel, vol.shape, angles, ndet, det_width, sod, odd)
+    sino = np.zeros((ang.size, ndet), dtype=np.float32)
+    assert lib_cpu().refcpu_fp2d(*args, vol.ctypes.data, sino.ctypes.data) == 0
+    return sino
+
+
+def cpu_bp2d(kind, kernel, sino, shape, angles, det_width=1.0, sod=0.0, odd=0.0):
+    """Reference CPU backprojection of an (angles, ndet) sinogram into a (rows, cols) volume."""
+    sino = np.ascontiguousarray(sino, dtype=np.float32)
+    args, ang = _cpu_args(kind, kernel, shape, angles, sino.shape[1], det_width, sod, odd)
+    vol = np.zeros(shape, dtype=np.float32)
+    assert lib_cpu().refcpu_bp2d(*args, sino.ctypes.data, vol.ctypes.data) == 0
+    return vol
+
+
+def cpu_sirt2d(kind, kernel, sino, shape, angles, iterations, det_width=1.0, sod=0.0, odd=0.0, vol0=None):
+    """Reference CPU SIRT (CSirtAlgorithm) from vol0 (zeros by default)."""
+    sino = np.ascontiguousarray(sino, dtype=np.float32)
+    args, ang = _cpu_args(kind, kernel, shape, angles, sino.shape[1], det_width, sod, odd)
+    vol = np.zeros(shape, dtype=np.float32) if vol0 is None else np.array(vol0, dtype=np.float32, order='C')
+    assert lib_cpu().refcpu_sirt2d(*args, sino.ctypes.data, vol.ctypes.data, int(iterations)) == 0
+    return vol
+
+
 def gen_filter(ref_type, N, d=1.0, parameter=-1.0):
     """The reference's genFilter spectrum (N // 2 + 1 floats) for E_FBPFILTER
     value ref_type (FILTER_ERROR = 0, FILTER_NONE = 1, FILTER_RAMLAK = 2, ...)."""

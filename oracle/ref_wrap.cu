@@ -53,6 +53,12 @@
 #include "astra/cuda/3d/fdk.h"
 #include "astra/cuda/3d/par3d_bp.h"
 #include "astra/cuda/3d/par3d_fp.h"
+#include "astra/cuda/3d/mem3d.h"
+#include "astra/CudaCglsAlgorithm3D.h"
+#include "astra/CudaFDKAlgorithm3D.h"
+#include "astra/CudaProjector3D.h"
+#include "astra/CudaSirtAlgorithm3D.h"
+#include "astra/Data3D.h"
 
 using namespace astra;
 
@@ -491,5 +497,88 @@ int ref_gen_filter(int type, float d, float parameter, int N, float *out)
     delete[] f;
     return 0;
 }
+
+// A reference 3D algorithm object (type 0: SIRT3D_CUDA, 1: CGLS3D_CUDA,
+// 2: FDK_CUDA with the Ram-Lak filter; src/CudaSirtAlgorithm3D.cpp,
+// CudaCglsAlgorithm3D.cpp, CudaFDKAlgorithm3D.cpp, unchanged) for a circular
+// cone geometry over caller device buffers: projections [v][angle][u],
+// volume [z][y][x].  FDK takes them linked as the reference's GPU data
+// (astraCUDA3d::wrapHandle, cuda/3d/mem3d.cu:521, the path its DLPack
+// interface takes); SIRT3D and CGLS3D accept host-memory data only
+// (CudaSirtAlgorithm3D.cpp, CudaCglsAlgorithm3D.cpp initialisation checks),
+// so their projections are copied to host memory at creation and every run
+// copies its result back into the device volume.
+struct RefAlgo3D {
+    std::unique_ptr<CConeProjectionGeometry3D> pg;
+    std::unique_ptr<CVolumeGeometry3D> vg;
+    std::unique_ptr<CCudaProjector3D> proj;
+    std::unique_ptr<CFloat32ProjectionData3D> sino;
+    std::unique_ptr<CFloat32VolumeData3D> vol;
+    std::unique_ptr<CReconstructionAlgorithm3D> alg;
+    float *d_vol = nullptr;  // host-memory volume: copied here after each run
+    size_t vol_bytes = 0;
+};
+
+void *ref_algo3d_create(int type, int nx, int ny, int nz, int na, int nu, int nv, float du, float dv,
+                        const float *angles, float sod, float odd, float *d_proj, float *d_vol)
+{
+    auto *h = new RefAlgo3D;
+    h->pg.reset(new CConeProjectionGeometry3D(na, nv, nu, du, dv, std::vector<float32>(angles, angles + na), sod,
+                                              odd));
+    h->vg.reset(new CVolumeGeometry3D(nx, ny, nz));
+    h->proj.reset(new CCudaProjector3D(*h->pg, *h->vg));
+    if (type == 2) {
+        h->sino.reset(new CFloat32ProjectionData3D(*h->pg, astraCUDA3d::wrapHandle(d_proj, nu, na, nv, nu)));
+        h->vol.reset(new CFloat32VolumeData3D(*h->vg, astraCUDA3d::wrapHandle(d_vol, nx, ny, nz, nx)));
+    } else {
+        h->sino.reset(createCFloat32ProjectionData3DMemory(*h->pg));
+        h->vol.reset(createCFloat32VolumeData3DMemory(*h->vg));
+        h->vol_bytes = sizeof(float) * (size_t)nx * ny * nz;
+        h->d_vol = d_vol;
+        if (cudaMemcpy(h->sino->getFloat32Memory(), d_proj, sizeof(float) * (size_t)nu * na * nv,
+                       cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(h->vol->getFloat32Memory(), d_vol, h->vol_bytes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            delete h;
+            return nullptr;
+        }
+    }
+    if (type == 0) {
+        h->alg.reset(new CCudaSirtAlgorithm3D(h->proj.get(), h->sino.get(), h->vol.get()));
+    } else if (type == 1) {
+        h->alg.reset(new CCudaCglsAlgorithm3D(h->proj.get(), h->sino.get(), h->vol.get()));
+    } else if (type == 2) {
+        SFilterConfig f;
+        f.m_eType = FILTER_RAMLAK;
+        h->alg.reset(new CCudaFDKAlgorithm3D(h->proj.get(), h->sino.get(), h->vol.get(), f, false));
+    }
+    if (!h->alg || !h->alg->isInitialized()) {
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+// iterations (ignored by FDK); synchronises the device
+int ref_algo3d_run(void *p, int iterations)
+{
+    auto *h = static_cast<RefAlgo3D *>(p);
+    const bool ok = h->alg->run(iterations);
+    cudaDeviceSynchronize();
+    if (ok && h->d_vol &&
+        cudaMemcpy(h->d_vol, h->vol->getFloat32Memory(), h->vol_bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return 2;
+    return ok ? 0 : 1;
+}
+
+int ref_algo3d_residual(void *p, float *norm)
+{
+    auto *h = static_cast<RefAlgo3D *>(p);
+    float32 v = 0.0f;
+    if (!h->alg->getResidualNorm(v)) return 1;
+    *norm = v;
+    return 0;
+}
+
+void ref_algo3d_destroy(void *p) { delete static_cast<RefAlgo3D *>(p); }
 
 }  // extern "C"
