@@ -23,23 +23,81 @@ def available():
     return os.path.exists(LIB)
 
 
+# The reference built with its cuda/3d projectors replaced by libb2tomo
+# (oracle/ref_shim.mk): the same entry points, the reference's own host code
+# (CompositeGeometryManager, FDK, algorithm objects) running on the library.
+LIB_SHIM = os.path.join(_HERE, "_ref", "libastra_ref_shim.so")
+_shim = None
+_use_shim = False
+
+
+def shim_available():
+    return os.path.exists(LIB_SHIM)
+
+
+class use_shim:
+    """with use_shim(): every function of this module calls the shim build."""
+
+    def __enter__(self):
+        global _use_shim
+        self._prev = _use_shim
+        _use_shim = True
+        return self
+
+    def __exit__(self, *exc):
+        global _use_shim
+        _use_shim = self._prev
+        return False
+
+
 def lib():
-    global _lib
+    global _lib, _shim
+    if _use_shim:
+        if _shim is None:
+            _shim = _declare(ctypes.CDLL(LIB_SHIM))
+        return _shim
     if _lib is None:
-        L = ctypes.CDLL(LIB)
-        L.ref_geom3d.argtypes = [_I, _I, _I, _I, _P, _I, _I, _I, _F, _F, _P, _F, _F, _P, _P, _P]
-        L.ref_geom2d.argtypes = [_I, _I, _I, _P, _I, _I, _F, _P, _F, _F, _P, _P, _P]
-        L.ref_cuda_fp3d.argtypes = [_I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _I, _P, _P]
-        L.ref_cuda_bp3d.argtypes = [_I, _I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _I, _P, _P]
-        L.ref_cuda_cyl.argtypes = [_I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _P, _P]
-        L.ref_cuda_sumsqw.argtypes = [_P, _I, _I, _I, _I, _I, _I, _P, _F, _P]
-        L.ref_cuda_fdk.argtypes = [_P, _I, _I, _I, _I, _I, _I, _P, _I, _F, _P, _P]
-        L.ref_cuda_fp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _P, _P]
-        L.ref_cuda_bp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _I, _P, _P]
-        L.ref_gen_filter.argtypes = [_I, _F, _F, _I, _P]
-        L.ref_sart2d.argtypes = [_I, _I, _I, _P, _I, _I, _F, _P, _F, _F, _P, _P, _P, _I, _I, _F, _I, _F]
-        _lib = L
+        _lib = _declare(ctypes.CDLL(LIB))
     return _lib
+
+
+def _declare(L):
+    L.ref_geom3d.argtypes = [_I, _I, _I, _I, _P, _I, _I, _I, _F, _F, _P, _F, _F, _P, _P, _P]
+    L.ref_geom2d.argtypes = [_I, _I, _I, _P, _I, _I, _F, _P, _F, _F, _P, _P, _P]
+    L.ref_cuda_fp3d.argtypes = [_I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _I, _P, _P]
+    L.ref_cuda_bp3d.argtypes = [_I, _I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _I, _P, _P]
+    L.ref_cuda_cyl.argtypes = [_I, _P, _I, _I, _I, _I, _I, _I, _P, _F, _P, _P]
+    L.ref_cuda_sumsqw.argtypes = [_P, _I, _I, _I, _I, _I, _I, _P, _F, _P]
+    L.ref_cuda_fdk.argtypes = [_P, _I, _I, _I, _I, _I, _I, _P, _I, _F, _P, _P]
+    L.ref_cuda_fp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _P, _P]
+    L.ref_cuda_bp2d.argtypes = [_I, _P, _I, _I, _I, _I, _F, _I, _I, _P, _P]
+    L.ref_gen_filter.argtypes = [_I, _F, _F, _I, _P]
+    L.ref_sart2d.argtypes = [_I, _I, _I, _P, _I, _I, _F, _P, _F, _F, _P, _P, _P, _I, _I, _F, _I, _F]
+    L.ref_cgm_cone.argtypes = [_I, _I, ctypes.c_size_t, _I, _I, _I, _I, _I, _I, _F, _F, _P, _F, _F, _P, _P]
+    return L
+
+
+def cgm_cone(op, angles, sod, odd, proj, vol, memory=0, gpu_data=True, det_spacing=(1.0, 1.0)):
+    """The reference's CompositeGeometryManager doFP (op 'fp': proj = A vol)
+    or doBP (op 'bp': vol = B proj) on a circular cone geometry, MODE_SET.
+    gpu_data: proj and vol are float32 CUDA tensors linked as the reference's
+    GPU data (the direct_FP3D / direct_BP3D path); else float32 numpy arrays in
+    the reference's host data objects (create_sino3d_gpu).  memory: the GPU
+    memory limit under which the manager splits the job (0: none)."""
+    ang = np.ascontiguousarray(angles, dtype=np.float32)
+    nv, na, nu = proj.shape
+    nz, ny, nx = vol.shape
+    if gpu_data:
+        import torch
+        torch.cuda.synchronize()
+        pp, vp = proj.data_ptr(), vol.data_ptr()
+    else:
+        assert proj.dtype == np.float32 and vol.dtype == np.float32
+        assert proj.flags.c_contiguous and vol.flags.c_contiguous
+        pp, vp = proj.ctypes.data, vol.ctypes.data
+    rc = lib().ref_cgm_cone(0 if op == 'fp' else 1, int(bool(gpu_data)), int(memory), nx, ny, nz, na, nu, nv,
+                            det_spacing[0], det_spacing[1], ang.ctypes.data, sod, odd, pp, vp)
+    assert rc == 0, "the reference's CompositeGeometryManager failed"
 
 
 def geom3d(vol_geom, proj_geom):

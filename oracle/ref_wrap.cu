@@ -54,6 +54,7 @@
 #include "astra/cuda/3d/par3d_bp.h"
 #include "astra/cuda/3d/par3d_fp.h"
 #include "astra/cuda/3d/mem3d.h"
+#include "astra/CompositeGeometryManager.h"
 #include "astra/CudaCglsAlgorithm3D.h"
 #include "astra/CudaFDKAlgorithm3D.h"
 #include "astra/CudaProjector3D.h"
@@ -580,5 +581,50 @@ int ref_algo3d_residual(void *p, float *norm)
 }
 
 void ref_algo3d_destroy(void *p) { delete static_cast<RefAlgo3D *>(p); }
+
+// The reference's CompositeGeometryManager doFP (op 0) / doBP (op 1) in
+// MODE_SET on a circular cone geometry: the path under
+// astra.experimental.direct_FP3D / direct_BP3D (linked device data, gpu_data
+// = 1; python/astra/experimental.pyx:172-227) and create_sino3d_gpu /
+// create_backprojection3d_gpu (host data, gpu_data = 0), with the GPU memory
+// limit of astra.set_gpu_index(0, memory) (0: none), under which the manager
+// splits the job (src/CompositeGeometryManager.cpp:218-379).
+int ref_cgm_cone(int op, int gpu_data, size_t memory, int nx, int ny, int nz, int na, int nu, int nv, float du,
+                 float dv, const float *angles, float sod, float odd, float *proj, float *vol)
+{
+    CConeProjectionGeometry3D pg(na, nv, nu, du, dv, std::vector<float32>(angles, angles + na), sod, odd);
+    CVolumeGeometry3D vg(nx, ny, nz);
+    CCudaProjector3D projector(pg, vg);
+    std::unique_ptr<CFloat32ProjectionData3D> P;
+    std::unique_ptr<CFloat32VolumeData3D> V;
+    if (gpu_data) {
+        P.reset(new CFloat32ProjectionData3D(pg, astraCUDA3d::wrapHandle(proj, nu, na, nv, nu)));
+        V.reset(new CFloat32VolumeData3D(vg, astraCUDA3d::wrapHandle(vol, nx, ny, nz, nx)));
+    } else {
+        P.reset(createCFloat32ProjectionData3DMemory(pg));
+        V.reset(createCFloat32VolumeData3DMemory(vg));
+        std::memcpy(op == 0 ? (void *)V->getFloat32Memory() : (void *)P->getFloat32Memory(), op == 0 ? vol : proj,
+                    sizeof(float) * (op == 0 ? (size_t)nx * ny * nz : (size_t)nu * na * nv));
+    }
+    SGPUParams gp;
+    gp.GPUIndices.push_back(0);
+    gp.memory = memory;
+    CCompositeGeometryManager::setGlobalGPUParams(gp);
+    CCompositeGeometryManager m;
+    std::vector<CFloat32VolumeData3D *> vv{V.get()};
+    std::vector<CFloat32ProjectionData3D *> pv{P.get()};
+    const bool ok = op == 0 ? m.doFP(&projector, vv, pv, CCompositeGeometryManager::MODE_SET)
+                            : m.doBP(&projector, vv, pv, CCompositeGeometryManager::MODE_SET);
+    SGPUParams none;
+    none.GPUIndices.push_back(0);
+    none.memory = 0;
+    CCompositeGeometryManager::setGlobalGPUParams(none);
+    if (!ok) return 1;
+    if (!gpu_data)
+        std::memcpy(op == 0 ? proj : vol, op == 0 ? (void *)P->getFloat32Memory() : (void *)V->getFloat32Memory(),
+                    sizeof(float) * (op == 0 ? (size_t)nu * na * nv : (size_t)nx * ny * nz));
+    cudaDeviceSynchronize();
+    return 0;
+}
 
 }  // extern "C"
