@@ -81,37 +81,131 @@ __device__ __forceinline__ void split_texel_t(float qm, int &k, float &f)
     f = __fadd_rn(__fadd_rn(qm, -r), 0.5f);
 }
 
-// shared-memory texel at 32-bit shared-window address a
-// Shared-memory load at 32-bit shared address a + OFF (OFF an immediate of
-// the instruction, so the four texels of a sample share one address register).
+// FP32 texel at 32-bit shared address a + OFF (OFF an immediate of the
+// instruction, so the texels of a sample share one address register).
 template <typename T, int OFF> __device__ __forceinline__ float lds_sh(uint32_t a)
 {
-    if constexpr (sizeof(T) == 4) {
-        float v;
-        asm volatile("ld.shared.f32 %0, [%1+%2];" : "=f"(v) : "r"(a), "n"(OFF));
-        return v;
-    } else {
-        unsigned short v;
-        asm volatile("ld.shared.u16 %0, [%1+%2];" : "=h"(v) : "r"(a), "n"(OFF));
-        if constexpr (std::is_same<T, __half>::value) return __half2float(__ushort_as_half(v));
-        else return __bfloat162float(__ushort_as_bfloat16(v));
-    }
+    static_assert(sizeof(T) == 4, "16-bit texels are read as pairs");
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1+%2];" : "=f"(v) : "r"(a), "n"(OFF));
+    return v;
 }
 
-// Tile width and ring row pitch in texels: a TMA box row must be a multiple
-// of 16 bytes, and rows that share shared-memory banks should be far apart
-// (84 x 4 B: 8 rows; 88 x 2 B: 16 rows).
-template <typename T> __host__ __device__ constexpr int tile_bu() { return sizeof(T) == 4 ? 84 : 88; }
-// Ring rows (multiple of BPT_CHUNK) in the BPT_RING_BYTES of shared memory.
-// An 8-row chunk is a multiple of 128 bytes for both pitches, so every chunk
-// destination (ring rows are allocated in whole chunks) is 128-byte aligned.
-template <typename T> __host__ __device__ constexpr int ring_rows()
+// A pair of 16-bit texels (x[u], x[u+1]) in one 32-bit word, as two floats.
+template <typename T> __device__ __forceinline__ float2 pair_f2(uint32_t v)
 {
-    return (BPT_RING_BYTES / (tile_bu<T>() * (int)sizeof(T))) & ~(BPT_CHUNK - 1);
+    if constexpr (std::is_same<T, __half>::value) return __half22float2(*reinterpret_cast<const __half2 *>(&v));
+    else return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&v));
 }
-static_assert(BPT_CHUNK * 84 * 4 % 128 == 0 && BPT_CHUNK * 88 * 2 % 128 == 0, "chunk alignment");
-static_assert((84 * 4) % 16 == 0 && (88 * 2) % 16 == 0, "TMA box row bytes");
-static_assert(ring_rows<float>() >= BPT_BV && ring_rows<__half>() >= BPT_BV, "the ring holds the largest view");
+// The pair at 32-bit shared address a + OFF.
+template <typename T, int OFF> __device__ __forceinline__ float2 lds_pair(uint32_t a)
+{
+    uint32_t v;
+    asm volatile("ld.shared.b32 %0, [%1+%2];" : "=r"(v) : "r"(a), "n"(OFF));
+    return pair_f2<T>(v);
+}
+
+// Two FP32 values in one 64-bit register, and the packed f32x2 arithmetic of
+// sm_100a on them: one instruction, each half rounded as the scalar
+// operation rounds it.
+__device__ __forceinline__ uint64_t pk2(float lo, float hi)
+{
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 upk2(uint64_t v)
+{
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c)
+{
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t add2_rd(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// Storage of the padded projections the kernel reads: FP32 texels, or for
+// the 16-bit types the pair layout (padded_elem_size), whose element u of a
+// row is the 32-bit word (x[u], x[u+1]).  A bilinear sample then takes one
+// 32-bit load per row instead of two 16-bit ones, and half the
+// shared-memory wavefronts; the arithmetic (in FP32) is the texel form's.
+template <typename T, bool PAIR> struct Elem {
+    using type = T;
+};
+template <> struct Elem<__half, true> {
+    using type = __half2;
+};
+template <> struct Elem<__nv_bfloat16, true> {
+    using type = __nv_bfloat162;
+};
+template <typename T, bool PAIR> using elem_t = typename Elem<T, PAIR>::type;
+
+// Bilinear sample with weights fu (along u) and fv (along v) from element p
+// of shared memory (GLOBAL false) or of the padded projections in global
+// memory, rows rs elements apart.
+template <typename T, bool PAIR, bool GLOBAL>
+__device__ __forceinline__ float bilerp(const elem_t<T, PAIR> *p, long long rs, float fu, float fv)
+{
+    float v00, v10, v01, v11;
+    if constexpr (PAIR) {
+        using E = elem_t<T, PAIR>;
+        const E e0 = GLOBAL ? __ldg(p) : *p, e1 = GLOBAL ? __ldg(p + rs) : p[rs];
+        const float2 r0 = pair_f2<T>(*reinterpret_cast<const uint32_t *>(&e0));
+        const float2 r1 = pair_f2<T>(*reinterpret_cast<const uint32_t *>(&e1));
+        v00 = r0.x;
+        v10 = r0.y;
+        v01 = r1.x;
+        v11 = r1.y;
+    } else {
+        v00 = GLOBAL ? ldgt(p) : lds(p);
+        v10 = GLOBAL ? ldgt(p + 1) : lds(p + 1);
+        v01 = GLOBAL ? ldgt(p + rs) : lds(p + rs);
+        v11 = GLOBAL ? ldgt(p + rs + 1) : lds(p + rs + 1);
+    }
+    const float a = fmaf(fu, v10 - v00, v00);
+    const float b = fmaf(fu, v11 - v01, v01);
+    return fmaf(fv, b - a, a);
+}
+
+// Tile width and ring row pitch in 4-byte elements: a TMA box row must be a
+// multiple of 16 bytes, and rows that share shared-memory banks should be far
+// apart (84 x 4 B: 8 rows).
+template <typename E> __host__ __device__ constexpr int tile_bu()
+{
+    static_assert(sizeof(E) == 4, "tile elements are FP32 texels or 16-bit pairs");
+    return 84;
+}
+// Ring rows (multiple of BPT_CHUNK) in the BPT_RING_BYTES of shared memory.
+// An 8-row chunk is a multiple of 128 bytes, so every chunk destination (ring
+// rows are allocated in whole chunks) is 128-byte aligned.
+template <typename E> __host__ __device__ constexpr int ring_rows()
+{
+    return (BPT_RING_BYTES / (tile_bu<E>() * (int)sizeof(E))) & ~(BPT_CHUNK - 1);
+}
+static_assert(BPT_CHUNK * 84 * 4 % 128 == 0, "chunk alignment");
+static_assert((84 * 4) % 16 == 0, "TMA box row bytes");
+static_assert(ring_rows<float>() >= BPT_BV, "the ring holds the largest view");
 
 // Per-view record written by the producer warp: the tile's origin in padded
 // texels (u0, v0), its first ring row and its row count (0: the footprint does
@@ -165,13 +259,13 @@ __device__ __forceinline__ float4 fold_form(float4 c, float4 d, double k, double
 // lands in the ring.  The views then go through the ring one at a time: the
 // warp finds room together (waiting for the oldest views to be released) and
 // the view's own lane issues the loads and writes the record.
-template <typename T, int KIND, bool CIRC>
-__device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t *full, uint64_t *empty,
+template <typename E, int KIND, bool CIRC>
+__device__ __noinline__ void bp_produce(const BPTmaLaunch &L, E *ring, uint64_t *full, uint64_t *empty,
                                         StageInfo *info, int lane, float cx,
                                         float cy, float fz0)
 {
-    constexpr int R = ring_rows<T>();
-    constexpr int BU = tile_bu<T>();
+    constexpr int R = ring_rows<E>();
+    constexpr int BU = tile_bu<E>();
     // voxel-centre extent of the block; along z the block's full BPT_Z
     // slices, so that the voxels computed past the volume's last slice
     // (and discarded) also project inside the tile
@@ -299,7 +393,7 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t 
                 // phase cannot complete before the arrival, which releases
                 // the record
                 if (nrows > 0) {
-                    mbar_expect_tx(&full[slot], (uint32_t)(nrows * BU * sizeof(T)));
+                    mbar_expect_tx(&full[slot], (uint32_t)(nrows * BU * sizeof(E)));
                     for (int c = 0; c < nrows; c += BPT_CHUNK)
                         tma_load_3d(ring + (size_t)(at + c) * BU, &L.tmap, r.u0, L.a0 + vk, r.v0 + c, &full[slot]);
                 }
@@ -321,11 +415,13 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, T *ring, uint64_t 
 template <typename T, int KIND, int KER, bool CIRC>
 __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __grid_constant__ BPTmaLaunch L)
 {
-    constexpr int R = ring_rows<T>();
-    constexpr int BU = tile_bu<T>();
+    constexpr bool PAIR = sizeof(T) == 2;  // 16-bit texels are stored as pairs
+    using E = elem_t<T, PAIR>;
+    constexpr int R = ring_rows<E>();
+    constexpr int BU = tile_bu<E>();
     extern __shared__ __align__(128) unsigned char smraw[];
-    T *ring = reinterpret_cast<T *>(smraw);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smraw + (size_t)R * BU * sizeof(T));
+    E *ring = reinterpret_cast<E *>(smraw);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smraw + (size_t)R * BU * sizeof(E));
     uint64_t *empty = full + BPT_SLOTS;
     StageInfo *info = reinterpret_cast<StageInfo *>(empty + BPT_SLOTS);
 
@@ -347,7 +443,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
     if (warp == 8) {
         const float cx = 0.5f - 0.5f * (float)L.nx, cy = 0.5f - 0.5f * (float)L.ny;
         const float fz0 = (float)z0 + 0.5f - 0.5f * (float)L.nz;
-        bp_produce<T, KIND, CIRC>(L, ring, full, empty, info, lane, cx, cy, fz0);
+        bp_produce<E, KIND, CIRC>(L, ring, full, empty, info, lane, cx, cy, fz0);
         return;
     }
 
@@ -377,7 +473,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
             return;
         }
         const int4 hd = *reinterpret_cast<const int4 *>(&info[slot]);  // u0, v0, row0, nrows
-        const T *tile = ring + (size_t)hd.z * BU;
+        const E *tile = ring + (size_t)hd.z * BU;
         bool done = false;
         if (CIRC && active && hd.w > 0) {
             // u and the weight are independent of z, v is linear in z
@@ -406,19 +502,45 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
                 const int ku = min(max(__float_as_int(tU) - 0x4B400000, 0), BU - 2);
                 // shared address of row floor(q_j), column ku, is
                 // bits(q_j + M) * row bytes + abase (32-bit wrap-around)
-                constexpr uint32_t ROWB = BU * sizeof(T);
-                const uint32_t abase = smem_u32(tile) + (uint32_t)ku * (uint32_t)sizeof(T) - 0x4B400000u * ROWB;
+                constexpr uint32_t ROWB = BU * sizeof(E);
+                // the row bytes come from the launch record: with the literal
+                // constant the compiler expands each multiplication below
+                // into a chain of shift-and-add instructions (3 issue slots
+                // instead of one multiply-add)
+                const uint32_t rowb = L.tile_row_bytes;
+                const uint32_t abase = smem_u32(tile) + (uint32_t)ku * (uint32_t)sizeof(E) - 0x4B400000u * rowb;
+                // voxels j, j + 1 in the two halves of packed f32x2
+                // operations; each half rounds as the scalar texel form
+                // fmaf(fv, b - a, a), a = fmaf(fu, v10 - v00, v00), ...
+                const uint64_t dV2 = pk2(dV, dV), Vq2 = pk2(Vq, Vq), w2 = pk2(w, w), fu2 = pk2(fu, fu);
+                const uint64_t M2 = pk2(M, M), nM2 = pk2(-M, -M);
 #pragma unroll
-                for (int j = 0; j < BPT_Z; ++j) {
-                    const float q = fmaf((float)j, dV, Vq);
-                    const float t = __fadd_rd(q, M);
-                    const float fv = q - (t - M);
-                    const uint32_t a = (uint32_t)__float_as_int(t) * ROWB + abase;
-                    const float v00 = lds_sh<T, 0>(a), v10 = lds_sh<T, (int)sizeof(T)>(a);
-                    const float v01 = lds_sh<T, (int)ROWB>(a), v11 = lds_sh<T, (int)(ROWB + sizeof(T))>(a);
-                    const float av = fmaf(fu, v10 - v00, v00);
-                    const float bv = fmaf(fu, v11 - v01, v01);
-                    acc[j] = fmaf(fmaf(fv, bv - av, av), w, acc[j]);
+                for (int j = 0; j < BPT_Z; j += 2) {
+                    const uint64_t q2 = fma2(pk2((float)j, (float)(j + 1)), dV2, Vq2);
+                    const uint64_t t2 = add2_rd(q2, M2);
+                    const uint64_t fv2 = sub2(q2, add2(t2, nM2));
+                    const float2 t = upk2(t2);
+                    const uint32_t a0 = (uint32_t)__float_as_int(t.x) * rowb + abase;
+                    const uint32_t a1 = (uint32_t)__float_as_int(t.y) * rowb + abase;
+                    uint64_t v00, v10, v01, v11;
+                    if constexpr (PAIR) {
+                        const float2 p0 = lds_pair<T, 0>(a0), p1 = lds_pair<T, 0>(a1);
+                        const float2 q0 = lds_pair<T, (int)ROWB>(a0), q1 = lds_pair<T, (int)ROWB>(a1);
+                        v00 = pk2(p0.x, p1.x);
+                        v10 = pk2(p0.y, p1.y);
+                        v01 = pk2(q0.x, q1.x);
+                        v11 = pk2(q0.y, q1.y);
+                    } else {
+                        v00 = pk2(lds_sh<T, 0>(a0), lds_sh<T, 0>(a1));
+                        v10 = pk2(lds_sh<T, 4>(a0), lds_sh<T, 4>(a1));
+                        v01 = pk2(lds_sh<T, (int)ROWB>(a0), lds_sh<T, (int)ROWB>(a1));
+                        v11 = pk2(lds_sh<T, (int)ROWB + 4>(a0), lds_sh<T, (int)ROWB + 4>(a1));
+                    }
+                    const uint64_t av = fma2(fu2, sub2(v10, v00), v00);
+                    const uint64_t bv = fma2(fu2, sub2(v11, v01), v01);
+                    const float2 r = upk2(fma2(fma2(fv2, sub2(bv, av), av), w2, pk2(acc[j], acc[j + 1])));
+                    acc[j] = r.x;
+                    acc[j + 1] = r.y;
                 }
                 done = true;
             }
@@ -429,7 +551,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
         if (active && !done) {
             // the general paths recompute the voxel centre here rather than
             // keeping it live across the hot loop above
-            const T *gproj = static_cast<const T *>(L.proj);
+            const E *gproj = static_cast<const E *>(L.proj);
             const float fx = (float)(blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7)) + 0.5f - 0.5f * (float)L.nx;
             const float fy = (float)(blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3)) + 0.5f - 0.5f * (float)L.ny;
             const float fz0 = (float)(blockIdx.z * BPT_Z) + 0.5f - 0.5f * (float)L.nz;
@@ -463,15 +585,10 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
                         float fv;
                         split_texel_t(fmaf((float)j, dV, Vb) + vofs, kv, fv);
                         kv = min(max(kv, 0), nrows - 2);
-                        const T *p = tile + kv * BU + ku;
-                        const float v00 = lds(p), v10 = lds(p + 1);
-                        const float v01 = lds(p + BU), v11 = lds(p + BU + 1);
-                        const float a = fmaf(fu, v10 - v00, v00);
-                        const float b = fmaf(fu, v11 - v01, v01);
-                        acc[j] = fmaf(fmaf(fv, b - a, a), w, acc[j]);
+                        acc[j] = fmaf(bilerp<T, PAIR, false>(tile + kv * BU + ku, BU, fu, fv), w, acc[j]);
                     }
                 } else {
-                    const T *P = gproj + (long long)(L.a0 + i) * L.pu;
+                    const E *P = gproj + (long long)(L.a0 + i) * L.pu;
                     int ku;
                     float fu;
                     split_texel_t(U - 1.0f, ku, fu);
@@ -482,12 +599,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
                         float fv;
                         split_texel_t(fmaf((float)j, dV, Vb) - 1.0f, kv, fv);
                         kv = min(max(kv, -2), L.nv);
-                        const T *p = P + (long long)kv * L.pv + ku;
-                        const float v00 = ldgt(p), v10 = ldgt(p + 1);
-                        const float v01 = ldgt(p + L.pv), v11 = ldgt(p + L.pv + 1);
-                        const float a = fmaf(fu, v10 - v00, v00);
-                        const float b = fmaf(fu, v11 - v01, v01);
-                        acc[j] = fmaf(fmaf(fv, b - a, a), w, acc[j]);
+                        acc[j] = fmaf(bilerp<T, PAIR, true>(P + (long long)kv * L.pv + ku, L.pv, fu, fv), w, acc[j]);
                     }
                 }
             } else {
@@ -509,32 +621,22 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
                         w = W.den.w;
                     }
                     int ku, kv;
-                    float fu, fv;
-                    float v00, v10, v01, v11;
+                    float fu, fv, r;
                     if (nrows > 0) {
                         split_texel_t(U + 1.0f - (float)u0, ku, fu);
                         split_texel_t(Vc + 1.0f - (float)v0, kv, fv);
                         ku = min(max(ku, 0), BU - 2);
                         kv = min(max(kv, 0), nrows - 2);
-                        const T *p = tile + kv * BU + ku;
-                        v00 = lds(p);
-                        v10 = lds(p + 1);
-                        v01 = lds(p + BU);
-                        v11 = lds(p + BU + 1);
+                        r = bilerp<T, PAIR, false>(tile + kv * BU + ku, BU, fu, fv);
                     } else {
                         split_texel_t(U - 1.0f, ku, fu);
                         split_texel_t(Vc - 1.0f, kv, fv);
                         ku = min(max(ku, -2), L.nu);
                         kv = min(max(kv, -2), L.nv);
-                        const T *p = gproj + (long long)(L.a0 + i) * L.pu + (long long)kv * L.pv + ku;
-                        v00 = ldgt(p);
-                        v10 = ldgt(p + 1);
-                        v01 = ldgt(p + L.pv);
-                        v11 = ldgt(p + L.pv + 1);
+                        r = bilerp<T, PAIR, true>(gproj + (long long)(L.a0 + i) * L.pu + (long long)kv * L.pv + ku,
+                                                  L.pv, fu, fv);
                     }
-                    const float a = fmaf(fu, v10 - v00, v00);
-                    const float b = fmaf(fu, v11 - v01, v01);
-                    acc[j] = fmaf(fmaf(fv, b - a, a), w, acc[j]);
+                    acc[j] = fmaf(r, w, acc[j]);
                     nu += W.nu.z;
                     nv += W.nv.z;
                     dn += W.den.z;
@@ -582,8 +684,9 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
 template <typename T, int KIND, int KER, bool CIRC>
 b2t_status launch_one(const BPTmaLaunch &L, const b2t_dims3d &d, cudaStream_t s)
 {
+    using E = elem_t<T, sizeof(T) == 2>;
     const size_t smem =
-        (size_t)ring_rows<T>() * tile_bu<T>() * sizeof(T) + BPT_SLOTS * (2 * sizeof(uint64_t) + sizeof(StageInfo));
+        (size_t)ring_rows<E>() * tile_bu<E>() * sizeof(E) + BPT_SLOTS * (2 * sizeof(uint64_t) + sizeof(StageInfo));
     auto kern = bp3d_tma_kernel<T, KIND, KER, CIRC>;
     B2T_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                  "bp3d_tma smem attribute");
@@ -609,20 +712,21 @@ b2t_status launch_kind(const BPTmaLaunch &L, int kind, int ker, bool circ, const
 
 }  // namespace
 
-b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *padded, void *vol, size_t vol_pitch,
-                    int32_t dtype, int32_t mode, cudaStream_t s)
+b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *padded, bool pairs, void *vol,
+                    size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s)
 {
     const b2t_dims3d &d = g->dims;
-    const size_t esz = dtype_size(dtype);
+    if (pairs != (dtype != B2T_F32))
+        return fail(B2T_ERR_INVALID_ARG, "bp3d_tma: 16-bit projections in the pair layout, FP32 as texels");
+    const size_t esz = padded_elem_size(dtype, pairs);  // 4 bytes: FP32 texels or 16-bit pairs
     const size_t pu = padded_pu(d.det_u);
     BPTmaLaunch *Lp = new BPTmaLaunch;
     BPTmaLaunch &L = *Lp;
     const uint64_t dims[3] = {pu, d.angles, (uint64_t)d.det_v + 4};
     const uint64_t strides[2] = {pu * esz, pu * esz * d.angles};
-    const uint32_t box[3] = {(uint32_t)(esz == 4 ? tile_bu<float>() : tile_bu<__half>()), 1u, (uint32_t)BPT_CHUNK};
-    const CUtensorMapDataType tdt = (dtype == B2T_F32) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
-                                    : (dtype == B2T_F16) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
-                                                         : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const uint32_t box[3] = {(uint32_t)tile_bu<float>(), 1u, (uint32_t)BPT_CHUNK};
+    // a pair is moved as one 32-bit element (a TMA copy does no arithmetic)
+    const CUtensorMapDataType tdt = pairs ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     b2t_status st = encode_tensor_map(&L.tmap, tdt, 3, padded, dims, strides, box);
     if (st != B2T_OK) {
         delete Lp;
@@ -636,6 +740,7 @@ b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *p
     L.nx = d.vol_x; L.ny = d.vol_y; L.nz = d.vol_z;
     L.nu = d.det_u; L.nv = d.det_v; L.na = d.angles;
     L.out_scale = out_scale;
+    L.tile_row_bytes = (uint32_t)(tile_bu<float>() * esz);
     const int kker = (ker == B2T_KER_FDK_WEIGHTING) ? B2T_KER_DEFAULT : ker;
     for (uint32_t c0 = 0; c0 < d.angles && st == B2T_OK; c0 += BPT_MAX_VIEWS) {
         const uint32_t cn = std::min(d.angles - c0, (uint32_t)BPT_MAX_VIEWS);

@@ -707,20 +707,25 @@ b2t_status fdk_impl(const b2t_geom3d *g, const b2t_filter_config *filter, int32_
     if (proj_pitch == 0) proj_pitch = d.det_u;
     if (vol_pitch == 0) vol_pitch = d.vol_x;
     if (proj_pitch < d.det_u || vol_pitch < d.vol_x) return fail(B2T_ERR_INVALID_ARG, "b2t_fdk: pitch below row length");
-    // filtered projections go straight into the zero-padded BP input
-    Scratch sp;
-    const size_t bytes = padded_proj_bytes(d, dtype);
-    B2T_TRY(sp.alloc(bytes, s, "b2t_fdk scratch (filtered projections)"));
-    B2T_CUDA_TRY(cudaMemsetAsync(sp.as<void>(), 0, bytes, s), "b2t_fdk memset");
-    const long long pu = (long long)padded_pu(d.det_u);
-    const long long pv = pu * d.angles;
-    char *interior = sp.as<char>() + (2 * pv + 2) * dtype_size(dtype);
-    B2T_TRY(run_weight_filter(g, filter, short_scan, proj, proj_pitch, interior, pu, pv, dtype, s));
     b2t_params3d p;
     p.det_supersample = 1;
     p.voxel_supersample = 1;
     p.output_scale = output_scale;
     p.kernel = B2T_KER_FDK_WEIGHTING;
+    // filtered projections go straight into the zero-padded BP input; in
+    // the pair layout the filter writes each row's texels into the second
+    // half of the row, which pairs_in_place then rewrites as pairs
+    const bool pairs = bp_pairs(dtype, &p);
+    Scratch sp;
+    const size_t bytes = padded_proj_bytes(d, dtype, pairs);
+    B2T_TRY(sp.alloc(bytes, s, "b2t_fdk scratch (filtered projections)"));
+    B2T_CUDA_TRY(cudaMemsetAsync(sp.as<void>(), 0, bytes, s), "b2t_fdk memset");
+    // (rows and slices in texels of dtype)
+    const long long pu = (long long)padded_pu(d.det_u);
+    const long long row = pairs ? 2 * pu : pu, pv = row * d.angles;
+    char *interior = sp.as<char>() + (2 * pv + (pairs ? pu : 0) + 2) * (long long)dtype_size(dtype);
+    B2T_TRY(run_weight_filter(g, filter, short_scan, proj, proj_pitch, interior, row, pv, dtype, s));
+    if (pairs) B2T_TRY(pairs_in_place(sp.as<void>(), d, dtype, s));
     return bp3d_from_padded(g, &p, sp.as<void>(), vol, vol_pitch, dtype, mode, s);
 }
 

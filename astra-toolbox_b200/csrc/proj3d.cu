@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <type_traits>
 #include <vector>
 
 #include "b2t_internal.h"
@@ -144,6 +145,57 @@ __global__ void pad_proj(const T *__restrict__ src, size_t src_pitch, int nu, in
     T val = from_float<T>(0.0f);
     if (su >= 0 && su < nu && sv >= 0 && sv < nv) val = src[((size_t)sv * na + a) * src_pitch + su];
     dst[((size_t)v * na + a) * pu + u] = val;
+}
+
+// The same in the pair layout of 16-bit texels: dst[v+2][a][u] is the word
+// (x[u], x[u+1]) of the padded row x (x past the row's end zero).
+template <typename T, typename T2>
+__global__ void pad_proj_pairs(const T *__restrict__ src, size_t src_pitch, int nu, int na, int nv, int pu,
+                               T2 *__restrict__ dst)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = blockIdx.y;
+    const int v = blockIdx.z;
+    if (u >= pu) return;
+    const int su = u - 2, sv = v - 2;
+    T x0 = from_float<T>(0.0f), x1 = from_float<T>(0.0f);
+    if (sv >= 0 && sv < nv) {
+        const T *row = src + ((size_t)sv * na + a) * src_pitch;
+        if (su >= 0 && su < nu) x0 = row[su];
+        if (su + 1 >= 0 && su + 1 < nu) x1 = row[su + 1];
+    }
+    T2 w;
+    w.x = x0;
+    w.y = x1;
+    dst[((size_t)v * na + a) * pu + u] = w;
+}
+
+// Rows (v, a), v in [2, nv + 2), of a pair-layout buffer whose 16-bit texels
+// x were written into the second half of each row (elements pu + u of a row
+// of 2 pu), rewritten in place as pairs.  One CTA per row walks it in
+// ascending tiles, reading a tile's texels before writing its pairs: pair u
+// lands on elements 2u, 2u + 1, which hold texels 2u - pu and 2u + 1 - pu,
+// below u, so a tile's writes reach only texels of tiles already done (or of
+// itself, on the row's last tile, after its reads).
+template <typename T, typename T2>
+__global__ void __launch_bounds__(256) pairs_in_place_kernel(T *buf, int na, int pu)
+{
+    const size_t m = (size_t)(blockIdx.y + 2) * na + blockIdx.x;
+    T *row = buf + m * 2 * (size_t)pu;
+    T2 *out = reinterpret_cast<T2 *>(row);
+    for (int base = 0; base < pu; base += blockDim.x) {
+        const int u = base + threadIdx.x;
+        T2 w;
+        w.x = from_float<T>(0.0f);
+        w.y = from_float<T>(0.0f);
+        if (u < pu) {
+            w.x = row[pu + u];
+            if (u + 1 < pu) w.y = row[pu + u + 1];
+        }
+        __syncthreads();
+        if (u < pu) out[u] = w;
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -446,11 +498,21 @@ b2t_status pad_volumes_f32(const float *vol, size_t pitch, const b2t_dims3d &d, 
 namespace {
 
 template <typename T>
-b2t_status pad_projections(const void *proj, size_t pitch, const b2t_dims3d &d, void *pp,
+b2t_status pad_projections(const void *proj, size_t pitch, const b2t_dims3d &d, void *pp, bool pairs,
                            cudaStream_t s)
 {
     const int pu = (int)padded_pu(d.det_u);
     dim3 grid((pu + 127) / 128, d.angles, d.det_v + 4);
+    if constexpr (sizeof(T) == 2) {
+        if (pairs) {
+            using T2 = typename std::conditional<std::is_same<T, __half>::value, __half2, __nv_bfloat162>::type;
+            pad_proj_pairs<T, T2><<<grid, 128, 0, s>>>(static_cast<const T *>(proj), pitch, d.det_u, d.angles,
+                                                       d.det_v, pu, static_cast<T2 *>(pp));
+            count_launches(1);
+            B2T_CUDA_TRY(cudaGetLastError(), "pad_proj_pairs launch");
+            return B2T_OK;
+        }
+    }
     pad_proj<T><<<grid, 128, 0, s>>>(static_cast<const T *>(proj), pitch, d.det_u, d.angles, d.det_v, pu,
                                      static_cast<T *>(pp));
     count_launches(1);
@@ -809,21 +871,45 @@ b2t_status bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *pro
     if (vol_pitch < d.vol_x || proj_pitch < d.det_u)
         return fail(B2T_ERR_INVALID_ARG, "b2t_bp3d: pitch below row length");
 
+    const bool pairs = bp_pairs(dtype, p);
     Scratch sp;
-    B2T_TRY(sp.alloc(padded_proj_bytes(d, dtype), s, "b2t_bp3d scratch (padded projections)"));
-    if (dtype == B2T_F32) B2T_TRY(pad_projections<float>(proj, proj_pitch, d, sp.as<void>(), s));
-    else if (dtype == B2T_F16) B2T_TRY(pad_projections<__half>(proj, proj_pitch, d, sp.as<void>(), s));
-    else B2T_TRY(pad_projections<__nv_bfloat16>(proj, proj_pitch, d, sp.as<void>(), s));
+    B2T_TRY(sp.alloc(padded_proj_bytes(d, dtype, pairs), s, "b2t_bp3d scratch (padded projections)"));
+    if (dtype == B2T_F32) B2T_TRY(pad_projections<float>(proj, proj_pitch, d, sp.as<void>(), false, s));
+    else if (dtype == B2T_F16) B2T_TRY(pad_projections<__half>(proj, proj_pitch, d, sp.as<void>(), pairs, s));
+    else B2T_TRY(pad_projections<__nv_bfloat16>(proj, proj_pitch, d, sp.as<void>(), pairs, s));
     return bp3d_from_padded(g, p, sp.as<void>(), vol, vol_pitch, dtype, mode, s);
 }
 
-size_t padded_proj_bytes(const b2t_dims3d &d, int32_t dtype)
+bool bp_pairs(int32_t dtype, const b2t_params3d *p)
 {
-    return padded_pu(d.det_u) * d.angles * (size_t)(d.det_v + 4) * dtype_size(dtype);
+    return dtype != B2T_F32 && p->voxel_supersample == 1 && !force_simple_bp();
 }
 
-// BP from a zero-padded projection buffer [v+2][angle][u+2] (pitch det_u + 4,
-// border of 2 texels in u and v), already validated by the caller.
+size_t padded_proj_bytes(const b2t_dims3d &d, int32_t dtype, bool pairs)
+{
+    return padded_pu(d.det_u) * d.angles * (size_t)(d.det_v + 4) * padded_elem_size(dtype, pairs);
+}
+
+b2t_status pairs_in_place(void *padded, const b2t_dims3d &d, int32_t dtype, cudaStream_t s)
+{
+    const int pu = (int)padded_pu(d.det_u);
+    const dim3 grid(d.angles, d.det_v);
+    if (dtype == B2T_F16)
+        pairs_in_place_kernel<__half, __half2><<<grid, 256, 0, s>>>(static_cast<__half *>(padded), (int)d.angles, pu);
+    else if (dtype == B2T_BF16)
+        pairs_in_place_kernel<__nv_bfloat16, __nv_bfloat162>
+            <<<grid, 256, 0, s>>>(static_cast<__nv_bfloat16 *>(padded), (int)d.angles, pu);
+    else
+        return fail(B2T_ERR_INVALID_ARG, "pairs_in_place: the pair layout holds 16-bit texels");
+    count_launches(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "pairs_in_place launch");
+    return B2T_OK;
+}
+
+// BP from a zero-padded projection buffer [v+2][angle][u+2] (pitch
+// padded_pu(det_u), border of 2 texels in u and v; pairs of texels when
+// bp_pairs(dtype, p)), already validated by the caller.  The direct-load
+// kernels below read the texel layout, which bp_pairs selects for them.
 b2t_status bp3d_from_padded(const b2t_geom3d *g, const b2t_params3d *p, const void *padded, void *vol,
                             size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s)
 {
@@ -837,7 +923,7 @@ b2t_status bp3d_from_padded(const b2t_geom3d *g, const b2t_params3d *p, const vo
         const float outs = (g->kind == B2T_GEOM_CONE && ker == B2T_KER_FDK_WEIGHTING)
                                ? p->output_scale / vs0[0]
                                : p->output_scale * (vs0[0] * vs0[1] * vs0[2]);
-        return bp3d_tma(g, ker, outs, padded, vol, vol_pitch, dtype, mode, s);
+        return bp3d_tma(g, ker, outs, padded, bp_pairs(dtype, p), vol, vol_pitch, dtype, mode, s);
     }
     BPLaunch *Lp = new BPLaunch;
     BPLaunch &L = *Lp;

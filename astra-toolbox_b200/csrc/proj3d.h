@@ -68,8 +68,9 @@ struct BPLaunch {
 constexpr int BPT_Z = 32;             // voxels per thread along z
 constexpr int BPT_CHUNK = 8;          // tile rows per TMA box; a view loads the chunks its footprint needs
 constexpr int BPT_BV = 96;            // most rows one view's tile may take
-constexpr int BPT_RING_BYTES = 96768; // ring of tile rows (288 f32 rows of 84, 544 f16/bf16 rows of 88);
-                                      // two CTAs of ring + records fit an SM's 228 KB
+constexpr int BPT_RING_BYTES = 112896; // ring of tile rows (336 rows of 84 4-byte elements: FP32 texels or
+                                       // 16-bit pairs); two CTAs of ring + records (and the 1 KB each
+                                       // reserves) fit an SM's 228 KB
 constexpr int BPT_CTAS_PER_SM = 2;    // resident CTAs (96 registers a thread with 32 accumulators)
 constexpr int BPT_SLOTS = 8;          // views in flight at most (barrier pairs and stage records)
 constexpr int BPT_MAX_VIEWS = 640;
@@ -84,6 +85,7 @@ struct alignas(64) BPTmaLaunch {
     int nx, ny, nz, nu, nv, na;
     int a0, nviews, accumulate;
     float out_scale;
+    uint32_t tile_row_bytes;  // bytes per ring row (a launch value: see the kernel's addressing)
     BPView views[BPT_MAX_VIEWS];
 };
 
@@ -92,8 +94,14 @@ struct alignas(64) BPTmaLaunch {
 // for TMA in every storage type.
 inline size_t padded_pu(uint32_t det_u) { return ((size_t)det_u + 4 + 7) & ~(size_t)7; }
 
-b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *padded, void *vol, size_t vol_pitch,
-                    int32_t dtype, int32_t mode, cudaStream_t s);
+// Bytes per element of the padded projection buffer.  16-bit projections
+// bound for the TMA backprojector use the pair layout: element u of a row is
+// the 32-bit word (x[u], x[u+1]) (x past the row's end zero); every other
+// case stores the texels themselves.
+inline size_t padded_elem_size(int32_t dtype, bool pairs) { return (pairs || dtype == B2T_F32) ? 4 : 2; }
+
+b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *padded, bool pairs, void *vol,
+                    size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status device_errors_impl(uint32_t *flags);
 b2t_status bp_path_stats_impl(uint64_t *stats);
 // One warp waits, bounded by limit cycles, for an mbarrier phase (which 0) or
@@ -173,7 +181,17 @@ b2t_status fp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *vol
                      void *proj, size_t proj_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *proj, size_t proj_pitch,
                      void *vol, size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
-size_t padded_proj_bytes(const b2t_dims3d &d, int32_t dtype);
+// Whether the padded projections of a backprojection with these parameters
+// use the pair layout (padded_elem_size).
+bool bp_pairs(int32_t dtype, const b2t_params3d *p);
+size_t padded_proj_bytes(const b2t_dims3d &d, int32_t dtype, bool pairs);
+// Pair layout from rows written as 16-bit texels (dtype F16 or BF16): row m
+// of the buffer (pitch 2 pu texels) holds its pu padded texels in its second
+// half, texels pu .. 2 pu - 1; rows v in [2, det_v + 2) are rewritten in
+// place as pairs.
+b2t_status pairs_in_place(void *padded, const b2t_dims3d &d, int32_t dtype, cudaStream_t s);
+// BP from a zero-padded projection buffer in the layout bp_pairs(dtype, p)
+// names.
 b2t_status bp3d_from_padded(const b2t_geom3d *g, const b2t_params3d *p, const void *padded, void *vol,
                             size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *proj,

@@ -216,7 +216,7 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
     if (R.op == Op::fdk) {
         b2t_dims3d db = d;
         db.angles = R.block;
-        B2T_TRY(padded.alloc(padded_proj_bytes(db, B2T_F32), cs.s, "streamed FDK filtered block"));
+        B2T_TRY(padded.alloc(padded_proj_bytes(db, B2T_F32, false), cs.s, "streamed FDK filtered block"));
     }
     // the copy streams touch the buffers only after their allocation
     B2T_CUDA_TRY(cudaEventCreateWithFlags(&allocated.e, cudaEventDisableTiming), "event create");
@@ -303,7 +303,7 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
                 B2T_TRY(bp3d_impl(&sub.g, &R.params, inb[ib].f(), 0, obuf, 0, B2T_F32, mode, cs.s));
             } else {
                 sub.set(G, c0, cn, o0, on);
-                const size_t pbytes = padded_proj_bytes(sub.g.dims, B2T_F32);
+                const size_t pbytes = padded_proj_bytes(sub.g.dims, B2T_F32, false);
                 B2T_CUDA_TRY(cudaMemsetAsync(padded.p, 0, pbytes, cs.s), "FDK block clear");
                 const long long pu = (long long)padded_pu(d.det_u), pv = pu * cn;
                 float *interior = padded.f() + 2 * pv + 2;

@@ -50,6 +50,23 @@ def test_fdk_vs_oracle(astra, orc, short):
     assert rel_l2(rec.cpu().numpy(), ref) < 1e-5
 
 
+@pytest.mark.parametrize("dtype,tol", [("float16", 2e-3), ("bfloat16", 1.5e-2)])
+def test_fdk_16bit_storage(astra, orc, dtype, tol):
+    """FDK of 16-bit projections: the filtered rows are stored in 16 bits,
+    in the pair layout of the TMA backprojector (written into the second
+    half of each row, then rewritten in place as pairs).  Against the oracle
+    on the same (16-bit rounded) projections, at the storage precision."""
+    P, pr = _setup(astra, nu=60)
+    vol = np.random.default_rng(5).random(pr.vol_shape, dtype=np.float32)
+    tp = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(torch.from_numpy(vol).cuda(), tp)
+    th = tp.to(getattr(torch, dtype))
+    rec = torch.zeros(pr.vol_shape, device='cuda', dtype=th.dtype)
+    P.fdk(pr, th, rec)
+    ref = orc.fdk(pr.geom.views_array(), th.float().cpu().numpy(), pr.vol_shape, pr.geom.vol_scale)
+    assert rel_l2(rec.float().cpu().numpy(), ref) < tol
+
+
 def test_fdk_no_filter_and_unsupported_filter(astra, orc):
     P, pr = _setup(astra)
     proj = np.random.default_rng(3).random(pr.proj_shape, dtype=np.float32)

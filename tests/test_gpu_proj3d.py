@@ -265,11 +265,14 @@ def _bp_path_stats():
     return list(st)
 
 
+@pytest.mark.parametrize("dtype", ["float32", "float16", "bfloat16"])
 @pytest.mark.parametrize("geom", ["c2_like", "high_mag", "cone_vec", "par3d"])
-def test_tma_bp_matches_direct_bp(astra, geom, monkeypatch):
+def test_tma_bp_matches_direct_bp(astra, geom, dtype, monkeypatch):
     """The TMA-staged BP (default) and the direct-load BP implement the same
     model; includes a high-magnification case whose tiles overflow the stage
-    (fallback path) and a non-circular cone_vec case."""
+    (fallback path) and a non-circular cone_vec case.  16-bit projections
+    reach the TMA path in the pair layout (two texels per 32-bit word) and the
+    direct path as texels."""
     if geom == "c2_like":
         ang = np.linspace(0, 2 * np.pi, 90, endpoint=False).astype(np.float32)
         vg = astra.create_vol_geom(96, 96, 80)
@@ -285,8 +288,9 @@ def test_tma_bp_matches_direct_bp(astra, geom, monkeypatch):
         vg = astra.create_vol_geom(70, 60, 50)
         pg = astra.create_proj_geom('parallel3d', 1.0, 1.0, 60, 80, ang)
     pr = _proj(astra, vg, pg)
-    proj = torch.from_numpy(np.random.default_rng(11).random(pr.proj_shape, dtype=np.float32)).cuda()
-    a = torch.zeros(pr.vol_shape, device='cuda')
+    tdt = getattr(torch, dtype)
+    proj = torch.from_numpy(np.random.default_rng(11).random(pr.proj_shape, dtype=np.float32)).cuda().to(tdt)
+    a = torch.zeros(pr.vol_shape, device='cuda', dtype=tdt)
     _bp_path_stats()
     pr.bp(proj, a)
     assert _device_errors() == 0
@@ -306,13 +310,16 @@ def test_tma_bp_matches_direct_bp(astra, geom, monkeypatch):
     else:
         assert fast == 0  # non-circular orbit: general path only
     monkeypatch.setenv("B2T_SIMPLE_BP", "1")
-    b = torch.zeros(pr.vol_shape, device='cuda')
+    b = torch.zeros(pr.vol_shape, device='cuda', dtype=tdt)
     pr.bp(proj, b)
     monkeypatch.delenv("B2T_SIMPLE_BP")
     # the TMA path takes v at voxel j of a 32-voxel column as v0 + j dv from
     # per-block folded coefficients (rounded to FP32 once); the direct path
     # projects every voxel from the view's coefficients
-    assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 4e-6
+    # (16-bit outputs: the two sums round to neighbouring 16-bit values now
+    # and then)
+    tol = {"float32": 4e-6, "float16": 1e-4, "bfloat16": 8e-4}[dtype]
+    assert rel_l2(a.float().cpu().numpy(), b.float().cpu().numpy()) < tol
 
 
 @pytest.mark.parametrize("idx", range(6))
