@@ -18,7 +18,10 @@
 //     geometries (detector v axis along z) the detector u coordinate and the
 //     ray-density weight do not depend on z, so each thread computes them once
 //     per view (from affine forms the producer folds per block) and only v
-//     changes along its 32-voxel column;
+//     changes along its 32-voxel column; voxels j and j + 1 of the column
+//     share packed f32x2 instructions (sm_100a), and 16-bit projections are
+//     staged as pairs of vertically adjacent texels, so that a sample takes
+//     two 32-bit shared loads and one packed 16-bit interpolation along u;
 //   - a tile that does not fit (extreme magnification) is read from the padded
 //     projections in global memory instead.
 //
@@ -91,18 +94,18 @@ template <typename T, int OFF> __device__ __forceinline__ float lds_sh(uint32_t 
     return v;
 }
 
-// A pair of 16-bit texels (x[u], x[u+1]) in one 32-bit word, as two floats.
-template <typename T> __device__ __forceinline__ float2 pair_f2(uint32_t v)
+// A pair of 16-bit texels in one 32-bit word, as two floats.
+template <typename T, typename E> __device__ __forceinline__ float2 pair_f2(E v)
 {
-    if constexpr (std::is_same<T, __half>::value) return __half22float2(*reinterpret_cast<const __half2 *>(&v));
-    else return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&v));
+    if constexpr (std::is_same<T, __half>::value) return __half22float2(v);
+    else return __bfloat1622float2(v);
 }
-// The pair at 32-bit shared address a + OFF.
-template <typename T, int OFF> __device__ __forceinline__ float2 lds_pair(uint32_t a)
+// The 32-bit word at shared address a + OFF.
+template <int OFF> __device__ __forceinline__ uint32_t lds_b32(uint32_t a)
 {
     uint32_t v;
     asm volatile("ld.shared.b32 %0, [%1+%2];" : "=r"(v) : "r"(a), "n"(OFF));
-    return pair_f2<T>(v);
+    return v;
 }
 
 // Two FP32 values in one 64-bit register, and the packed f32x2 arithmetic of
@@ -146,10 +149,12 @@ __device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b)
 }
 
 // Storage of the padded projections the kernel reads: FP32 texels, or for
-// the 16-bit types the pair layout (padded_elem_size), whose element u of a
-// row is the 32-bit word (x[u], x[u+1]).  A bilinear sample then takes one
-// 32-bit load per row instead of two 16-bit ones, and half the
-// shared-memory wavefronts; the arithmetic (in FP32) is the texel form's.
+// the 16-bit types the pair layout (padded_elem_size), whose element (v, u)
+// is the 32-bit word (x[v][u], x[v+1][u]), a texel and the one below it.  A
+// bilinear sample then takes two 32-bit loads from one row of pairs (columns
+// u and u + 1) instead of four 16-bit loads, half the shared-memory
+// wavefronts, and the interpolation along u of both rows is one packed
+// 16-bit fused multiply-add.
 template <typename T, bool PAIR> struct Elem {
     using type = T;
 };
@@ -161,6 +166,14 @@ template <> struct Elem<__nv_bfloat16, true> {
 };
 template <typename T, bool PAIR> using elem_t = typename Elem<T, PAIR>::type;
 
+// x in both halves of a 16-bit pair (x itself for FP32).
+template <typename T> __device__ __forceinline__ elem_t<T, true> splat2(float x)
+{
+    if constexpr (std::is_same<T, __half>::value) return __float2half2_rn(x);
+    else if constexpr (std::is_same<T, __nv_bfloat16>::value) return __float2bfloat162_rn(x);
+    else return x;
+}
+
 // Bilinear sample with weights fu (along u) and fv (along v) from element p
 // of shared memory (GLOBAL false) or of the padded projections in global
 // memory, rows rs elements apart.
@@ -169,14 +182,12 @@ __device__ __forceinline__ float bilerp(const elem_t<T, PAIR> *p, long long rs, 
 {
     float v00, v10, v01, v11;
     if constexpr (PAIR) {
-        using E = elem_t<T, PAIR>;
-        const E e0 = GLOBAL ? __ldg(p) : *p, e1 = GLOBAL ? __ldg(p + rs) : p[rs];
-        const float2 r0 = pair_f2<T>(*reinterpret_cast<const uint32_t *>(&e0));
-        const float2 r1 = pair_f2<T>(*reinterpret_cast<const uint32_t *>(&e1));
-        v00 = r0.x;
-        v10 = r0.y;
-        v01 = r1.x;
-        v11 = r1.y;
+        // columns u and u + 1 of the pair row (rs unused)
+        const float2 c0 = pair_f2<T>(GLOBAL ? __ldg(p) : p[0]), c1 = pair_f2<T>(GLOBAL ? __ldg(p + 1) : p[1]);
+        v00 = c0.x;
+        v01 = c0.y;
+        v10 = c1.x;
+        v11 = c1.y;
     } else {
         v00 = GLOBAL ? ldgt(p) : lds(p);
         v10 = GLOBAL ? ldgt(p + 1) : lds(p + 1);
@@ -513,31 +524,41 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
                 // operations; each half rounds as the scalar texel form
                 // fmaf(fv, b - a, a), a = fmaf(fu, v10 - v00, v00), ...
                 const uint64_t dV2 = pk2(dV, dV), Vq2 = pk2(Vq, Vq), w2 = pk2(w, w), fu2 = pk2(fu, fu);
-                const uint64_t M2 = pk2(M, M), nM2 = pk2(-M, -M);
+                const uint64_t M2 = pk2(M, M), nM2 = pk2(-M, -M), two2 = pk2(2.0f, 2.0f);
+                // (j, j + 1), stepped by exact additions (the literal pairs
+                // would take two register moves each)
+                uint64_t j2 = pk2(0.0f, 1.0f);
+                using H2 = elem_t<T, true>;
+                const H2 fuh = splat2<T>(fu);  // 16-bit pairs: fu for the packed interpolation along u
 #pragma unroll
-                for (int j = 0; j < BPT_Z; j += 2) {
-                    const uint64_t q2 = fma2(pk2((float)j, (float)(j + 1)), dV2, Vq2);
+                for (int j = 0; j < BPT_Z; j += 2, j2 = add2(j2, two2)) {
+                    const uint64_t q2 = fma2(j2, dV2, Vq2);
                     const uint64_t t2 = add2_rd(q2, M2);
                     const uint64_t fv2 = sub2(q2, add2(t2, nM2));
                     const float2 t = upk2(t2);
                     const uint32_t a0 = (uint32_t)__float_as_int(t.x) * rowb + abase;
                     const uint32_t a1 = (uint32_t)__float_as_int(t.y) * rowb + abase;
-                    uint64_t v00, v10, v01, v11;
+                    uint64_t av, bv;
                     if constexpr (PAIR) {
-                        const float2 p0 = lds_pair<T, 0>(a0), p1 = lds_pair<T, 0>(a1);
-                        const float2 q0 = lds_pair<T, (int)ROWB>(a0), q1 = lds_pair<T, (int)ROWB>(a1);
-                        v00 = pk2(p0.x, p1.x);
-                        v10 = pk2(p0.y, p1.y);
-                        v01 = pk2(q0.x, q1.x);
-                        v11 = pk2(q0.y, q1.y);
+                        // (a, b) = (v00, v01) + fu ((v10, v11) - (v00, v01))
+                        // in 16-bit arithmetic, then the blend along v in FP32
+                        float2 ab[2];
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const uint32_t c0 = lds_b32<0>(h ? a1 : a0), c1 = lds_b32<4>(h ? a1 : a0);
+                            const H2 x0 = *reinterpret_cast<const H2 *>(&c0), x1 = *reinterpret_cast<const H2 *>(&c1);
+                            ab[h] = pair_f2<T>(__hfma2(fuh, __hsub2(x1, x0), x0));
+                        }
+                        av = pk2(ab[0].x, ab[1].x);
+                        bv = pk2(ab[0].y, ab[1].y);
                     } else {
-                        v00 = pk2(lds_sh<T, 0>(a0), lds_sh<T, 0>(a1));
-                        v10 = pk2(lds_sh<T, 4>(a0), lds_sh<T, 4>(a1));
-                        v01 = pk2(lds_sh<T, (int)ROWB>(a0), lds_sh<T, (int)ROWB>(a1));
-                        v11 = pk2(lds_sh<T, (int)ROWB + 4>(a0), lds_sh<T, (int)ROWB + 4>(a1));
+                        const uint64_t v00 = pk2(lds_sh<T, 0>(a0), lds_sh<T, 0>(a1));
+                        const uint64_t v10 = pk2(lds_sh<T, 4>(a0), lds_sh<T, 4>(a1));
+                        const uint64_t v01 = pk2(lds_sh<T, (int)ROWB>(a0), lds_sh<T, (int)ROWB>(a1));
+                        const uint64_t v11 = pk2(lds_sh<T, (int)ROWB + 4>(a0), lds_sh<T, (int)ROWB + 4>(a1));
+                        av = fma2(fu2, sub2(v10, v00), v00);
+                        bv = fma2(fu2, sub2(v11, v01), v01);
                     }
-                    const uint64_t av = fma2(fu2, sub2(v10, v00), v00);
-                    const uint64_t bv = fma2(fu2, sub2(v11, v01), v01);
                     const float2 r = upk2(fma2(fma2(fv2, sub2(bv, av), av), w2, pk2(acc[j], acc[j + 1])));
                     acc[j] = r.x;
                     acc[j + 1] = r.y;

@@ -712,20 +712,26 @@ b2t_status fdk_impl(const b2t_geom3d *g, const b2t_filter_config *filter, int32_
     p.voxel_supersample = 1;
     p.output_scale = output_scale;
     p.kernel = B2T_KER_FDK_WEIGHTING;
-    // filtered projections go straight into the zero-padded BP input; in
-    // the pair layout the filter writes each row's texels into the second
-    // half of the row, which pairs_in_place then rewrites as pairs
     const bool pairs = bp_pairs(dtype, &p);
     Scratch sp;
     const size_t bytes = padded_proj_bytes(d, dtype, pairs);
     B2T_TRY(sp.alloc(bytes, s, "b2t_fdk scratch (filtered projections)"));
-    B2T_CUDA_TRY(cudaMemsetAsync(sp.as<void>(), 0, bytes, s), "b2t_fdk memset");
-    // (rows and slices in texels of dtype)
-    const long long pu = (long long)padded_pu(d.det_u);
-    const long long row = pairs ? 2 * pu : pu, pv = row * d.angles;
-    char *interior = sp.as<char>() + (2 * pv + (pairs ? pu : 0) + 2) * (long long)dtype_size(dtype);
-    B2T_TRY(run_weight_filter(g, filter, short_scan, proj, proj_pitch, interior, row, pv, dtype, s));
-    if (pairs) B2T_TRY(pairs_in_place(sp.as<void>(), d, dtype, s));
+    if (pairs) {
+        // 16-bit pair layout (each element holds a texel and the one below
+        // it): filtered rows into a texel buffer, then paired
+        Scratch st;
+        B2T_TRY(st.alloc((size_t)d.det_u * d.angles * d.det_v * dtype_size(dtype), s,
+                         "b2t_fdk scratch (filtered rows)"));
+        B2T_TRY(run_weight_filter(g, filter, short_scan, proj, proj_pitch, st.as<void>(), (long long)d.det_u,
+                                  (long long)d.det_u * d.angles, dtype, s));
+        B2T_TRY(pad_projections_impl(st.as<void>(), d.det_u, d, sp.as<void>(), dtype, true, s));
+    } else {
+        // filtered projections straight into the zero-padded BP input
+        B2T_CUDA_TRY(cudaMemsetAsync(sp.as<void>(), 0, bytes, s), "b2t_fdk memset");
+        const long long pu = (long long)padded_pu(d.det_u), pv = pu * d.angles;
+        char *interior = sp.as<char>() + (2 * pv + 2) * (long long)dtype_size(dtype);
+        B2T_TRY(run_weight_filter(g, filter, short_scan, proj, proj_pitch, interior, pu, pv, dtype, s));
+    }
     return bp3d_from_padded(g, &p, sp.as<void>(), vol, vol_pitch, dtype, mode, s);
 }
 

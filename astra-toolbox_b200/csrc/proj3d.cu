@@ -147,8 +147,9 @@ __global__ void pad_proj(const T *__restrict__ src, size_t src_pitch, int nu, in
     dst[((size_t)v * na + a) * pu + u] = val;
 }
 
-// The same in the pair layout of 16-bit texels: dst[v+2][a][u] is the word
-// (x[u], x[u+1]) of the padded row x (x past the row's end zero).
+// The same in the pair layout of 16-bit texels: dst[v][a][u] is the word
+// (x[v][a][u], x[v+1][a][u]) of the padded texels x (the texel and the one
+// below it; x past the last row zero).
 template <typename T, typename T2>
 __global__ void pad_proj_pairs(const T *__restrict__ src, size_t src_pitch, int nu, int na, int nv, int pu,
                                T2 *__restrict__ dst)
@@ -159,43 +160,14 @@ __global__ void pad_proj_pairs(const T *__restrict__ src, size_t src_pitch, int 
     if (u >= pu) return;
     const int su = u - 2, sv = v - 2;
     T x0 = from_float<T>(0.0f), x1 = from_float<T>(0.0f);
-    if (sv >= 0 && sv < nv) {
-        const T *row = src + ((size_t)sv * na + a) * src_pitch;
-        if (su >= 0 && su < nu) x0 = row[su];
-        if (su + 1 >= 0 && su + 1 < nu) x1 = row[su + 1];
+    if (su >= 0 && su < nu) {
+        if (sv >= 0 && sv < nv) x0 = src[((size_t)sv * na + a) * src_pitch + su];
+        if (sv + 1 >= 0 && sv + 1 < nv) x1 = src[((size_t)(sv + 1) * na + a) * src_pitch + su];
     }
     T2 w;
     w.x = x0;
     w.y = x1;
     dst[((size_t)v * na + a) * pu + u] = w;
-}
-
-// Rows (v, a), v in [2, nv + 2), of a pair-layout buffer whose 16-bit texels
-// x were written into the second half of each row (elements pu + u of a row
-// of 2 pu), rewritten in place as pairs.  One CTA per row walks it in
-// ascending tiles, reading a tile's texels before writing its pairs: pair u
-// lands on elements 2u, 2u + 1, which hold texels 2u - pu and 2u + 1 - pu,
-// below u, so a tile's writes reach only texels of tiles already done (or of
-// itself, on the row's last tile, after its reads).
-template <typename T, typename T2>
-__global__ void __launch_bounds__(256) pairs_in_place_kernel(T *buf, int na, int pu)
-{
-    const size_t m = (size_t)(blockIdx.y + 2) * na + blockIdx.x;
-    T *row = buf + m * 2 * (size_t)pu;
-    T2 *out = reinterpret_cast<T2 *>(row);
-    for (int base = 0; base < pu; base += blockDim.x) {
-        const int u = base + threadIdx.x;
-        T2 w;
-        w.x = from_float<T>(0.0f);
-        w.y = from_float<T>(0.0f);
-        if (u < pu) {
-            w.x = row[pu + u];
-            if (u + 1 < pu) w.y = row[pu + u + 1];
-        }
-        __syncthreads();
-        if (u < pu) out[u] = w;
-        __syncthreads();
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -880,6 +852,14 @@ b2t_status bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *pro
     return bp3d_from_padded(g, p, sp.as<void>(), vol, vol_pitch, dtype, mode, s);
 }
 
+b2t_status pad_projections_impl(const void *proj, size_t pitch, const b2t_dims3d &d, void *padded, int32_t dtype,
+                                bool pairs, cudaStream_t s)
+{
+    if (dtype == B2T_F32) return pad_projections<float>(proj, pitch, d, padded, false, s);
+    if (dtype == B2T_F16) return pad_projections<__half>(proj, pitch, d, padded, pairs, s);
+    return pad_projections<__nv_bfloat16>(proj, pitch, d, padded, pairs, s);
+}
+
 bool bp_pairs(int32_t dtype, const b2t_params3d *p)
 {
     return dtype != B2T_F32 && p->voxel_supersample == 1 && !force_simple_bp();
@@ -888,22 +868,6 @@ bool bp_pairs(int32_t dtype, const b2t_params3d *p)
 size_t padded_proj_bytes(const b2t_dims3d &d, int32_t dtype, bool pairs)
 {
     return padded_pu(d.det_u) * d.angles * (size_t)(d.det_v + 4) * padded_elem_size(dtype, pairs);
-}
-
-b2t_status pairs_in_place(void *padded, const b2t_dims3d &d, int32_t dtype, cudaStream_t s)
-{
-    const int pu = (int)padded_pu(d.det_u);
-    const dim3 grid(d.angles, d.det_v);
-    if (dtype == B2T_F16)
-        pairs_in_place_kernel<__half, __half2><<<grid, 256, 0, s>>>(static_cast<__half *>(padded), (int)d.angles, pu);
-    else if (dtype == B2T_BF16)
-        pairs_in_place_kernel<__nv_bfloat16, __nv_bfloat162>
-            <<<grid, 256, 0, s>>>(static_cast<__nv_bfloat16 *>(padded), (int)d.angles, pu);
-    else
-        return fail(B2T_ERR_INVALID_ARG, "pairs_in_place: the pair layout holds 16-bit texels");
-    count_launches(1);
-    B2T_CUDA_TRY(cudaGetLastError(), "pairs_in_place launch");
-    return B2T_OK;
 }
 
 // BP from a zero-padded projection buffer [v+2][angle][u+2] (pitch

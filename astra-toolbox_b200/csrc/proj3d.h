@@ -95,9 +95,9 @@ struct alignas(64) BPTmaLaunch {
 inline size_t padded_pu(uint32_t det_u) { return ((size_t)det_u + 4 + 7) & ~(size_t)7; }
 
 // Bytes per element of the padded projection buffer.  16-bit projections
-// bound for the TMA backprojector use the pair layout: element u of a row is
-// the 32-bit word (x[u], x[u+1]) (x past the row's end zero); every other
-// case stores the texels themselves.
+// bound for the TMA backprojector use the pair layout: element (v, a, u) is
+// the 32-bit word (x[v][a][u], x[v+1][a][u]), the texel and the one below it
+// (x past the last row zero); every other case stores the texels themselves.
 inline size_t padded_elem_size(int32_t dtype, bool pairs) { return (pairs || dtype == B2T_F32) ? 4 : 2; }
 
 b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *padded, bool pairs, void *vol,
@@ -185,11 +185,10 @@ b2t_status bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *pro
 // use the pair layout (padded_elem_size).
 bool bp_pairs(int32_t dtype, const b2t_params3d *p);
 size_t padded_proj_bytes(const b2t_dims3d &d, int32_t dtype, bool pairs);
-// Pair layout from rows written as 16-bit texels (dtype F16 or BF16): row m
-// of the buffer (pitch 2 pu texels) holds its pu padded texels in its second
-// half, texels pu .. 2 pu - 1; rows v in [2, det_v + 2) are rewritten in
-// place as pairs.
-b2t_status pairs_in_place(void *padded, const b2t_dims3d &d, int32_t dtype, cudaStream_t s);
+// The zero-padded projection buffer of projections proj (row pitch in
+// texels) in the layout bp_pairs selects.
+b2t_status pad_projections_impl(const void *proj, size_t pitch, const b2t_dims3d &d, void *padded, int32_t dtype,
+                                bool pairs, cudaStream_t s);
 // BP from a zero-padded projection buffer in the layout bp_pairs(dtype, p)
 // names.
 b2t_status bp3d_from_padded(const b2t_geom3d *g, const b2t_params3d *p, const void *padded, void *vol,

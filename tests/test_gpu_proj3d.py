@@ -316,9 +316,9 @@ def test_tma_bp_matches_direct_bp(astra, geom, dtype, monkeypatch):
     # the TMA path takes v at voxel j of a 32-voxel column as v0 + j dv from
     # per-block folded coefficients (rounded to FP32 once); the direct path
     # projects every voxel from the view's coefficients
-    # (16-bit outputs: the two sums round to neighbouring 16-bit values now
-    # and then)
-    tol = {"float32": 4e-6, "float16": 1e-4, "bfloat16": 8e-4}[dtype]
+    # (16-bit: the TMA path interpolates along u in 16-bit arithmetic, and
+    # the outputs round to 16 bits)
+    tol = {"float32": 4e-6, "float16": 5e-4, "bfloat16": 4e-3}[dtype]
     assert rel_l2(a.float().cpu().numpy(), b.float().cpu().numpy()) < tol
 
 
