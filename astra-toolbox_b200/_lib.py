@@ -173,6 +173,7 @@ SIGNATURES = {
     "b2t_selftest_bounded_wait": (_I32, [_I32, ctypes.c_uint64, _P]),
     "b2t_release_cached_memory": (_I32, []),
     "b2t_autotune_fp3d": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _P, _P]),
+    "b2t_autotune_bp3d": (_I32, [_P, _P, _P, _SZ, _P, _SZ, _I32, _P, _P]),
     "b2t_batch2d_create": (_I32, [_P, _I32, _P]),
     "b2t_batch2d_layout": (_I32, [_P, _P, _P, _P, _P]),
     "b2t_batch2d_fp": (_I32, [_P, _P, _P, _I32, _P]),

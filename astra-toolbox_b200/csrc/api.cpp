@@ -401,6 +401,14 @@ b2t_status b2t_autotune_fp3d(const b2t_geom3d *geom, const b2t_params3d *params,
                               vpc);
 }
 
+b2t_status b2t_autotune_bp3d(const b2t_geom3d *geom, const b2t_params3d *params, const void *proj, size_t proj_pitch,
+                             void *vol, size_t vol_pitch, int32_t dtype, void *stream, int32_t *vpt)
+{
+    clear_error();
+    return bp3d_autotune_impl(geom, params, proj, proj_pitch, vol, vol_pitch, dtype, static_cast<cudaStream_t>(stream),
+                              vpt);
+}
+
 b2t_status b2t_release_cached_memory(void)
 {
     clear_error();

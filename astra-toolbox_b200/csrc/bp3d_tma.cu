@@ -34,8 +34,13 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
-#include <type_traits>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+#include <type_traits>
 
 #include "b2t_internal.h"
 #include "proj3d.h"
@@ -48,7 +53,7 @@ namespace b2t {
 static __device__ unsigned int g_b2t_device_errors = 0;
 
 // Path statistics of the TMA backprojection, read and cleared by
-// b2t_bp_path_stats.  In voxel-column views (one thread's column of BPT_Z
+// b2t_bp_path_stats.  In voxel-column views (one thread's column of 16 or 32
 // voxels for one view): [0] the circular fast path (all samples from the
 // shared-memory tile), [1] the general path (other orbits, columns whose
 // rows leave the tile, views read from global memory), [2] lanes idle
@@ -207,16 +212,23 @@ template <typename E> __host__ __device__ constexpr int tile_bu()
     static_assert(sizeof(E) == 4, "tile elements are FP32 texels or 16-bit pairs");
     return 84;
 }
-// Ring rows (multiple of BPT_CHUNK) in the BPT_RING_BYTES of shared memory.
+// Launch shapes: voxels per thread along z (ZB) and, with them, the CTAs an
+// SM holds (the registers of ZB accumulators) and the ring each CTA gets.
+template <int ZB> struct BPShape {
+    static_assert(ZB == 16 || ZB == 32, "16 or 32 voxels per thread");
+    static constexpr int ctas = ZB == 32 ? 2 : 3;
+    static constexpr int ring_bytes = ZB == 32 ? BPT_RING_BYTES : BPT_RING_BYTES_Z16;
+};
+// Ring rows (multiple of BPT_CHUNK) in the shape's ring of shared memory.
 // An 8-row chunk is a multiple of 128 bytes, so every chunk destination (ring
 // rows are allocated in whole chunks) is 128-byte aligned.
-template <typename E> __host__ __device__ constexpr int ring_rows()
+template <typename E, int ZB> __host__ __device__ constexpr int ring_rows()
 {
-    return (BPT_RING_BYTES / (tile_bu<E>() * (int)sizeof(E))) & ~(BPT_CHUNK - 1);
+    return (BPShape<ZB>::ring_bytes / (tile_bu<E>() * (int)sizeof(E))) & ~(BPT_CHUNK - 1);
 }
 static_assert(BPT_CHUNK * 84 * 4 % 128 == 0, "chunk alignment");
 static_assert((84 * 4) % 16 == 0, "TMA box row bytes");
-static_assert(ring_rows<float>() >= BPT_BV, "the ring holds the largest view");
+static_assert(ring_rows<float, 32>() >= BPT_BV && ring_rows<float, 16>() >= BPT_BV, "the ring holds the largest view");
 
 // Per-view record written by the producer warp: the tile's origin in padded
 // texels (u0, v0), its first ring row and its row count (0: the footprint does
@@ -270,19 +282,19 @@ __device__ __forceinline__ float4 fold_form(float4 c, float4 d, double k, double
 // lands in the ring.  The views then go through the ring one at a time: the
 // warp finds room together (waiting for the oldest views to be released) and
 // the view's own lane issues the loads and writes the record.
-template <typename E, int KIND, bool CIRC>
+template <typename E, int KIND, bool CIRC, int ZB>
 __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, E *ring, uint64_t *full, uint64_t *empty,
                                         StageInfo *info, int lane, float cx,
                                         float cy, float fz0)
 {
-    constexpr int R = ring_rows<E>();
+    constexpr int R = ring_rows<E, ZB>();
     constexpr int BU = tile_bu<E>();
-    // voxel-centre extent of the block; along z the block's full BPT_Z
+    // voxel-centre extent of the block; along z the block's full ZB
     // slices, so that the voxels computed past the volume's last slice
     // (and discarded) also project inside the tile
     const float bx0 = (float)(blockIdx.x * 32) + cx, bx1 = (float)(min(L.nx, (int)blockIdx.x * 32 + 32) - 1) + cx;
     const float by0 = (float)(blockIdx.y * 8) + cy, by1 = (float)(min(L.ny, (int)blockIdx.y * 8 + 8) - 1) + cy;
-    const float bz0 = fz0, bz1 = fz0 + (float)(BPT_Z - 1);
+    const float bz0 = fz0, bz1 = fz0 + (float)(ZB - 1);
     int j0 = 0;         // oldest view still held by the compute warps
     int head = 0;       // next free ring row
     int slot_row0 = 0;  // lane s < BPT_SLOTS: first ring row of the view in slot s
@@ -421,14 +433,14 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, E *ring, uint64_t 
         (void)mbar_wait_bounded_sleep(&full[q % BPT_SLOTS], (uint32_t)((q / BPT_SLOTS) & 1), 2000000000LL);
 }
 
-// 288 threads: warps 0-7 backproject a 32 x 8 x BPT_Z voxel block, warp 8
+// 288 threads: warps 0-7 backproject a 32 x 8 x ZB voxel block, warp 8
 // streams the views' tiles into the ring ahead of them.
-template <typename T, int KIND, int KER, bool CIRC>
-__global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __grid_constant__ BPTmaLaunch L)
+template <typename T, int KIND, int KER, bool CIRC, int ZB>
+__global__ void __launch_bounds__(288, BPShape<ZB>::ctas) bp3d_tma_kernel(const __grid_constant__ BPTmaLaunch L)
 {
     constexpr bool PAIR = sizeof(T) == 2;  // 16-bit texels are stored as pairs
     using E = elem_t<T, PAIR>;
-    constexpr int R = ring_rows<E>();
+    constexpr int R = ring_rows<E, ZB>();
     constexpr int BU = tile_bu<E>();
     extern __shared__ __align__(128) unsigned char smraw[];
     E *ring = reinterpret_cast<E *>(smraw);
@@ -439,7 +451,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
-    const int z0 = blockIdx.z * BPT_Z;
+    const int z0 = blockIdx.z * ZB;
 
     if (tid == 0) {
         for (int s = 0; s < BPT_SLOTS; ++s) {
@@ -454,7 +466,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
     if (warp == 8) {
         const float cx = 0.5f - 0.5f * (float)L.nx, cy = 0.5f - 0.5f * (float)L.ny;
         const float fz0 = (float)z0 + 0.5f - 0.5f * (float)L.nz;
-        bp_produce<E, KIND, CIRC>(L, ring, full, empty, info, lane, cx, cy, fz0);
+        bp_produce<E, KIND, CIRC, ZB>(L, ring, full, empty, info, lane, cx, cy, fz0);
         return;
     }
 
@@ -467,9 +479,9 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
     // this thread's offset inside the block
     const float lx = (float)(x - (int)blockIdx.x * 32), ly = (float)(y - (int)blockIdx.y * 8);
 
-    float acc[BPT_Z];
+    float acc[ZB];
 #pragma unroll
-    for (int j = 0; j < BPT_Z; ++j) acc[j] = 0.0f;
+    for (int j = 0; j < ZB; ++j) acc[j] = 0.0f;
 
     unsigned long long n_fast = 0, n_general = 0, n_idle = 0;  // this thread's column-views by path
     const long long t_loop = clock64();
@@ -503,10 +515,10 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
             }
             const float M = 12582912.0f;  // 1.5 * 2^23: q + M rounded down holds floor(q) in its mantissa
             // q_j = Vq + j dV is monotone in j (fmaf and rounding down are
-            // monotone), so the rows of all BPT_Z voxels are inside the tile
+            // monotone), so the rows of all ZB voxels are inside the tile
             // when the first and the last are
             const int ka = __float_as_int(__fadd_rd(Vq, M)) - 0x4B400000;
-            const int kb = __float_as_int(__fadd_rd(fmaf((float)(BPT_Z - 1), dV, Vq), M)) - 0x4B400000;
+            const int kb = __float_as_int(__fadd_rd(fmaf((float)(ZB - 1), dV, Vq), M)) - 0x4B400000;
             if (min(ka, kb) >= 0 && max(ka, kb) <= hd.w - 2) {
                 const float tU = __fadd_rd(Uq, M);
                 const float fu = Uq - (tU - M);
@@ -531,7 +543,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
                 using H2 = elem_t<T, true>;
                 const H2 fuh = splat2<T>(fu);  // 16-bit pairs: fu for the packed interpolation along u
 #pragma unroll
-                for (int j = 0; j < BPT_Z; j += 2, j2 = add2(j2, two2)) {
+                for (int j = 0; j < ZB; j += 2, j2 = add2(j2, two2)) {
                     const uint64_t q2 = fma2(j2, dV2, Vq2);
                     const uint64_t t2 = add2_rd(q2, M2);
                     const uint64_t fv2 = sub2(q2, add2(t2, nM2));
@@ -575,7 +587,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
             const E *gproj = static_cast<const E *>(L.proj);
             const float fx = (float)(blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7)) + 0.5f - 0.5f * (float)L.nx;
             const float fy = (float)(blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3)) + 0.5f - 0.5f * (float)L.ny;
-            const float fz0 = (float)(blockIdx.z * BPT_Z) + 0.5f - 0.5f * (float)L.nz;
+            const float fz0 = (float)(blockIdx.z * ZB) + 0.5f - 0.5f * (float)L.nz;
             const BPView &W = L.views[i];
             const int u0 = hd.x, v0 = hd.y, nrows = hd.w;
             if (CIRC) {
@@ -601,7 +613,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
                     ku = min(max(ku, 0), BU - 2);
                     const float vofs = 1.0f - (float)v0;
 #pragma unroll
-                    for (int j = 0; j < BPT_Z; ++j) {
+                    for (int j = 0; j < ZB; ++j) {
                         int kv;
                         float fv;
                         split_texel_t(fmaf((float)j, dV, Vb) + vofs, kv, fv);
@@ -615,7 +627,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
                     split_texel_t(U - 1.0f, ku, fu);
                     ku = min(max(ku, -2), L.nu);
 #pragma unroll
-                    for (int j = 0; j < BPT_Z; ++j) {
+                    for (int j = 0; j < ZB; ++j) {
                         int kv;
                         float fv;
                         split_texel_t(fmaf((float)j, dV, Vb) - 1.0f, kv, fv);
@@ -629,7 +641,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
                 float nv = fmaf(fz0, W.nv.z, fmaf(fy, W.nv.y, fmaf(fx, W.nv.x, W.nv.w)));
                 float dn = fmaf(fz0, W.den.z, fmaf(fy, W.den.y, fmaf(fx, W.den.x, W.den.w)));
 #pragma unroll
-                for (int j = 0; j < BPT_Z; ++j) {
+                for (int j = 0; j < ZB; ++j) {
                     float U, Vc, w;
                     if (KIND == B2T_GEOM_CONE) {
                         const float fr = __frcp_rn(dn);
@@ -690,8 +702,8 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
     if (xo < L.nx && yo < L.ny) {
         T *out = static_cast<T *>(L.vol);
 #pragma unroll
-        for (int j = 0; j < BPT_Z; ++j) {
-            const int z = (int)blockIdx.z * BPT_Z + j;
+        for (int j = 0; j < ZB; ++j) {
+            const int z = (int)blockIdx.z * ZB + j;
             if (z < L.nz) {
                 T *o = out + ((size_t)z * L.ny + yo) * L.vol_pitch + xo;
                 float r = acc[j] * L.out_scale;
@@ -702,33 +714,75 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
     }
 }
 
-template <typename T, int KIND, int KER, bool CIRC>
+template <typename T, int KIND, int KER, bool CIRC, int ZB>
 b2t_status launch_one(const BPTmaLaunch &L, const b2t_dims3d &d, cudaStream_t s)
 {
     using E = elem_t<T, sizeof(T) == 2>;
-    const size_t smem =
-        (size_t)ring_rows<E>() * tile_bu<E>() * sizeof(E) + BPT_SLOTS * (2 * sizeof(uint64_t) + sizeof(StageInfo));
-    auto kern = bp3d_tma_kernel<T, KIND, KER, CIRC>;
+    const size_t smem = (size_t)ring_rows<E, ZB>() * tile_bu<E>() * sizeof(E) +
+                        BPT_SLOTS * (2 * sizeof(uint64_t) + sizeof(StageInfo));
+    auto kern = bp3d_tma_kernel<T, KIND, KER, CIRC, ZB>;
     B2T_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                  "bp3d_tma smem attribute");
-    dim3 grid((d.vol_x + 31) / 32, (d.vol_y + 7) / 8, (d.vol_z + BPT_Z - 1) / BPT_Z);
+    dim3 grid((d.vol_x + 31) / 32, (d.vol_y + 7) / 8, (d.vol_z + ZB - 1) / ZB);
     kern<<<grid, dim3(32, 9), smem, s>>>(L);
     count_launches(1);
     B2T_CUDA_TRY(cudaGetLastError(), "bp3d_tma launch");
     return B2T_OK;
 }
 
-template <typename T>
+template <typename T, int ZB>
 b2t_status launch_kind(const BPTmaLaunch &L, int kind, int ker, bool circ, const b2t_dims3d &d, cudaStream_t s)
 {
     if (kind == B2T_GEOM_PAR3D)
-        return circ ? launch_one<T, B2T_GEOM_PAR3D, B2T_KER_DEFAULT, true>(L, d, s)
-                    : launch_one<T, B2T_GEOM_PAR3D, B2T_KER_DEFAULT, false>(L, d, s);
+        return circ ? launch_one<T, B2T_GEOM_PAR3D, B2T_KER_DEFAULT, true, ZB>(L, d, s)
+                    : launch_one<T, B2T_GEOM_PAR3D, B2T_KER_DEFAULT, false, ZB>(L, d, s);
     if (ker == B2T_KER_2D_WEIGHTING)
-        return circ ? launch_one<T, B2T_GEOM_CONE, B2T_KER_2D_WEIGHTING, true>(L, d, s)
-                    : launch_one<T, B2T_GEOM_CONE, B2T_KER_2D_WEIGHTING, false>(L, d, s);
-    return circ ? launch_one<T, B2T_GEOM_CONE, B2T_KER_DEFAULT, true>(L, d, s)
-                : launch_one<T, B2T_GEOM_CONE, B2T_KER_DEFAULT, false>(L, d, s);
+        return circ ? launch_one<T, B2T_GEOM_CONE, B2T_KER_2D_WEIGHTING, true, ZB>(L, d, s)
+                    : launch_one<T, B2T_GEOM_CONE, B2T_KER_2D_WEIGHTING, false, ZB>(L, d, s);
+    return circ ? launch_one<T, B2T_GEOM_CONE, B2T_KER_DEFAULT, true, ZB>(L, d, s)
+                : launch_one<T, B2T_GEOM_CONE, B2T_KER_DEFAULT, false, ZB>(L, d, s);
+}
+
+template <typename T>
+b2t_status launch_shape(const BPTmaLaunch &L, int kind, int ker, bool circ, int vpt, const b2t_dims3d &d,
+                        cudaStream_t s)
+{
+    return vpt == 16 ? launch_kind<T, 16>(L, kind, ker, circ, d, s) : launch_kind<T, 32>(L, kind, ker, circ, d, s);
+}
+
+// Voxels per thread chosen by b2t_autotune_bp3d, per problem class, for this
+// process; the autotuner's candidate while it times one on this thread.
+std::mutex g_vpt_mutex;
+std::map<std::string, int> g_vpt;
+thread_local int t_vpt_override = 0;
+
+std::string vpt_key(const b2t_geom3d *g, int32_t dtype)
+{
+    const b2t_dims3d &d = g->dims;
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "%d/%d/%u/%u/%u/%u/%u/%u", g->kind, dtype, d.vol_x, d.vol_y, d.vol_z, d.angles,
+                  d.det_u, d.det_v);
+    return buf;
+}
+
+// The autotuner's candidate; else B2T_BP_VPT (16 or 32) from the
+// environment; else the tuned shape of this problem class; else 32, unless
+// the volume's depth leaves 32-voxel columns mostly past its last slice: a
+// 16-voxel column costs about 1.1 times a 32-voxel one per slice (measured
+// on B200 at 128^3 to 512^3), so 16 when 1.1 x the slices it computes is
+// fewer than the 32-voxel shape computes.
+int choose_vpt(const b2t_geom3d *g, int32_t dtype)
+{
+    if (t_vpt_override) return t_vpt_override;
+    if (const char *e = std::getenv("B2T_BP_VPT")) return std::atoi(e) == 16 ? 16 : 32;
+    {
+        std::lock_guard<std::mutex> lock(g_vpt_mutex);
+        auto it = g_vpt.find(vpt_key(g, dtype));
+        if (it != g_vpt.end()) return it->second;
+    }
+    const double nz = g->dims.vol_z;
+    const double z16 = 16.0 * std::ceil(nz / 16.0), z32 = 32.0 * std::ceil(nz / 32.0);
+    return 1.1 * z16 < z32 ? 16 : 32;
 }
 
 }  // namespace
@@ -762,6 +816,7 @@ b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *p
     L.nu = d.det_u; L.nv = d.det_v; L.na = d.angles;
     L.out_scale = out_scale;
     L.tile_row_bytes = (uint32_t)(tile_bu<float>() * esz);
+    const int vpt = choose_vpt(g, dtype);
     const int kker = (ker == B2T_KER_FDK_WEIGHTING) ? B2T_KER_DEFAULT : ker;
     for (uint32_t c0 = 0; c0 < d.angles && st == B2T_OK; c0 += BPT_MAX_VIEWS) {
         const uint32_t cn = std::min(d.angles - c0, (uint32_t)BPT_MAX_VIEWS);
@@ -774,12 +829,67 @@ b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *p
             const BPView &w = L.views[i];
             if (w.nu.z != 0.0f || (g->kind == B2T_GEOM_CONE && w.den.z != 0.0f)) circ = false;
         }
-        if (dtype == B2T_F32) st = launch_kind<float>(L, g->kind, kker, circ, d, s);
-        else if (dtype == B2T_F16) st = launch_kind<__half>(L, g->kind, kker, circ, d, s);
-        else st = launch_kind<__nv_bfloat16>(L, g->kind, kker, circ, d, s);
+        if (dtype == B2T_F32) st = launch_shape<float>(L, g->kind, kker, circ, vpt, d, s);
+        else if (dtype == B2T_F16) st = launch_shape<__half>(L, g->kind, kker, circ, vpt, d, s);
+        else st = launch_shape<__nv_bfloat16>(L, g->kind, kker, circ, vpt, d, s);
     }
     delete Lp;
     return st;
+}
+
+b2t_status bp3d_autotune_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *proj, size_t proj_pitch,
+                              void *vol, size_t vol_pitch, int32_t dtype, cudaStream_t s, int32_t *vpt_out)
+{
+    B2T_TRY(validate3d(g, "b2t_autotune_bp3d"));
+    if (!p || !vol || !proj) return fail(B2T_ERR_INVALID_ARG, "b2t_autotune_bp3d: null argument");
+    if (!dtype_valid(dtype)) return fail(B2T_ERR_INVALID_ARG, "b2t_autotune_bp3d: bad dtype %d", dtype);
+    if (p->voxel_supersample != 1 || p->kernel == B2T_KER_MATCHED_BP || force_simple_bp())
+        return fail(B2T_ERR_UNSUPPORTED, "b2t_autotune_bp3d: only the TMA backprojector has launch shapes to choose");
+    static const int cands[] = {32, 16};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    B2T_CUDA_TRY(cudaEventCreate(&e0), "autotune event");
+    cudaError_t ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_fail(ce, "autotune event");
+    }
+    int best = 32;
+    float best_ms = 1e30f;
+    b2t_status st = B2T_OK;
+    for (const int c : cands) {
+        t_vpt_override = c;
+        // one untimed run, then the best of two timed runs of the whole call
+        st = bp3d_impl(g, p, proj, proj_pitch, vol, vol_pitch, dtype, B2T_MODE_SET, s);
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2 && st == B2T_OK; ++rep) {
+            cudaEventRecord(e0, s);
+            st = bp3d_impl(g, p, proj, proj_pitch, vol, vol_pitch, dtype, B2T_MODE_SET, s);
+            cudaEventRecord(e1, s);
+            ce = cudaEventSynchronize(e1);
+            if (ce != cudaSuccess) {
+                st = cuda_fail(ce, "autotune timing");
+                break;
+            }
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms = std::min(ms, t);
+        }
+        t_vpt_override = 0;
+        if (st != B2T_OK) break;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != B2T_OK) return st;
+    {
+        std::lock_guard<std::mutex> lock(g_vpt_mutex);
+        g_vpt[vpt_key(g, dtype)] = best;
+    }
+    if (vpt_out) *vpt_out = best;
+    return B2T_OK;
 }
 
 b2t_status encode_tensor_map(CUtensorMap *map, CUtensorMapDataType dtype, uint32_t rank, const void *base,

@@ -65,13 +65,14 @@ struct BPLaunch {
 
 // TMA-staged backprojection (bp3d_tma.cu): voxel block, tile geometry and
 // the shared-memory ring the tiles stream through.
-constexpr int BPT_Z = 32;             // voxels per thread along z
+// voxels per thread along z: 32 (two CTAs an SM) unless b2t_autotune_bp3d
+// chose 16 (three CTAs an SM) for the problem class
 constexpr int BPT_CHUNK = 8;          // tile rows per TMA box; a view loads the chunks its footprint needs
 constexpr int BPT_BV = 96;            // most rows one view's tile may take
 constexpr int BPT_RING_BYTES = 112896; // ring of tile rows (336 rows of 84 4-byte elements: FP32 texels or
                                        // 16-bit pairs); two CTAs of ring + records (and the 1 KB each
                                        // reserves) fit an SM's 228 KB
-constexpr int BPT_CTAS_PER_SM = 2;    // resident CTAs (96 registers a thread with 32 accumulators)
+constexpr int BPT_RING_BYTES_Z16 = 75264; // the ring of the 16-voxel shape: 224 rows, three CTAs an SM
 constexpr int BPT_SLOTS = 8;          // views in flight at most (barrier pairs and stage records)
 constexpr int BPT_MAX_VIEWS = 640;
 
@@ -104,6 +105,8 @@ b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *p
                     size_t vol_pitch, int32_t dtype, int32_t mode, cudaStream_t s);
 b2t_status device_errors_impl(uint32_t *flags);
 b2t_status bp_path_stats_impl(uint64_t *stats);
+b2t_status bp3d_autotune_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *proj, size_t proj_pitch,
+                              void *vol, size_t vol_pitch, int32_t dtype, cudaStream_t s, int32_t *vpt_out);
 // One warp waits, bounded by limit cycles, for an mbarrier phase (which 0) or
 // a device flag (which 1) that nothing completes; B2T_ERR_TIMEOUT when the
 // wait gave up and set the device error word.

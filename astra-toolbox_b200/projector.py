@@ -114,6 +114,21 @@ class Projector3D:
                       proj.data_ptr(), 0, _DTYPES[vol.dtype], stream_handle(vol.device), ctypes.byref(vpc))
         return vpc.value
 
+    def autotune_bp(self, proj, vol):
+        """Time the TMA backprojector's launch shapes on these buffers and keep
+        the fastest for this problem class (b2t_autotune_bp3d); vol is
+        overwritten with B proj.  Returns the chosen voxels per thread."""
+        _check_tensor(vol, self.vol_shape, "volume")
+        _check_tensor(proj, self.proj_shape, "projection data", vol.device)
+        if self.is_cyl:
+            raise AstraError(3, "autotune_bp: the cyl_cone_vec projector has a single launch shape")
+        p = self.params()
+        vpt = ctypes.c_int32(0)
+        with torch.cuda.device(vol.device):
+            _lib.call("b2t_autotune_bp3d", ctypes.byref(self.geom.c), ctypes.byref(p), proj.data_ptr(), 0,
+                      vol.data_ptr(), 0, _DTYPES[vol.dtype], stream_handle(vol.device), ctypes.byref(vpt))
+        return vpt.value
+
     def bp(self, proj, vol, mode=_lib.MODE_SET, output_scale=1.0, kernel=None):
         """vol (=|+=) B proj on torch tensors (B = ASTRA's BP, or A^T for matched_bp)."""
         _check_tensor(vol, self.vol_shape, "volume")

@@ -608,6 +608,19 @@ void b2t_batch2d_destroy(b2t_batch2d *batch);
 b2t_status b2t_autotune_fp3d(const b2t_geom3d *geom, const b2t_params3d *params, const void *vol, size_t vol_pitch,
                              void *proj, size_t proj_pitch, int32_t dtype, void *stream, int32_t *vpc);
 
+/* Choose the launch shape of the TMA 3D backprojector for this problem class
+ * (geometry kind, storage type, volume and detector sizes, view count) by
+ * timing both on the caller's buffers: 32 voxels per thread along z (two
+ * CTAs an SM) or 16 (three CTAs an SM, half the per-view set-up shared).
+ * The choice is kept for the process and used by every later b2t_bp3d (and
+ * the BP of b2t_fdk) of the same class; B2T_BP_VPT in the environment still
+ * overrides it.  Overwrites vol with B proj; synchronises the stream.
+ * B2T_ERR_UNSUPPORTED for voxel supersampling or the matched BP, which have
+ * one shape.  No counterpart in the reference, whose launch shapes are
+ * compile-time constants (cuda/3d/cone_bp.cu:38-42).  vpt may be NULL. */
+b2t_status b2t_autotune_bp3d(const b2t_geom3d *geom, const b2t_params3d *params, const void *proj, size_t proj_pitch,
+                             void *vol, size_t vol_pitch, int32_t dtype, void *stream, int32_t *vpt);
+
 /* On-chip load bandwidth of the current GPU in GB/s (no counterpart in the
  * reference): which = 0 streams 16-byte shared-memory loads, which = 1
  * streams 16-byte global loads that hit L1.  The projectors' interpolation

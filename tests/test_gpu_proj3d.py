@@ -265,6 +265,13 @@ def _bp_path_stats():
     return list(st)
 
 
+def _bp_vpt(nz):
+    """Voxels per thread of the TMA BP when nothing is tuned: 16 when 1.1 x
+    the slices 16-voxel columns compute is fewer than 32-voxel columns do."""
+    z16, z32 = 16 * ((nz + 15) // 16), 32 * ((nz + 31) // 32)
+    return 16 if 1.1 * z16 < z32 else 32
+
+
 @pytest.mark.parametrize("dtype", ["float32", "float16", "bfloat16"])
 @pytest.mark.parametrize("geom", ["c2_like", "high_mag", "cone_vec", "par3d"])
 def test_tma_bp_matches_direct_bp(astra, geom, dtype, monkeypatch):
@@ -296,10 +303,10 @@ def test_tma_bp_matches_direct_bp(astra, geom, dtype, monkeypatch):
     assert _device_errors() == 0
     fast, general, idle, cycles = _bp_path_stats()
     nz, ny, nx = pr.vol_shape
-    # every voxel column (32 slices per thread) is counted once per view;
-    # idle lanes pad the 32 x 8 column blocks
+    # every voxel column (16 or 32 slices per thread) is counted once per
+    # view; idle lanes pad the 32 x 8 column blocks
     nviews = pr.proj_shape[1]
-    zb = (nz + 31) // 32
+    zb = (nz + _bp_vpt(nz) - 1) // _bp_vpt(nz)
     assert fast + general == nx * ny * zb * nviews
     assert idle == (((nx + 31) // 32) * 32 * ((ny + 7) // 8) * 8 - nx * ny) * zb * nviews
     assert cycles > 0
@@ -408,6 +415,43 @@ def test_slab_fp_vs_oracle_and_cells(astra, orc, case, monkeypatch):
     import importlib
     assert importlib.import_module("astra-toolbox_b200._lib").load().b2t_device_errors(ctypes.byref(flags)) == 0
     assert flags.value == 0
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float16"])
+def test_autotune_bp3d_shapes_agree(astra, orc, dtype, monkeypatch):
+    """The BP autotuner times 32 and 16 voxels per thread and keeps the
+    fastest; both shapes backproject the same volume (their per-block folded
+    coefficients start at different slices: FP32 rounding apart), every
+    column is counted once per view, and the 16-voxel shape matches the
+    oracle."""
+    ang = np.linspace(0, 2 * np.pi, 60, endpoint=False).astype(np.float32)
+    vg = astra.create_vol_geom(72, 64, 40)
+    pg = astra.create_proj_geom('cone', 1.0, 1.0, 70, 90, ang, 180.0, 90.0)
+    pr = _proj(astra, vg, pg)
+    tdt = getattr(torch, dtype)
+    proj = torch.from_numpy(np.random.default_rng(13).random(pr.proj_shape, dtype=np.float32)).cuda().to(tdt)
+    nz, ny, nx = pr.vol_shape
+    out = {}
+    for vpt in (32, 16):
+        monkeypatch.setenv("B2T_BP_VPT", str(vpt))
+        v = torch.zeros(pr.vol_shape, device='cuda', dtype=tdt)
+        _bp_path_stats()
+        pr.bp(proj, v)
+        fast, general, idle, _ = _bp_path_stats()
+        assert fast + general == nx * ny * ((nz + vpt - 1) // vpt) * pr.proj_shape[1]
+        out[vpt] = v.float().cpu().numpy()
+    monkeypatch.delenv("B2T_BP_VPT")
+    tol = 4e-6 if dtype == "float32" else 5e-4
+    assert rel_l2(out[16], out[32]) < tol
+    b = torch.zeros(pr.vol_shape, device='cuda', dtype=tdt)
+    vpt = pr.autotune_bp(proj, b)
+    assert vpt in (16, 32)
+    assert rel_l2(b.float().cpu().numpy(), out[vpt]) < tol
+    c = torch.zeros(pr.vol_shape, device='cuda', dtype=tdt)
+    pr.bp(proj, c)  # runs with the tuned shape
+    assert np.array_equal(c.float().cpu().numpy(), out[vpt])
+    refb = orc.bp3d(2, pr.geom.views_array(), proj.float().cpu().numpy(), pr.vol_shape, pr.geom.vol_scale)
+    assert rel_l2(out[16], refb) < (1e-5 if dtype == "float32" else 1e-3)
 
 
 @pytest.mark.parametrize("idx", [0, 4])
