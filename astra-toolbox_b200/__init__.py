@@ -17,7 +17,7 @@ from ._lib import AstraError
 from .geometry import create_proj_geom, create_vol_geom
 from .projector import Projector2D, Projector3D
 from . import algorithm, batch, data2d, data3d, experimental, projector, projector3d  # noqa: F401
-from .batch import Batch2D  # noqa: F401
+from .batch import Batch2D, Batch3D  # noqa: F401
 from .optomo import OpTomo  # noqa: F401
 from .gpu import get_gpu_info, set_gpu_index  # noqa: F401
 from .algorithm import astra_dict

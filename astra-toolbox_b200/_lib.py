@@ -108,6 +108,10 @@ class Problem2D(ctypes.Structure):
     _fields_ = [("geom", Geom2D), ("det_supersample", ctypes.c_uint32), ("pixel_supersample", ctypes.c_uint32)]
 
 
+class Problem3D(ctypes.Structure):
+    _fields_ = [("geom", Geom3D), ("det_supersample", ctypes.c_uint32), ("output_scale", ctypes.c_float)]
+
+
 ALGO_SIRT, ALGO_CGLS, ALGO_SART = 1, 2, 3
 
 
@@ -180,6 +184,12 @@ SIGNATURES = {
     "b2t_batch2d_bp": (_I32, [_P, _P, _P, _I32, _P]),
     "b2t_algo_create_batch2d": (_I32, [_I32, _P, _P, _P]),
     "b2t_batch2d_destroy": (None, [_P]),
+    "b2t_batch3d_create": (_I32, [_P, _I32, _P]),
+    "b2t_batch3d_layout": (_I32, [_P, _P, _P, _P, _P]),
+    "b2t_batch3d_fp": (_I32, [_P, _P, _P, _I32, _P]),
+    "b2t_batch3d_bp": (_I32, [_P, _P, _P, _I32, _P]),
+    "b2t_batch3d_matched_bp": (_I32, [_P, _P, _P, _I32, _P]),
+    "b2t_batch3d_destroy": (None, [_P]),
 }
 
 _lib = None

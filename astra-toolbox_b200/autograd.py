@@ -13,13 +13,22 @@ returns the gradient one would get by using that BP in place of A^T, so its
 deviation from the exact gradient can be measured.
 
 Volumes are (z, y, x) and projections (v, angle, u) tensors on a CUDA
-device, float32 / float16 / bfloat16; a leading batch dimension is projected
-item by item.
+device, float32 / float16 / bfloat16, with optional leading batch
+dimensions.  A float32 batch of small problems (up to BATCH_MAX_VOXELS voxels
+each) is projected in one persistent launch per direction (b2t_batch3d_fp
+and its exact adjoint b2t_batch3d_matched_bp: the items of a batch are one
+packed buffer as they are); larger or 16-bit items go through the
+single-problem projectors one by one, each of which fills the GPU.
 """
+import numpy as np
 import torch
 
 from . import _lib
+from .batch import Batch3D
 from .projector import Projector3D
+
+# Largest item (voxels) projected through the batched kernels.
+BATCH_MAX_VOXELS = 128 ** 3
 
 
 def _fp(projector, vol):
@@ -34,11 +43,33 @@ def _at(projector, proj):
     return out
 
 
+def _batch_plan(projector, n):
+    """The Batch3D of n copies of this projector's problem, or None when the
+    items go one by one (see the module docstring)."""
+    if projector.is_cyl or projector.vox_ss != 1:
+        return None
+    nvox, nproj = int(np.prod(projector.vol_shape)), int(np.prod(projector.proj_shape))
+    if nvox > BATCH_MAX_VOXELS or nvox % 32 or nproj % 32:
+        return None  # (packed items start on 32-element boundaries)
+    cache = projector.__dict__.setdefault('_batch3d', {})
+    if n not in cache:
+        opts = {'DetectorSuperSampling': projector.det_ss}
+        cache[n] = Batch3D([(projector.proj_geom, projector.vol_geom, opts)] * n)
+    return cache[n]
+
+
 def _batched(fn, projector, x, base_ndim):
     if x.dim() == base_ndim:
         return fn(projector, x)
-    return torch.stack([fn(projector, xi) for xi in x.reshape(-1, *x.shape[-base_ndim:])]).reshape(
-        *x.shape[:-base_ndim], *(projector.proj_shape if fn is _fp else projector.vol_shape))
+    out_shape = projector.proj_shape if fn is _fp else projector.vol_shape
+    items = x.reshape(-1, *x.shape[-base_ndim:])
+    B = _batch_plan(projector, items.shape[0]) if x.dtype == torch.float32 else None
+    if B is not None:
+        flat = items.contiguous().view(-1)
+        with torch.cuda.device(x.device):
+            out = B.fp(flat) if fn is _fp else B.bp(flat, matched=True)
+        return out.view(*x.shape[:-base_ndim], *out_shape)
+    return torch.stack([fn(projector, xi) for xi in items]).reshape(*x.shape[:-base_ndim], *out_shape)
 
 
 class ForwardProjection(torch.autograd.Function):

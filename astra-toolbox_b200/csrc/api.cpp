@@ -11,6 +11,7 @@
 #include "algorithms.h"
 #include "arith.h"
 #include "batch2d.h"
+#include "batch3d.h"
 #include "b2t_internal.h"
 #include "fdk.h"
 #include "filters.h"
@@ -374,6 +375,52 @@ b2t_status b2t_algo_create_batch2d(int32_t type, b2t_batch2d *batch, const b2t_a
 void b2t_batch2d_destroy(b2t_batch2d *batch)
 {
     delete reinterpret_cast<Batch2D *>(batch);
+}
+
+b2t_status b2t_batch3d_create(const b2t_problem3d *problems, int32_t n, b2t_batch3d **out)
+{
+    clear_error();
+    return batch3d_create_impl(problems, n, reinterpret_cast<Batch3D **>(out));
+}
+
+b2t_status b2t_batch3d_layout(const b2t_batch3d *batch, uint64_t *vol_offsets, uint64_t *proj_offsets,
+                              uint64_t *vol_total, uint64_t *proj_total)
+{
+    clear_error();
+    const Batch3D *b = reinterpret_cast<const Batch3D *>(batch);
+    if (!b) return fail(B2T_ERR_INVALID_ARG, "b2t_batch3d_layout: null batch");
+    for (size_t i = 0; i < b->probs.size(); ++i) {
+        if (vol_offsets) vol_offsets[i] = (uint64_t)b->probs[i].vol_off;
+        if (proj_offsets) proj_offsets[i] = (uint64_t)b->probs[i].proj_off;
+    }
+    if (vol_total) *vol_total = b->vol_total;
+    if (proj_total) *proj_total = b->proj_total;
+    return B2T_OK;
+}
+
+b2t_status b2t_batch3d_fp(b2t_batch3d *batch, const float *vols, float *projs, int32_t mode, void *stream)
+{
+    clear_error();
+    return batch3d_fp_impl(reinterpret_cast<Batch3D *>(batch), vols, projs, mode, static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_batch3d_bp(b2t_batch3d *batch, const float *projs, float *vols, int32_t mode, void *stream)
+{
+    clear_error();
+    return batch3d_bp_impl(reinterpret_cast<Batch3D *>(batch), projs, vols, mode, false,
+                           static_cast<cudaStream_t>(stream));
+}
+
+b2t_status b2t_batch3d_matched_bp(b2t_batch3d *batch, const float *projs, float *vols, int32_t mode, void *stream)
+{
+    clear_error();
+    return batch3d_bp_impl(reinterpret_cast<Batch3D *>(batch), projs, vols, mode, true,
+                           static_cast<cudaStream_t>(stream));
+}
+
+void b2t_batch3d_destroy(b2t_batch3d *batch)
+{
+    delete reinterpret_cast<Batch3D *>(batch);
 }
 
 b2t_status b2t_filter_taps(const b2t_filter_config *filter, uint32_t n, uint32_t n_views, float *out, size_t *count)

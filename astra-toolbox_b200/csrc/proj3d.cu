@@ -38,51 +38,9 @@
 
 #include "b2t_internal.h"
 #include "proj3d.h"
+#include "proj3d_dev.cuh"
 
 namespace b2t {
-
-// ---------------------------------------------------------------------------
-// storage loads
-// ---------------------------------------------------------------------------
-
-template <typename T> __device__ __forceinline__ float ld(const T *p);
-template <> __device__ __forceinline__ float ld<float>(const float *p) { return __ldg(p); }
-template <> __device__ __forceinline__ float ld<__half>(const __half *p) { return __half2float(__ldg(p)); }
-template <> __device__ __forceinline__ float ld<__nv_bfloat16>(const __nv_bfloat16 *p)
-{
-    return __bfloat162float(__ldg(p));
-}
-
-template <typename T> __device__ __forceinline__ float ldplain(const T *p);
-template <> __device__ __forceinline__ float ldplain<float>(const float *p) { return *p; }
-template <> __device__ __forceinline__ float ldplain<__half>(const __half *p) { return __half2float(*p); }
-template <> __device__ __forceinline__ float ldplain<__nv_bfloat16>(const __nv_bfloat16 *p)
-{
-    return __bfloat162float(*p);
-}
-
-template <typename T> __device__ __forceinline__ T from_float(float v);
-template <> __device__ __forceinline__ float from_float<float>(float v) { return v; }
-template <> __device__ __forceinline__ __half from_float<__half>(float v) { return __float2half_rn(v); }
-template <> __device__ __forceinline__ __nv_bfloat16 from_float<__nv_bfloat16>(float v)
-{
-    return __float2bfloat16_rn(v);
-}
-
-// Split a continuous texel index q (texel i at q = i) into the base texel
-// k = floor(q) and the weight f = q - k, using the round-to-nearest of the
-// FP32 adder (q - 0.5 + 1.5*2^23 holds rint(q - 0.5) in its mantissa) rather
-// than the conversion pipe.  qm = q - 0.5 is passed in; valid for |q| < 2^22.
-// At exact ties either neighbour is chosen and f is 0 or 1, which selects the
-// same texel value.
-__device__ __forceinline__ void split_texel(float qm, int &k, float &f)
-{
-    const float M = 12582912.0f;  // 1.5 * 2^23
-    float t = __fadd_rn(qm, M);
-    float r = __fadd_rn(t, -M);
-    k = __float_as_int(t) - 0x4B400000;
-    f = __fadd_rn(__fadd_rn(qm, -r), 0.5f);
-}
 
 // ---------------------------------------------------------------------------
 // padded copies
@@ -174,41 +132,6 @@ __global__ void pad_proj_pairs(const T *__restrict__ src, size_t src_pitch, int 
 // forward projection
 // ---------------------------------------------------------------------------
 
-// Clip the slice range [smin, smax] to where lo <= A*s + B <= hi.
-__device__ __forceinline__ void clip_slices(float A, float B, float lo, float hi, float &smin,
-                                            float &smax)
-{
-    if (fabsf(A) < 1e-12f) {
-        if (!(B >= lo && B <= hi)) {
-            smin = 1.0f;
-            smax = 0.0f;
-        }
-        return;
-    }
-    float s1 = (lo - B) / A, s2 = (hi - B) / A;
-    smin = fmaxf(smin, fminf(s1, s2));
-    smax = fminf(smax, fmaxf(s1, s2));
-}
-
-// The FP's split (shared with the cell kernels and the matched BP): sample
-// position plus one half qh = A s + (B + 1/2); texel floor(qh) by rounding
-// down, weight qh - floor(qh).
-constexpr float SPLIT_M = 12582912.0f;  // 1.5 * 2^23
-__device__ __forceinline__ void split_floor(float qh, int &k, float &f)
-{
-    const float t = __fadd_rd(qh, SPLIT_M);
-    k = __float_as_int(t) - 0x4B400000;
-    f = qh - (t - SPLIT_M);
-}
-
-__device__ __forceinline__ bool fp_texel_ok(float A, float Bh, int s, int n)
-{
-    int k;
-    float f;
-    split_floor(fmaf(A, (float)s, Bh), k, f);
-    return k >= -2 && k <= n;
-}
-
 template <typename T>
 __global__ void __launch_bounds__(256) fp3d_kernel(const __grid_constant__ FPLaunch L)
 {
@@ -216,64 +139,8 @@ __global__ void __launch_bounds__(256) fp3d_kernel(const __grid_constant__ FPLau
     const int u = blockIdx.y * 32 + threadIdx.x;
     const int v = blockIdx.z * 8 + threadIdx.y;
     if (u >= L.nu || v >= L.nv) return;
-    const T *__restrict__ vol = static_cast<const T *>(L.vol);
-    const long long st0 = L.st0, st2 = L.st2;
-    const int R = L.rays;
-    const float n0 = (float)L.n0;
-    float acc = 0.0f;
-    for (int iu = 0; iu < R; ++iu) {
-        for (int iv = 0; iv < R; ++iv) {
-            // detector position relative to the detector centre, in pixels
-            float uu = (float)u + 0.5f - 0.5f * (float)L.nu;
-            float vv = (float)v + 0.5f - 0.5f * (float)L.nv;
-            if (R > 1) {
-                uu += -0.5f + (0.5f + (float)iu) / (float)R;
-                vv += -0.5f + (0.5f + (float)iv) / (float)R;
-            }
-            const float den = fmaf(vv, V.e[2], fmaf(uu, V.e[1], V.e[0]));
-            const float inv = 1.0f / den;
-            const float A1 = fmaf(vv, V.m1[2], fmaf(uu, V.m1[1], V.m1[0])) * inv;
-            const float A2 = fmaf(vv, V.m2[2], fmaf(uu, V.m2[1], V.m2[0])) * inv;
-            const float B1 = fmaf(vv, V.n1[2], fmaf(uu, V.n1[1], V.n1[0])) * inv;
-            const float B2 = fmaf(vv, V.n2[2], fmaf(uu, V.n2[1], V.n2[0])) * inv;
-            // slices whose sample can touch the volume: q - 0.5 in [-1.5, n - 0.5)
-            float smin = 0.0f, smax = n0 - 1.0f;
-            clip_slices(A1, B1, -1.6f, (float)L.n1 - 0.4f, smin, smax);
-            clip_slices(A2, B2, -1.6f, (float)L.n2 - 0.4f, smin, smax);
-            int s_lo = max(0, (int)ceilf(fmaxf(smin, -1.0f)));
-            int s_hi = min(L.n0 - 1, (int)floorf(fminf(smax, n0)));
-            const float B1h = B1 + 0.5f, B2h = B2 + 0.5f;
-            // guarantee every access is inside the padded copy: the base
-            // texel is monotone in s, so checking the end points suffices
-            for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
-                if (fp_texel_ok(A1, B1h, s_lo, L.n1) && fp_texel_ok(A2, B2h, s_lo, L.n2)) break;
-                ++s_lo;
-            }
-            for (int it = 0; it < 3 && s_lo <= s_hi; ++it) {
-                if (fp_texel_ok(A1, B1h, s_hi, L.n1) && fp_texel_ok(A2, B2h, s_hi, L.n2)) break;
-                --s_hi;
-            }
-            if (!(fp_texel_ok(A1, B1h, s_lo, L.n1) && fp_texel_ok(A2, B2h, s_lo, L.n2) &&
-                  fp_texel_ok(A1, B1h, s_hi, L.n1) && fp_texel_ok(A2, B2h, s_hi, L.n2)))
-                s_hi = s_lo - 1;
-            float sum = 0.0f;
-            for (int s = s_lo; s <= s_hi; ++s) {
-                int k1, k2;
-                float f1, f2;
-                split_floor(fmaf(A1, (float)s, B1h), k1, f1);
-                split_floor(fmaf(A2, (float)s, B2h), k2, f2);
-                const T *p = vol + (long long)s * st0 + (long long)k2 * st2 + k1;
-                const float v00 = ld(p), v10 = ld(p + 1);
-                const float v01 = ld(p + st2), v11 = ld(p + st2 + 1);
-                const float a = fmaf(f1, v10 - v00, v00);
-                const float b = fmaf(f1, v11 - v01, v01);
-                sum += fmaf(f2, b - a, a);
-            }
-            const float sc = sqrtf(fmaf(A1 * A1, L.f1, fmaf(A2 * A2, L.f2, 1.0f))) * L.mul;
-            acc = fmaf(sum, sc, acc);
-        }
-    }
-    if (R > 1) acc /= (float)(R * R);
+    const FPPadded<T> Ld{static_cast<const T *>(L.vol), L.st0, L.st2};
+    float acc = fp3d_ray(Ld, V, u, v, L.n0, L.n1, L.n2, L.nu, L.nv, L.rays, L.f1, L.f2, L.mul);
     T *out = static_cast<T *>(L.proj) + ((size_t)v * L.na + V.a) * L.proj_pitch + u;
     if (L.accumulate) acc += ldplain(out);
     *out = from_float<T>(acc);
@@ -290,51 +157,12 @@ __global__ void __launch_bounds__(256) bp3d_kernel(const __grid_constant__ BPLau
     const int y = blockIdx.y * 8 + threadIdx.y;
     const int z0 = blockIdx.z * ZB;
     if (x >= L.nx || y >= L.ny) return;
-    const T *__restrict__ proj = static_cast<const T *>(L.proj);
     const float fx = (float)x - 0.5f * (float)L.nx + 0.5f;
     const float fy = (float)y - 0.5f * (float)L.ny + 0.5f;
     const float fz = (float)z0 - 0.5f * (float)L.nz + 0.5f;
+    const BPPadded<T> Ld{static_cast<const T *>(L.proj), L.pv, L.pu};
     float acc[ZB];
-#pragma unroll
-    for (int j = 0; j < ZB; ++j) acc[j] = 0.0f;
-
-    for (int i = 0; i < L.nviews; ++i) {
-        const BPView &W = L.views[i];
-        const T *P = proj + (long long)(L.a0 + i) * L.pu;
-        float nu = fmaf(fz, W.nu.z, fmaf(fy, W.nu.y, fmaf(fx, W.nu.x, W.nu.w)));
-        float nv = fmaf(fz, W.nv.z, fmaf(fy, W.nv.y, fmaf(fx, W.nv.x, W.nv.w)));
-        float dn = fmaf(fz, W.den.z, fmaf(fy, W.den.y, fmaf(fx, W.den.x, W.den.w)));
-#pragma unroll
-        for (int j = 0; j < ZB; ++j) {
-            float U, Vc, w;
-            if (KIND == B2T_GEOM_CONE) {
-                const float fr = __frcp_rn(dn);
-                U = nu * fr;
-                Vc = nv * fr;
-                w = (KER == B2T_KER_2D_WEIGHTING) ? fr : fr * fr;
-            } else {
-                U = nu;
-                Vc = nv;
-                w = W.den.w;
-            }
-            // texture coordinates (U, V): texel i at i + 0.5 -> q - 0.5 = U - 1
-            int ku, kv;
-            float fu, fv;
-            split_texel(U - 1.0f, ku, fu);
-            split_texel(Vc - 1.0f, kv, fv);
-            ku = min(max(ku, -2), L.nu);
-            kv = min(max(kv, -2), L.nv);
-            const T *p = P + (long long)kv * L.pv + ku;
-            const float v00 = ld(p), v10 = ld(p + 1);
-            const float v01 = ld(p + L.pv), v11 = ld(p + L.pv + 1);
-            const float a = fmaf(fu, v10 - v00, v00);
-            const float b = fmaf(fu, v11 - v01, v01);
-            acc[j] = fmaf(fmaf(fv, b - a, a), w, acc[j]);
-            nu += W.nu.z;
-            nv += W.nv.z;
-            dn += W.den.z;
-        }
-    }
+    bp3d_column<KIND, KER, ZB>(Ld, L.views, L.nviews, L.a0, L.nu, L.nv, fx, fy, fz, acc);
     T *out = static_cast<T *>(L.vol);
 #pragma unroll
     for (int j = 0; j < ZB; ++j) {

@@ -594,6 +594,51 @@ b2t_status b2t_algo_create_batch2d(int32_t type, b2t_batch2d *batch, const b2t_a
 void b2t_batch2d_destroy(b2t_batch2d *batch);
 
 /* ---------------------------------------------------------------------- */
+/* batched 3D problems                                                     */
+/* ---------------------------------------------------------------------- */
+
+/* One problem of a 3D batch: a parallel3d / parallel3d_vec or cone / cone_vec
+ * geometry (views as for b2t_fp3d), FP32 storage, the default kernel. */
+typedef struct b2t_problem3d {
+    b2t_geom3d geom;              /* kind, dims, voxel size, host views           */
+    uint32_t det_supersample;     /* FP rays per detector pixel side (1..16)       */
+    float output_scale;           /* as b2t_params3d.output_scale                  */
+} b2t_problem3d;
+
+typedef struct b2t_batch3d b2t_batch3d;  /* opaque: device tables + work list */
+
+/* Plan a batch of n independent 3D problems (parallel and cone mixed, any
+ * sizes and view counts).  No counterpart in the reference, which projects
+ * such a set one problem at a time through astraCUDA3d::FP / BP
+ * (include/astra/cuda/3d/mem3d.h:107-113), at least one launch each.
+ * Copies the geometry to the device (synchronous, allocates with
+ * cudaMalloc).  Problem i's volume (z, y, x) and projections (v, angle, u)
+ * live in two packed buffers at the element offsets b2t_batch3d_layout
+ * reports. */
+b2t_status b2t_batch3d_create(const b2t_problem3d *problems, int32_t n, b2t_batch3d **out);
+/* Offsets (elements) of every problem in the packed buffers, and the buffer
+ * lengths.  vol_offsets / proj_offsets hold n entries each (may be NULL). */
+b2t_status b2t_batch3d_layout(const b2t_batch3d *batch, uint64_t *vol_offsets, uint64_t *proj_offsets,
+                              uint64_t *vol_total, uint64_t *proj_total);
+/* projs (=|+=) FP of vols for every problem, in one persistent launch:
+ * b2t_fp3d's direct-load ray model (cuda/3d/cone_fp.cu:154-231,
+ * par3d_fp.cu:146-220). */
+b2t_status b2t_batch3d_fp(b2t_batch3d *batch, const float *vols, float *projs, int32_t mode, void *stream);
+/* vols (=|+=) BP of projs for every problem (the reference's BP, default
+ * weighting: cuda/3d/cone_bp.cu:55-133, par3d_bp.cu:55-120), in one
+ * persistent launch. */
+b2t_status b2t_batch3d_bp(b2t_batch3d *batch, const float *projs, float *vols, int32_t mode, void *stream);
+/* vols (=|+=) A^T projs for every problem: the exact adjoint of
+ * b2t_batch3d_fp (its rays walked again, each detector value scattered over
+ * the texels its samples read with the same weights), for gradients; the
+ * scatter's atomic sums make the last bits depend on timing.  No counterpart
+ * in the reference, whose only matched backprojector is the cylindrical
+ * one (cuda/3d/cone_cyl.cu:309-470).  One persistent launch (plus a clear
+ * for B2T_MODE_SET). */
+b2t_status b2t_batch3d_matched_bp(b2t_batch3d *batch, const float *projs, float *vols, int32_t mode, void *stream);
+void b2t_batch3d_destroy(b2t_batch3d *batch);
+
+/* ---------------------------------------------------------------------- */
 /* measurement and tuning                                                  */
 /* ---------------------------------------------------------------------- */
 
