@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "b2t_internal.h"
@@ -321,6 +322,15 @@ __global__ void fold_accumulators(const float *__restrict__ accA, const float *_
     *o = tom<T>(r);
 }
 
+// B2T_MATCHED_PLAIN=1 selects the per-lane reductions of
+// fp3d_transpose_cols_kernel (the path of arrays of 2^32 cells or more)
+// instead of the merged ones (same sums, another order; tests compare them).
+bool matched_force_plain()
+{
+    const char *e = getenv("B2T_MATCHED_PLAIN");
+    return e && e[0] == '1';
+}
+
 template <typename T> b2t_status launch_T(const FPLaunch &L, dim3 grid, cudaStream_t s)
 {
     fp3d_transpose_kernel<T><<<grid, dim3(32, 8), 0, s>>>(L);
@@ -435,7 +445,7 @@ b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const v
                         // the lanes' sentinels above the cell count)
                         const unsigned long long cells =
                             (unsigned long long)(P.n1 + 4) * P.n0 * (unsigned long long)(P.n2 + 4);
-                        const bool agg = cells < (1ull << 32) - 64;
+                        const bool agg = cells < (1ull << 32) - 64 && !matched_force_plain();
                         if (dtype == B2T_F32) {
                             if (agg) fp3d_transpose_cols_kernel<float, true><<<grid, dim3(32, 8), 0, s>>>(P);
                             else fp3d_transpose_cols_kernel<float, false><<<grid, dim3(32, 8), 0, s>>>(P);

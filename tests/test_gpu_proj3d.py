@@ -176,6 +176,33 @@ def test_matched_bp_is_exact_transpose(astra, orc, idx):
     assert abs(lhs - rhs) / abs(lhs) < 1e-5, (lhs, rhs)
 
 
+@pytest.mark.parametrize("plain", [False, True])
+def test_matched_bp_fine_detector(astra, orc, plain, monkeypatch):
+    """Matched BP with a detector finer than the voxels (pixel 0.25 at
+    magnification ~2: about four rays per cell along a detector column), so
+    runs of three or more lanes fall on one cell in the merged reductions;
+    B2T_MATCHED_PLAIN=1 forces the per-lane reductions of very large
+    arrays.  Against the oracle's transpose and the dot-product test."""
+    if plain:
+        monkeypatch.setenv("B2T_MATCHED_PLAIN", "1")
+    ang = np.linspace(0, 2 * np.pi, 12, endpoint=False).astype(np.float32)
+    vg = astra.create_vol_geom(24, 28, 20)
+    pg = astra.create_proj_geom('cone', 0.25, 0.25, 160, 180, ang, 60.0, 60.0)
+    pr = _proj(astra, vg, pg, {'ProjectionKernel': 'matched_bp'})
+    rng = np.random.default_rng(21)
+    proj = rng.standard_normal(pr.proj_shape).astype(np.float32)
+    tv = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(torch.from_numpy(proj).cuda(), tv)
+    ref = orc.fp3d_transpose(2, pr.geom.views_array(), proj, pr.vol_shape, pr.geom.vol_scale)
+    assert rel_l2(tv.cpu().numpy(), ref) < TOL_F32
+    x = rng.standard_normal(pr.vol_shape).astype(np.float32)
+    ax = torch.zeros(pr.proj_shape, device='cuda')
+    pr.fp(torch.from_numpy(x).cuda(), ax)
+    lhs = float(np.dot(ax.cpu().numpy().ravel().astype(np.float64), proj.ravel().astype(np.float64)))
+    rhs = float(np.dot(x.ravel().astype(np.float64), tv.cpu().numpy().ravel().astype(np.float64)))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5, (lhs, rhs)
+
+
 @pytest.mark.parametrize("dtype,tol", [("float16", 1e-3), ("bfloat16", 8e-3)])
 def test_half_storage(astra, orc, dtype, tol):
     _, vg, pg = _cone_geoms(astra)[0]
