@@ -48,6 +48,7 @@
 #include <vector>
 
 #include "b2t_internal.h"
+#include "f32x2.cuh"
 #include "proj3d.h"
 #include "tma.h"
 
@@ -313,8 +314,34 @@ __device__ __forceinline__ void sample_smem(const SlabLaunch &L, uint32_t rb, fl
         int b1 = __float_as_int(t1);
         if (CLAMP) b1 = min(max(b1, SPLIT_BITS - 2), SPLIT_BITS + L.n1);
         const uint32_t row = (uint32_t)b1 * ROWB + rb;
+        // rows r, r + 1 in the two halves of packed f32x2 operations (each
+        // half rounds as the scalar form of the odd row below)
+        const uint64_t sf2 = pk2(sf, sf), M2 = pk2(SPLIT_M, SPLIT_M), nM2 = pk2(-SPLIT_M, -SPLIT_M);
+        const uint64_t f12 = pk2(f1, f1), g12 = pk2(g1, g1);
 #pragma unroll
-        for (int r = 0; r < RE; ++r) {
+        for (int r = 0; r + 1 < RE; r += 2) {
+            const uint64_t q2 = fma2(pk2(R.A2[w][r], R.A2[w][r + 1]), sf2, pk2(R.B2h[w][r], R.B2h[w][r + 1]));
+            const uint64_t t2 = add2_rd(q2, M2);
+            const float2 f2 = upk2(sub2(q2, add2(t2, nM2)));
+            const float2 tb = upk2(t2);
+            int b2a = __float_as_int(tb.x), b2b = __float_as_int(tb.y);
+            if (CLAMP) {
+                b2a = min(max(b2a, SPLIT_BITS - 2), SPLIT_BITS + L.n2);
+                b2b = min(max(b2b, SPLIT_BITS - 2), SPLIT_BITS + L.n2);
+            }
+            const uint32_t a0 = (uint32_t)b2a * 8u + row, a1 = (uint32_t)b2b * 8u + row;
+            const float2 p0a = lds_pair<0>(a0), p1a = lds_pair<(int)ROWB>(a0);
+            const float2 p0b = lds_pair<0>(a1), p1b = lds_pair<(int)ROWB>(a1);
+            // rows k1 and k1 + 1 interpolated along z, then blended by the
+            // shared in-plane weights straight into the sum
+            const uint64_t lo = pk2(fmaf(f2.x, p0a.y, p0a.x), fmaf(f2.y, p0b.y, p0b.x));
+            const uint64_t hi = pk2(fmaf(f2.x, p1a.y, p1a.x), fmaf(f2.y, p1b.y, p1b.x));
+            const float2 acc = upk2(fma2(f12, hi, fma2(g12, lo, pk2(R.acc[w][r], R.acc[w][r + 1]))));
+            R.acc[w][r] = acc.x;
+            R.acc[w][r + 1] = acc.y;
+        }
+        if constexpr (RE % 2 == 1) {
+            constexpr int r = RE - 1;
             const float q2 = fmaf(R.A2[w][r], sf, R.B2h[w][r]);
             const float t2 = __fadd_rd(q2, SPLIT_M);
             const float f2 = q2 - (t2 - SPLIT_M);
@@ -322,8 +349,6 @@ __device__ __forceinline__ void sample_smem(const SlabLaunch &L, uint32_t rb, fl
             if (CLAMP) b2 = min(max(b2, SPLIT_BITS - 2), SPLIT_BITS + L.n2);
             const uint32_t a = (uint32_t)b2 * 8u + row;
             const float2 p0 = lds_pair<0>(a), p1 = lds_pair<(int)ROWB>(a);
-            // rows k1 and k1 + 1 interpolated along z, then blended by the
-            // shared in-plane weights straight into the sum
             const float lo = fmaf(f2, p0.y, p0.x), hi = fmaf(f2, p1.y, p1.x);
             R.acc[w][r] = fmaf(f1, hi, fmaf(g1, lo, R.acc[w][r]));
         }
