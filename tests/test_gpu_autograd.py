@@ -149,6 +149,6 @@ def test_batch_dimension_is_one_launch_each_way(astra, kind):
     assert abs(lhs - rhs) / abs(lhs) < 1e-5, (lhs, rhs)
     for i in range(3):
         yi = AG.forward_project(x[i].detach(), pr)
-        assert float((y[i] - yi).norm() / yi.norm()) < 2e-6
+        assert float((y[i].detach() - yi).norm() / yi.norm()) < 2e-6
         gi = AG._at(pr, g[i])
         assert float((x.grad[i] - gi).norm() / gi.norm()) < 2e-5
