@@ -173,23 +173,16 @@ template <typename E> __host__ __device__ constexpr int tile_bu()
     static_assert(sizeof(E) == 4, "tile elements are FP32 texels or 16-bit pairs");
     return 84;
 }
-// Launch shapes: voxels per thread along z (ZB) and, with them, the CTAs an
-// SM holds (the registers of ZB accumulators) and the ring each CTA gets.
-template <int ZB> struct BPShape {
-    static_assert(ZB == 16 || ZB == 32, "16 or 32 voxels per thread");
-    static constexpr int ctas = ZB == 32 ? 2 : 3;
-    static constexpr int ring_bytes = ZB == 32 ? BPT_RING_BYTES : BPT_RING_BYTES_Z16;
-};
-// Ring rows (multiple of BPT_CHUNK) in the shape's ring of shared memory.
+// Ring rows (multiple of BPT_CHUNK) in the BPT_RING_BYTES of shared memory.
 // An 8-row chunk is a multiple of 128 bytes, so every chunk destination (ring
 // rows are allocated in whole chunks) is 128-byte aligned.
-template <typename E, int ZB> __host__ __device__ constexpr int ring_rows()
+template <typename E> __host__ __device__ constexpr int ring_rows()
 {
-    return (BPShape<ZB>::ring_bytes / (tile_bu<E>() * (int)sizeof(E))) & ~(BPT_CHUNK - 1);
+    return (BPT_RING_BYTES / (tile_bu<E>() * (int)sizeof(E))) & ~(BPT_CHUNK - 1);
 }
 static_assert(BPT_CHUNK * 84 * 4 % 128 == 0, "chunk alignment");
 static_assert((84 * 4) % 16 == 0, "TMA box row bytes");
-static_assert(ring_rows<float, 32>() >= BPT_BV && ring_rows<float, 16>() >= BPT_BV, "the ring holds the largest view");
+static_assert(ring_rows<float>() >= BPT_BV, "the ring holds the largest view");
 
 // Per-view record written by the producer warp: the tile's origin in padded
 // texels (u0, v0), its first ring row and its row count (0: the footprint does
@@ -248,7 +241,7 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, E *ring, uint64_t 
                                         StageInfo *info, int lane, float cx,
                                         float cy, float fz0)
 {
-    constexpr int R = ring_rows<E, ZB>();
+    constexpr int R = ring_rows<E>();
     constexpr int BU = tile_bu<E>();
     // voxel-centre extent of the block; along z the block's full ZB
     // slices, so that the voxels computed past the volume's last slice
@@ -397,11 +390,11 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, E *ring, uint64_t 
 // 288 threads: warps 0-7 backproject a 32 x 8 x ZB voxel block, warp 8
 // streams the views' tiles into the ring ahead of them.
 template <typename T, int KIND, int KER, bool CIRC, int ZB>
-__global__ void __launch_bounds__(288, BPShape<ZB>::ctas) bp3d_tma_kernel(const __grid_constant__ BPTmaLaunch L)
+__global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __grid_constant__ BPTmaLaunch L)
 {
     constexpr bool PAIR = sizeof(T) == 2;  // 16-bit texels are stored as pairs
     using E = elem_t<T, PAIR>;
-    constexpr int R = ring_rows<E, ZB>();
+    constexpr int R = ring_rows<E>();
     constexpr int BU = tile_bu<E>();
     extern __shared__ __align__(128) unsigned char smraw[];
     E *ring = reinterpret_cast<E *>(smraw);
@@ -679,7 +672,7 @@ template <typename T, int KIND, int KER, bool CIRC, int ZB>
 b2t_status launch_one(const BPTmaLaunch &L, const b2t_dims3d &d, cudaStream_t s)
 {
     using E = elem_t<T, sizeof(T) == 2>;
-    const size_t smem = (size_t)ring_rows<E, ZB>() * tile_bu<E>() * sizeof(E) +
+    const size_t smem = (size_t)ring_rows<E>() * tile_bu<E>() * sizeof(E) +
                         BPT_SLOTS * (2 * sizeof(uint64_t) + sizeof(StageInfo));
     auto kern = bp3d_tma_kernel<T, KIND, KER, CIRC, ZB>;
     B2T_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),

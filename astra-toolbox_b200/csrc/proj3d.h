@@ -65,14 +65,14 @@ struct BPLaunch {
 
 // TMA-staged backprojection (bp3d_tma.cu): voxel block, tile geometry and
 // the shared-memory ring the tiles stream through.
-// voxels per thread along z: 32 (two CTAs an SM) unless b2t_autotune_bp3d
-// chose 16 (three CTAs an SM) for the problem class
+// voxels per thread along z: 32 unless b2t_autotune_bp3d (or the volume's
+// depth) chose 16 for the problem class
 constexpr int BPT_CHUNK = 8;          // tile rows per TMA box; a view loads the chunks its footprint needs
 constexpr int BPT_BV = 96;            // most rows one view's tile may take
-constexpr int BPT_RING_BYTES = 112896; // ring of tile rows (336 rows of 84 4-byte elements: FP32 texels or
-                                       // 16-bit pairs); two CTAs of ring + records (and the 1 KB each
-                                       // reserves) fit an SM's 228 KB
-constexpr int BPT_RING_BYTES_Z16 = 75264; // the ring of the 16-voxel shape: 224 rows, three CTAs an SM
+constexpr int BPT_RING_BYTES = 75264; // ring of tile rows (224 rows of 84 4-byte elements: FP32 texels or
+                                      // 16-bit pairs); three CTAs of ring + records (and the 1 KB each
+                                      // reserves) fit an SM's 228 KB
+constexpr int BPT_CTAS_PER_SM = 3;    // resident CTAs (72 registers a thread with 32 accumulators)
 constexpr int BPT_SLOTS = 8;          // views in flight at most (barrier pairs and stage records)
 constexpr int BPT_MAX_VIEWS = 640;
 

@@ -655,8 +655,9 @@ b2t_status b2t_autotune_fp3d(const b2t_geom3d *geom, const b2t_params3d *params,
 
 /* Choose the launch shape of the TMA 3D backprojector for this problem class
  * (geometry kind, storage type, volume and detector sizes, view count) by
- * timing both on the caller's buffers: 32 voxels per thread along z (two
- * CTAs an SM) or 16 (three CTAs an SM, half the per-view set-up shared).
+ * timing both on the caller's buffers: 32 or 16 voxels per thread along z
+ * (the per-view set-up amortised over more voxels, or fewer slices computed
+ * past the volume's depth).
  * The choice is kept for the process and used by every later b2t_bp3d (and
  * the BP of b2t_fdk) of the same class; B2T_BP_VPT in the environment still
  * overrides it.  Overwrites vol with B proj; synchronises the stream.
