@@ -41,6 +41,7 @@
 #include <mutex>
 #include <string>
 #include <type_traits>
+#include <vector>
 
 #include "b2t_internal.h"
 #include "f32x2.cuh"
@@ -184,6 +185,25 @@ static_assert(BPT_CHUNK * 84 * 4 % 128 == 0, "chunk alignment");
 static_assert((84 * 4) % 16 == 0, "TMA box row bytes");
 static_assert(ring_rows<float>() >= BPT_BV, "the ring holds the largest view");
 
+// View i's coefficients from the launch record: 10 floats a view in circular
+// launches (nu.z and den.z are zero there), 12 otherwise.
+template <bool CIRC> __device__ __forceinline__ BPView view_rec(const BPTmaLaunch &L, int i)
+{
+    BPView W;
+    if constexpr (CIRC) {
+        const float *f = L.vrec + 10 * i;
+        W.nu = make_float4(f[0], f[1], 0.0f, f[2]);
+        W.nv = make_float4(f[3], f[4], f[5], f[6]);
+        W.den = make_float4(f[7], f[8], 0.0f, f[9]);
+    } else {
+        const float *f = L.vrec + 12 * i;
+        W.nu = make_float4(f[0], f[1], f[2], f[3]);
+        W.nv = make_float4(f[4], f[5], f[6], f[7]);
+        W.den = make_float4(f[8], f[9], f[10], f[11]);
+    }
+    return W;
+}
+
 // Per-view record written by the producer warp: the tile's origin in padded
 // texels (u0, v0), its first ring row and its row count (0: the footprint does
 // not fit a tile, read global memory), and for circular geometries the
@@ -259,7 +279,7 @@ __device__ __noinline__ void bp_produce(const BPTmaLaunch &L, E *ring, uint64_t 
         r.u0 = r.v0 = r.row0 = r.nrows = 0;
         r.cu = r.cv = r.cd = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (v < L.nviews) {
-            const BPView &W = L.views[v];
+            const BPView W = view_rec<CIRC>(L, v);
             float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f, dmin = 3.0e38f;
 #pragma unroll 1
             for (int c = 0; c < 8; ++c) {
@@ -542,7 +562,7 @@ __global__ void __launch_bounds__(288, BPT_CTAS_PER_SM) bp3d_tma_kernel(const __
             const float fx = (float)(blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7)) + 0.5f - 0.5f * (float)L.nx;
             const float fy = (float)(blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3)) + 0.5f - 0.5f * (float)L.ny;
             const float fz0 = (float)(blockIdx.z * ZB) + 0.5f - 0.5f * (float)L.nz;
-            const BPView &W = L.views[i];
+            const BPView W = view_rec<CIRC>(L, i);
             const int u0 = hd.x, v0 = hd.y, nrows = hd.w;
             if (CIRC) {
                 // u, weight independent of z; v linear in z
@@ -772,16 +792,33 @@ b2t_status bp3d_tma(const b2t_geom3d *g, int ker, float out_scale, const void *p
     L.tile_row_bytes = (uint32_t)(tile_bu<float>() * esz);
     const int vpt = choose_vpt(g, dtype);
     const int kker = (ker == B2T_KER_FDK_WEIGHTING) ? B2T_KER_DEFAULT : ker;
-    for (uint32_t c0 = 0; c0 < d.angles && st == B2T_OK; c0 += BPT_MAX_VIEWS) {
-        const uint32_t cn = std::min(d.angles - c0, (uint32_t)BPT_MAX_VIEWS);
+    std::vector<BPView> W(d.angles);
+    for (uint32_t a = 0; a < d.angles; ++a) bp_view_coeffs(g->kind, ker, g->views[a], g->vol_scale, W[a]);
+    auto circular = [&](const BPView &w) { return w.nu.z == 0.0f && (g->kind != B2T_GEOM_CONE || w.den.z == 0.0f); };
+    for (uint32_t c0 = 0, cn = 0; c0 < d.angles && st == B2T_OK; c0 += cn) {
+        // a launch of circular views holds more of them
+        cn = std::min(d.angles - c0, (uint32_t)BPT_MAX_VIEWS_CIRC);
+        bool circ = true;
+        for (uint32_t i = 0; i < cn && circ; ++i) circ = circular(W[c0 + i]);
+        if (!circ) {
+            cn = std::min(cn, (uint32_t)BPT_MAX_VIEWS);
+            circ = true;
+            for (uint32_t i = 0; i < cn && circ; ++i) circ = circular(W[c0 + i]);
+        }
         L.a0 = (int)c0;
         L.nviews = (int)cn;
         L.accumulate = (c0 > 0 || mode == B2T_MODE_ADD) ? 1 : 0;
-        bool circ = true;
         for (uint32_t i = 0; i < cn; ++i) {
-            bp_view_coeffs(g->kind, ker, g->views[c0 + i], g->vol_scale, L.views[i]);
-            const BPView &w = L.views[i];
-            if (w.nu.z != 0.0f || (g->kind == B2T_GEOM_CONE && w.den.z != 0.0f)) circ = false;
+            const BPView &w = W[c0 + i];
+            float *f = L.vrec + (circ ? 10 : 12) * i;
+            if (circ) {
+                const float r[10] = {w.nu.x, w.nu.y, w.nu.w, w.nv.x, w.nv.y, w.nv.z, w.nv.w, w.den.x, w.den.y, w.den.w};
+                std::copy(r, r + 10, f);
+            } else {
+                const float r[12] = {w.nu.x, w.nu.y, w.nu.z, w.nu.w, w.nv.x, w.nv.y,
+                                     w.nv.z, w.nv.w, w.den.x, w.den.y, w.den.z, w.den.w};
+                std::copy(r, r + 12, f);
+            }
         }
         if (dtype == B2T_F32) st = launch_shape<float>(L, g->kind, kker, circ, vpt, d, s);
         else if (dtype == B2T_F16) st = launch_shape<__half>(L, g->kind, kker, circ, vpt, d, s);

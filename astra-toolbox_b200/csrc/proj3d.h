@@ -74,7 +74,11 @@ constexpr int BPT_RING_BYTES = 75264; // ring of tile rows (224 rows of 84 4-byt
                                       // reserves) fit an SM's 228 KB
 constexpr int BPT_CTAS_PER_SM = 3;    // resident CTAs (72 registers a thread with 32 accumulators)
 constexpr int BPT_SLOTS = 8;          // views in flight at most (barrier pairs and stage records)
-constexpr int BPT_MAX_VIEWS = 640;
+// Views per launch: their coefficients travel in the launch record, 12
+// floats a view, 10 when every view is circular (nu.z = den.z = 0).
+constexpr int BPT_VIEW_FLOATS = 7680;
+constexpr int BPT_MAX_VIEWS = BPT_VIEW_FLOATS / 12;
+constexpr int BPT_MAX_VIEWS_CIRC = BPT_VIEW_FLOATS / 10;
 
 struct alignas(64) BPTmaLaunch {
     CUtensorMap tmap;       // padded projections: dims (pu, angles, det_v + 4)
@@ -87,7 +91,7 @@ struct alignas(64) BPTmaLaunch {
     int a0, nviews, accumulate;
     float out_scale;
     uint32_t tile_row_bytes;  // bytes per ring row (a launch value: see the kernel's addressing)
-    BPView views[BPT_MAX_VIEWS];
+    float vrec[BPT_VIEW_FLOATS];  // the views' BPView coefficients, packed (see BPT_MAX_VIEWS)
 };
 
 // Row pitch (elements) of the zero-padded projection buffer: det_u plus a

@@ -1361,7 +1361,7 @@ def main():
                 "frac": (achieved / peak_on) if peak_on else None,
                 "traffic": traffic, "units_per_launch": units, "bytes_per_unit": 4 * esz,
                 "traffic_note": "DRAM bytes of one whole call (the FP's x- and y-major launches, or the BP's "
-                                "640- and 80-view launches) from one ncu capture of this workload; the "
+                                "launches) from one ncu capture of this workload; the "
                                 "slice boxes / tiles are re-read on chip, DRAM moves ~1/25 of the algorithmic "
                                 "bytes",
                 "peak_source": "measured on this GPU by b2t_onchip_peak (16-byte streaming loads); the FP "
