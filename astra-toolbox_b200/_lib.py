@@ -136,6 +136,7 @@ SIGNATURES = {
     "b2t_device_errors": (_I32, [_P]),
     "b2t_bp_path_stats": (_I32, [_P]),
     "b2t_fp_path_stats": (_I32, [_P]),
+    "b2t_matched_path_stats": (_I32, [_P]),
     "b2t_cone_views": (_I32, [_U32, _U32, _U32, _F, _F, _F, _F, _P, _P]),
     "b2t_par3d_views": (_I32, [_U32, _U32, _U32, _F, _F, _P, _P]),
     "b2t_vec_views3d": (_I32, [_U32, _U32, _U32, _P, _P]),

@@ -156,6 +156,14 @@ b2t_status b2t_fp_path_stats(uint64_t *stats)
     return fp_path_stats_impl(stats);
 }
 
+b2t_status b2t_matched_path_stats(uint64_t *stats)
+{
+    clear_error();
+    if (!stats) return fail(B2T_ERR_INVALID_ARG, "b2t_matched_path_stats: null pointer");
+    B2T_CUDA_TRY(cudaDeviceSynchronize(), "b2t_matched_path_stats synchronize");
+    return matched_path_stats_impl(stats);
+}
+
 b2t_status b2t_bp_path_stats(uint64_t *stats)
 {
     clear_error();

@@ -40,11 +40,14 @@
 // and returns.  The reference has no such kernel; its FP samples a 3D
 // texture per slice (cone_fp.cu:154-231).
 #include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "b2t_internal.h"
@@ -59,6 +62,9 @@ static __device__ unsigned int g_fp_slab_errors = 0;
 // slices staged in shared memory / read from global memory, summed over CTAs
 // (read and cleared by b2t_fp_path_stats)
 static __device__ unsigned long long g_fp_slab_slices[2] = {0, 0};
+// the same for the transpose (slices whose box went through shared memory /
+// scattered straight into the accumulator; read by b2t_matched_path_stats)
+static __device__ unsigned long long g_mt_slab_slices[2] = {0, 0};
 
 namespace {
 
@@ -81,11 +87,16 @@ constexpr int SPLIT_BITS = 0x4B400000;      // bits of SPLIT_M
 static_assert(SLAB_BY % SLAB_BOX_Y == 0, "buffer made of whole boxes");
 static_assert(4 * SLAB_W <= 32, "the producer projects the corner rays one per lane");
 
+// The launch record of the FP and of its transpose (bp3d_slab_matched_kernel,
+// which reads the projections and writes the accumulator through tmap / acc).
 struct alignas(64) SlabLaunch {
-    CUtensorMap tmap[2];   // slab copy as 8-byte z-pairs, dims (n2 + 4, n1 + 4, n0); box widths WA, WB
+    CUtensorMap tmap[2];   // FP: slab copy as 8-byte z-pairs, dims (n2 + 4, n1 + 4, n0); box widths WA, WB
+                           // transpose: FP32 accumulator, dims (az, ay, n0); box widths MT_WA, MT_WB
     const float2 *copy;    // z-pair (s, k1, k2) at (s * py + k1 + 2) * pz + k2 + 2
     long long py, pz;
-    void *proj;            // output projections [v][angle][u]
+    float *acc;            // transpose: cell (s, k1, k2) at (s * ay + k1 + 2) * az + k2 + 2
+    long long ay, az;
+    void *proj;            // FP: output projections [v][angle][u]; transpose: its input
     long long proj_pitch;
     int n0, n1, n2, nu, nv, na;
     int accumulate;
@@ -178,58 +189,76 @@ __device__ __forceinline__ int warp_max(int v)
 __device__ __forceinline__ float det_uu(const SlabLaunch &L, int u) { return (float)min(u, L.nu - 1) + 0.5f - 0.5f * (float)L.nu; }
 __device__ __forceinline__ float det_vv(const SlabLaunch &L, int v) { return (float)min(v, L.nv - 1) + 0.5f - 0.5f * (float)L.nv; }
 
+// The tile's corner rays (view, column end, row end), set up once: lane
+// c < 4 SLAB_W computes corner c, then every lane holds all of them.  The
+// rays of a detector rectangle cross a slice inside the convex hull of the
+// corners' crossings when their denominators share one sign (hull).
+constexpr int SLAB_NC = 4 * SLAB_W;
+struct Corners {
+    float A1[SLAB_NC], B1[SLAB_NC], A2[SLAB_NC], B2[SLAB_NC];
+    bool hull;
+};
+
+__device__ __forceinline__ void slab_corners(const SlabLaunch &L, int lane, Corners &C)
+{
+    const int c = lane % SLAB_NC;
+    const int w = c >> 2, uc = c & 1, vc = (c >> 1) & 1;
+    const int vi = min((int)blockIdx.x * SLAB_W + w, L.nviews - 1);
+    const int u = (int)blockIdx.y * SLAB_U + (uc ? SLAB_U - 1 : 0);
+    const int v = (int)blockIdx.z * SLAB_ROWS + (vc ? SLAB_ROWS - 1 : 0);
+    float A1, B1h, A2, B2h;
+    const float den = ray_setup(L.views[vi], det_uu(L, u), det_vv(L, v), A1, B1h, A2, B2h);
+    C.hull = __all_sync(0xffffffffu, den > 1e-6f) || __all_sync(0xffffffffu, den < -1e-6f);
+#pragma unroll
+    for (int k = 0; k < SLAB_NC; ++k) {
+        C.A1[k] = __shfl_sync(0xffffffffu, A1, k);
+        C.B1[k] = __shfl_sync(0xffffffffu, B1h, k);
+        C.A2[k] = __shfl_sync(0xffffffffu, A2, k);
+        C.B2[k] = __shfl_sync(0xffffffffu, B2h, k);
+    }
+}
+
+// The box of slice sf from the corners' texels, clamped to the zero border,
+// one texel of margin for rounding: in-plane texels [y0, y1], z texels
+// [zlo, z1].  sane: no corner position so large that its texel saturates.
+__device__ __forceinline__ bool slab_box(const SlabLaunch &L, const Corners &C, float sf, int &y0, int &y1,
+                                         int &zlo, int &z1)
+{
+    int k1lo = 0x7fffffff, k1hi = -0x7fffffff, k2lo = 0x7fffffff, k2hi = -0x7fffffff;
+    bool sane = true;
+#pragma unroll
+    for (int k = 0; k < SLAB_NC; ++k) {
+        const float q1 = fmaf(C.A1[k], sf, C.B1[k]), q2 = fmaf(C.A2[k], sf, C.B2[k]);
+        sane = sane && fabsf(q1) < 1.0e7f && fabsf(q2) < 1.0e7f;
+        const int k1 = min(max(floor_texel(q1), -2), L.n1), k2 = min(max(floor_texel(q2), -2), L.n2);
+        k1lo = min(k1lo, k1);
+        k1hi = max(k1hi, k1);
+        k2lo = min(k2lo, k2);
+        k2hi = max(k2hi, k2);
+    }
+    y0 = max(k1lo - 1, -2);
+    y1 = min(k1hi + 2, L.n1 + 1);
+    zlo = max(k2lo - 1, -2);
+    z1 = min(k2hi + 2, L.n2 + 1);
+    return sane;
+}
+
 // Producer warp: the buffer box of every slice of the CTA's range and its loads.
 __device__ __noinline__ void slab_produce(const SlabLaunch &L, float2 *buf, uint64_t *full, uint64_t *empty,
                                           SlabInfo *info, int lane, int s_lo, int s_hi)
 {
-    // The tile's corner rays (view, column end, row end), set up once: lane
-    // c < 4 SLAB_W computes corner c, then every lane holds all of them.  The
-    // rays of a detector rectangle cross a slice inside the convex hull of the
-    // corners' crossings when their denominators share one sign.
-    constexpr int NC = 4 * SLAB_W;
-    float cA1[NC], cB1[NC], cA2[NC], cB2[NC];
-    bool hull;
-    {
-        const int c = lane % NC;
-        const int w = c >> 2, uc = c & 1, vc = (c >> 1) & 1;
-        const int vi = min((int)blockIdx.x * SLAB_W + w, L.nviews - 1);
-        const int u = (int)blockIdx.y * SLAB_U + (uc ? SLAB_U - 1 : 0);
-        const int v = (int)blockIdx.z * SLAB_ROWS + (vc ? SLAB_ROWS - 1 : 0);
-        float A1, B1h, A2, B2h;
-        const float den = ray_setup(L.views[vi], det_uu(L, u), det_vv(L, v), A1, B1h, A2, B2h);
-        hull = __all_sync(0xffffffffu, den > 1e-6f) || __all_sync(0xffffffffu, den < -1e-6f);
-#pragma unroll
-        for (int k = 0; k < NC; ++k) {
-            cA1[k] = __shfl_sync(0xffffffffu, A1, k);
-            cB1[k] = __shfl_sync(0xffffffffu, B1h, k);
-            cA2[k] = __shfl_sync(0xffffffffu, A2, k);
-            cB2[k] = __shfl_sync(0xffffffffu, B2h, k);
-        }
-    }
+    Corners C;
+    slab_corners(L, lane, C);
     const uint32_t sbuf = smem_u32(buf);
     const int nst = s_hi - s_lo + 1;
     unsigned long long n_staged = 0, n_global = 0;
     for (int b0 = 0; b0 < nst; b0 += 32) {
-        // lane k: the buffer box of slice s_lo + b0 + k from the corners'
-        // texels, clamped to the zero border, one texel of margin for rounding
-        const float sf = (float)(s_lo + b0 + lane);
-        int k1lo = 0x7fffffff, k1hi = -0x7fffffff, k2lo = 0x7fffffff, k2hi = -0x7fffffff;
-        bool sane = true;
-#pragma unroll
-        for (int k = 0; k < NC; ++k) {
-            const float q1 = fmaf(cA1[k], sf, cB1[k]), q2 = fmaf(cA2[k], sf, cB2[k]);
-            sane = sane && fabsf(q1) < 1.0e7f && fabsf(q2) < 1.0e7f;
-            const int k1 = min(max(floor_texel(q1), -2), L.n1), k2 = min(max(floor_texel(q2), -2), L.n2);
-            k1lo = min(k1lo, k1);
-            k1hi = max(k1hi, k1);
-            k2lo = min(k2lo, k2);
-            k2hi = max(k2hi, k2);
-        }
-        const int y0 = max(k1lo - 1, -2), y1 = min(k1hi + 2, L.n1 + 1);
-        const int zlo = max(k2lo - 1, -2), z1 = min(k2hi + 2, L.n2 + 1);
+        // lane k: the buffer box of slice s_lo + b0 + k
+        int y0, y1, zlo, z1;
+        const bool sane = slab_box(L, C, (float)(s_lo + b0 + lane), y0, y1, zlo, z1);
         const int z0 = ((zlo + 2) & ~1) - 2;  // TMA: (z0 + 2) * 8 bytes on a 16-byte boundary
         const int ny = y1 - y0 + 1, nz = z1 - z0 + 1;
-        const int sel = (!hull || !sane || ny > SLAB_BY || nz > SLAB_WB) ? -1 : (nz <= SLAB_WA ? 0 : 1);
+        const int sel = (!C.hull || !sane || ny > SLAB_BY || nz > SLAB_WB) ? -1 : (nz <= SLAB_WA ? 0 : 1);
         const int pitch = sel == 0 ? SLAB_WA : SLAB_WB;
         const int nby = (ny + SLAB_BOX_Y - 1) / SLAB_BOX_Y;
         const int cnt = min(32, nst - b0);
@@ -528,6 +557,397 @@ __global__ void __launch_bounds__(SLAB_THREADS, 2) fp3d_slab_kernel(const __grid
     }
 }
 
+// ---------------------------------------------------------------------------
+// The FP's transpose on the same tiles (projection kernel "matched_bp" for
+// the views the slab FP takes).  A CTA takes the rays of one FP tile
+// (SLAB_W views x SLAB_U columns x SLAB_ROWS rows) and walks the same slices:
+// each sample's four bilinear taps, weighted as the FP weighs the texels it
+// reads at that sample, are added with shared-memory reductions into an
+// FP32 box of the slice (the FP's buffer box, as single floats); the
+// producer warp zeroes each box before its slice and, MT_LAG slices after
+// the compute warps have finished it, adds the box into an FP32
+// accumulator in global memory with TMA reduce-adds (cp.reduce.async.bulk
+// .tensor .add, one per SLAB_BOX_Y rows).  The accumulator has the slab
+// copy's layout (slice, in-plane texel + 2, z texel + 2) with room past the
+// far borders, so that no box leaves it; fold_cells (matched.cu) adds its
+// interior into the volume.  Global memory sees one reduction per box cell
+// instead of one per tap.
+//
+// Measured on B200 (512^3 x 720 views, 832^2 detector) this is 4.1x slower
+// than the per-sample global reductions of matched.cu (1538 against 372 ms;
+// 98.5 against 23.3 ms at 256^3 x 360, 416^2): FP32 reductions into shared
+// memory are not a native operation there (ncu counts 13.5 shared-memory
+// atomic instructions and 88 instructions per warp-sample where the kernel
+// issues 4 reductions), while the same kernel with 32-bit integer reductions
+// at the same addresses takes 29.9 ms and with plain stores 16.8 ms, which
+// bounds any shared-memory accumulation of this tiling at 0.72x of the
+// scatter.  So the scatter kernels stay the default and this kernel runs
+// only when B2T_MATCHED_PATH=slab selects it.
+//
+// A tap lands inside its box for the reason an FP sample reads inside it:
+// at a slice, the rays of a detector rectangle whose denominators share a
+// sign cross it inside the hull of the corner rays' crossings, and the box
+// is that hull's texel range with a texel of margin; samples outside the
+// volume are clamped to the zero border exactly as the FP clamps them (their
+// taps land on border cells, which the fold drops).
+constexpr int MT_STAGES = 4;              // slice boxes in flight
+constexpr int MT_LAG = 2;                 // slices between a box's last scatter and its flush
+constexpr int MT_WA = 96, MT_WB = 160;    // box widths (floats): a box's row pitch
+constexpr int MT_SLOT = SLAB_BY * MT_WB;  // floats per box
+static_assert(MT_LAG >= 1 && MT_LAG < MT_STAGES, "a box is flushed before its slot comes round again");
+static_assert((MT_WA * 4 * SLAB_BOX_Y) % 128 == 0 && (MT_WB * 4 * SLAB_BOX_Y) % 128 == 0,
+              "TMA boxes start on 128-byte boundaries of a slot");
+
+// A slice's box: sel 0 / 1 the width MT_WA / MT_WB, -1 scattered straight
+// into the accumulator; rbase as in SlabInfo (4-byte cells); (zc, yc) the
+// box origin in accumulator coordinates, nby its TMA boxes, s the slice
+struct MTInfo {
+    int sel, rbase, zc, yc, nby, s, pad0, pad1;
+};
+
+// The lane's rays: both views, SLAB_R rows each, with the value each
+// carries back (projection value x the FP's output scale of the ray)
+struct TRays {
+    float A1[SLAB_W], B1h[SLAB_W];
+    float A2[SLAB_W][SLAB_R], B2h[SLAB_W][SLAB_R];
+    float wv[SLAB_W][SLAB_R];
+};
+
+template <typename T> __device__ __forceinline__ float ld_proj(const T *p);
+template <> __device__ __forceinline__ float ld_proj<float>(const float *p) { return __ldg(p); }
+template <> __device__ __forceinline__ float ld_proj<__half>(const __half *p) { return __half2float(__ldg(p)); }
+template <> __device__ __forceinline__ float ld_proj<__nv_bfloat16>(const __nv_bfloat16 *p)
+{
+    return __bfloat162float(__ldg(p));
+}
+
+template <int OFF> __device__ __forceinline__ void red_smem(uint32_t a, float v)
+{
+    asm volatile("red.shared.add.f32 [%0+%1], %2;" ::"r"(a), "n"(OFF), "f"(v) : "memory");
+}
+
+// One slice of the lane's rays into a box of row pitch P (floats); CLAMP as
+// in sample_smem.  The taps of a sample at base texel (k1, k2) with weights
+// f1 (in-plane) and f2 (z): (1 - f1) (1 - f2), (1 - f1) f2, f1 (1 - f2),
+// f1 f2 at (k1, k2), (k1, k2 + 1), (k1 + 1, k2), (k1 + 1, k2 + 1).
+template <int P, bool CLAMP, int RE>
+__device__ __forceinline__ void scatter_smem(const SlabLaunch &L, uint32_t rb, float sf, const TRays &R)
+{
+    constexpr uint32_t ROWB = 4u * P;
+#pragma unroll
+    for (int w = 0; w < SLAB_W; ++w) {
+        const float q1 = fmaf(R.A1[w], sf, R.B1h[w]);
+        const float t1 = __fadd_rd(q1, SPLIT_M);
+        const float f1 = q1 - (t1 - SPLIT_M);
+        const float g1 = 1.0f - f1;
+        int b1 = __float_as_int(t1);
+        if (CLAMP) b1 = min(max(b1, SPLIT_BITS - 2), SPLIT_BITS + L.n1);
+        const uint32_t row = (uint32_t)b1 * ROWB + rb;
+        const uint64_t sf2 = pk2(sf, sf), M2 = pk2(SPLIT_M, SPLIT_M), nM2 = pk2(-SPLIT_M, -SPLIT_M);
+        const uint64_t f12 = pk2(f1, f1), g12 = pk2(g1, g1);
+#pragma unroll
+        for (int r = 0; r + 1 < RE; r += 2) {
+            const uint64_t q2 = fma2(pk2(R.A2[w][r], R.A2[w][r + 1]), sf2, pk2(R.B2h[w][r], R.B2h[w][r + 1]));
+            const uint64_t t2 = add2_rd(q2, M2);
+            const uint64_t f2 = sub2(q2, add2(t2, nM2));
+            const float2 tb = upk2(t2);
+            int b2a = __float_as_int(tb.x), b2b = __float_as_int(tb.y);
+            if (CLAMP) {
+                b2a = min(max(b2a, SPLIT_BITS - 2), SPLIT_BITS + L.n2);
+                b2b = min(max(b2b, SPLIT_BITS - 2), SPLIT_BITS + L.n2);
+            }
+            const uint32_t a0 = (uint32_t)b2a * 4u + row, a1 = (uint32_t)b2b * 4u + row;
+            const uint64_t c = pk2(R.wv[w][r], R.wv[w][r + 1]);
+            const uint64_t cb = mul2(c, f2), ca = sub2(c, cb);
+            const float2 la = upk2(mul2(g12, ca)), lb = upk2(mul2(g12, cb));
+            const float2 ha = upk2(mul2(f12, ca)), hb = upk2(mul2(f12, cb));
+            red_smem<0>(a0, la.x);
+            red_smem<4>(a0, lb.x);
+            red_smem<(int)ROWB>(a0, ha.x);
+            red_smem<(int)ROWB + 4>(a0, hb.x);
+            red_smem<0>(a1, la.y);
+            red_smem<4>(a1, lb.y);
+            red_smem<(int)ROWB>(a1, ha.y);
+            red_smem<(int)ROWB + 4>(a1, hb.y);
+        }
+        if constexpr (RE % 2 == 1) {
+            constexpr int r = RE - 1;
+            const float q2 = fmaf(R.A2[w][r], sf, R.B2h[w][r]);
+            const float t2 = __fadd_rd(q2, SPLIT_M);
+            const float f2 = q2 - (t2 - SPLIT_M);
+            int b2 = __float_as_int(t2);
+            if (CLAMP) b2 = min(max(b2, SPLIT_BITS - 2), SPLIT_BITS + L.n2);
+            const uint32_t a = (uint32_t)b2 * 4u + row;
+            const float cb = R.wv[w][r] * f2, ca = R.wv[w][r] - cb;
+            red_smem<0>(a, g1 * ca);
+            red_smem<4>(a, g1 * cb);
+            red_smem<(int)ROWB>(a, f1 * ca);
+            red_smem<(int)ROWB + 4>(a, f1 * cb);
+        }
+    }
+}
+
+// The same straight into the accumulator (a slice whose box did not fit).
+template <int RE>
+__device__ __forceinline__ void scatter_global(const SlabLaunch &L, int s, float sf, const TRays &R)
+{
+#pragma unroll
+    for (int w = 0; w < SLAB_W; ++w) {
+        const float q1 = fmaf(R.A1[w], sf, R.B1h[w]);
+        const float t1 = __fadd_rd(q1, SPLIT_M);
+        const float f1 = q1 - (t1 - SPLIT_M);
+        const float g1 = 1.0f - f1;
+        const int k1 = min(max(__float_as_int(t1) - SPLIT_BITS, -2), L.n1);
+        float *row = L.acc + ((long long)s * L.ay + k1 + 2) * L.az + 2;
+#pragma unroll
+        for (int r = 0; r < RE; ++r) {
+            const float q2 = fmaf(R.A2[w][r], sf, R.B2h[w][r]);
+            const float t2 = __fadd_rd(q2, SPLIT_M);
+            const float f2 = q2 - (t2 - SPLIT_M);
+            const int k2 = min(max(__float_as_int(t2) - SPLIT_BITS, -2), L.n2);
+            const float cb = R.wv[w][r] * f2, ca = R.wv[w][r] - cb;
+            atomicAdd(row + k2, g1 * ca);
+            atomicAdd(row + k2 + 1, g1 * cb);
+            atomicAdd(row + L.az + k2, f1 * ca);
+            atomicAdd(row + L.az + k2 + 1, f1 * cb);
+        }
+    }
+}
+
+// Producer warp of the transpose: for every slice of the CTA's range, in
+// order, flush the box finished MT_LAG slices earlier, then zero the slot
+// of this slice's box and hand it to the compute warps.
+__device__ __noinline__ void mt_produce(const SlabLaunch &L, float *buf, uint64_t *ready, uint64_t *done,
+                                        MTInfo *info, int lane, int s_lo, int s_hi)
+{
+    Corners C;
+    slab_corners(L, lane, C);
+    const int nst = s_hi - s_lo + 1;
+    unsigned long long n_staged = 0, n_global = 0;
+    bool ok = true;
+    // wait for the compute warps to finish slice st, then (lane 0) reduce its
+    // box into the accumulator; every slice commits one bulk group
+    auto flush = [&](int st) -> bool {
+        const int slot = st % MT_STAGES;
+        if (!__all_sync(0xffffffffu,
+                        mbar_wait_bounded_sleep(&done[slot], (uint32_t)((st / MT_STAGES) & 1), SLAB_WAIT))) {
+            if (lane == 0) atomicOr(&g_fp_slab_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
+            return false;
+        }
+        if (lane == 0) {
+            const MTInfo I = info[slot];
+            if (I.sel >= 0) {
+                const int pitch = I.sel == 0 ? MT_WA : MT_WB;
+                const float *src = buf + (size_t)slot * MT_SLOT;
+                for (int by = 0; by < I.nby; ++by)
+                    tma_reduce_add_3d(&L.tmap[I.sel], src + (size_t)(by * SLAB_BOX_Y) * pitch, I.zc,
+                                      I.yc + by * SLAB_BOX_Y, I.s);
+            }
+            bulk_commit_group();
+        }
+        __syncwarp();
+        return true;
+    };
+    for (int b0 = 0; b0 < nst && ok; b0 += 32) {
+        // lane k: the box of slice s_lo + b0 + k
+        int y0, y1, zlo, z1;
+        const bool sane = slab_box(L, C, (float)(s_lo + b0 + lane), y0, y1, zlo, z1);
+        const int z0 = ((zlo + 2) & ~3) - 2;  // TMA: (z0 + 2) * 4 bytes on a 16-byte boundary
+        const int ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+        const int sel_l = (!C.hull || !sane || ny > SLAB_BY || nz > MT_WB) ? -1 : (nz <= MT_WA ? 0 : 1);
+        const int nby_l = (ny + SLAB_BOX_Y - 1) / SLAB_BOX_Y;
+        const int cnt = min(32, nst - b0);
+        if (lane < cnt) {
+            if (sel_l >= 0) ++n_staged;
+            else ++n_global;
+        }
+        for (int k = 0; k < cnt; ++k) {
+            const int st = b0 + k;
+            const int slot = st % MT_STAGES;
+            if (st >= MT_LAG && !flush(st - MT_LAG)) {
+                ok = false;
+                break;
+            }
+            // the slot's previous box (slice st - MT_STAGES) has been read by
+            // its reduce: it was committed MT_STAGES - MT_LAG groups ago
+            if (st >= MT_STAGES && lane == 0) bulk_wait_group_read<MT_STAGES - MT_LAG>();
+            __syncwarp();
+            const int sel = __shfl_sync(0xffffffffu, sel_l, k);
+            const int y0k = __shfl_sync(0xffffffffu, y0, k);
+            const int z0k = __shfl_sync(0xffffffffu, z0, k);
+            const int nby = __shfl_sync(0xffffffffu, nby_l, k);
+            float *slotp = buf + (size_t)slot * MT_SLOT;
+            if (sel >= 0) {
+                const int n4 = nby * SLAB_BOX_Y * (sel == 0 ? MT_WA : MT_WB) / 4;
+                float4 *z4 = reinterpret_cast<float4 *>(slotp);
+                for (int i = lane; i < n4; i += 32) z4[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+            if (lane == 0) {
+                const int pitch = sel == 0 ? MT_WA : MT_WB;
+                MTInfo r;
+                r.sel = sel;
+                r.rbase = (int)(0u - (uint32_t)(SPLIT_BITS + y0k) * (uint32_t)(4 * pitch) -
+                                (uint32_t)(SPLIT_BITS + z0k) * 4u);
+                r.zc = z0k + 2;
+                r.yc = y0k + 2;
+                r.nby = nby;
+                r.s = s_lo + st;
+                r.pad0 = r.pad1 = 0;
+                info[slot] = r;
+            }
+            // every lane releases its own zero stores
+            mbar_arrive(&ready[slot]);
+        }
+    }
+    if (ok) {
+        for (int st = max(0, nst - MT_LAG); st < nst; ++st) {
+            if (!flush(st)) {
+                ok = false;
+                break;
+            }
+        }
+    }
+    // the reduces complete before the CTA leaves (on a timeout too)
+    if (lane == 0) bulk_wait_group_all();
+    __syncwarp();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n_staged += __shfl_xor_sync(0xffffffffu, n_staged, o);
+        n_global += __shfl_xor_sync(0xffffffffu, n_global, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&g_mt_slab_slices[0], n_staged);
+        atomicAdd(&g_mt_slab_slices[1], n_global);
+    }
+}
+
+// A compute warp's pass over the CTA's slices (rows r < RE): wait for the
+// slice's zeroed box, scatter, hand it back.  False when a wait gave up.
+template <int RE>
+__device__ __forceinline__ bool mt_consume(const SlabLaunch &L, const float *buf, uint64_t *ready, uint64_t *done,
+                                           const MTInfo *info, int lane, const Range &rg, const TRays &R)
+{
+    const uint32_t sbase = smem_u32(buf);
+    int slot = 0;
+    uint32_t par = 0;
+    float sf = (float)rg.s_lo;
+    for (int s = rg.s_lo; s <= rg.s_hi; ++s, sf += 1.0f) {
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&ready[slot], par, SLAB_WAIT))) {
+            if (lane == 0) atomicOr(&g_fp_slab_errors, (unsigned)B2T_DEVERR_WAIT_TIMEOUT);
+            return false;
+        }
+        if (s >= rg.wlo && s <= rg.whi) {
+            const MTInfo &I = info[slot];
+            const int sel = I.sel;
+            const uint32_t rb = sbase + (uint32_t)slot * (MT_SLOT * 4u) + (uint32_t)I.rbase;
+            const bool fast = s >= rg.ilo && s <= rg.ihi;
+            if (sel == 0) {
+                if (fast) scatter_smem<MT_WA, false, RE>(L, rb, sf, R);
+                else scatter_smem<MT_WA, true, RE>(L, rb, sf, R);
+            } else if (sel == 1) {
+                if (fast) scatter_smem<MT_WB, false, RE>(L, rb, sf, R);
+                else scatter_smem<MT_WB, true, RE>(L, rb, sf, R);
+            } else {
+                scatter_global<RE>(L, s, sf, R);
+            }
+            // the reductions are visible to the TMA reduce that reads the box
+            if (sel >= 0) fence_proxy_async_smem();
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&done[slot]);
+        if (++slot == MT_STAGES) {
+            slot = 0;
+            par ^= 1u;
+        }
+    }
+    return true;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SLAB_THREADS, 2) bp3d_slab_matched_kernel(const __grid_constant__ SlabLaunch L)
+{
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    float *buf = reinterpret_cast<float *>(smraw);
+    uint64_t *ready = reinterpret_cast<uint64_t *>(smraw + (size_t)MT_STAGES * MT_SLOT * sizeof(float));
+    uint64_t *done = ready + MT_STAGES;
+    MTInfo *info = reinterpret_cast<MTInfo *>(done + MT_STAGES);
+    int *range = reinterpret_cast<int *>(info + MT_STAGES);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (int k = 0; k < MT_STAGES; ++k) {
+            mbar_init(&ready[k], 32);
+            mbar_init(&done[k], SLAB_WARPS);
+        }
+        range[0] = 0x7fffffff;
+        range[1] = -0x7fffffff;
+        mbar_fence_init();
+        tma_prefetch_map(&L.tmap[0]);
+        tma_prefetch_map(&L.tmap[1]);
+    }
+    __syncthreads();
+
+    // ---- ray set-up (compute warps), as in fp3d_slab_kernel, plus the
+    // value each ray carries back: rays off the detector carry zero
+    const int u_raw = (int)blockIdx.y * SLAB_U + warp;
+    TRays R;
+    int wlo = 1, whi = 0, ilo = 1, ihi = 0;
+    if (warp < SLAB_WARPS) {
+        const float uu = det_uu(L, u_raw);
+        int lo_u = 0x7fffffff, hi_u = -0x7fffffff, lo_i = -0x7fffffff, hi_i = 0x7fffffff;
+#pragma unroll
+        for (int w = 0; w < SLAB_W; ++w) {
+            const int vi = (int)blockIdx.x * SLAB_W + w;
+            const FPView &V = L.views[min(vi, L.nviews - 1)];
+#pragma unroll
+            for (int r = 0; r < SLAB_R; ++r) {
+                const int v = (int)blockIdx.z * SLAB_ROWS + lane + 32 * r;
+                float a1, b1;
+                ray_setup(V, uu, det_vv(L, v), a1, b1, R.A2[w][r], R.B2h[w][r]);
+                R.A1[w] = a1;
+                R.B1h[w] = b1;
+                float val = 0.0f;
+                if (vi < L.nviews && u_raw < L.nu && v < L.nv)
+                    val = ld_proj(static_cast<const T *>(L.proj) + ((size_t)v * L.na + V.a) * L.proj_pitch + u_raw);
+                const float sc =
+                    sqrtf(fmaf(a1 * a1, L.f1, fmaf(R.A2[w][r] * R.A2[w][r], L.f2, 1.0f))) * L.mul;
+                R.wv[w][r] = val * sc;
+                int lo = 0, hi = L.n0 - 1;
+                clip_axis(a1, b1, L.n1, L.n0, lo, hi);
+                clip_axis(R.A2[w][r], R.B2h[w][r], L.n2, L.n0, lo, hi);
+                if (lo <= hi) {
+                    lo_u = min(lo_u, lo);
+                    hi_u = max(hi_u, hi);
+                }
+                lo_i = max(lo_i, lo);
+                hi_i = min(hi_i, hi);
+            }
+        }
+        wlo = warp_min(lo_u);
+        whi = warp_max(hi_u);
+        ilo = warp_max(lo_i);
+        ihi = warp_min(hi_i);
+        if (lane == 0 && wlo <= whi) {
+            atomicMin(&range[0], wlo);
+            atomicMax(&range[1], whi);
+        }
+    }
+    __syncthreads();
+    const int s_lo = range[0], s_hi = range[1];
+
+    if (warp == SLAB_WARPS) {
+        if (s_lo <= s_hi) mt_produce(L, buf, ready, done, info, lane, s_lo, s_hi);
+        return;
+    }
+    const int re = min(SLAB_R, (L.nv - (int)blockIdx.z * SLAB_ROWS + 31) >> 5);
+    const Range rg{s_lo, s_hi, wlo, whi, ilo, ihi};
+    if (re >= 4) (void)mt_consume<4>(L, buf, ready, done, info, lane, rg, R);
+    else if (re == 3) (void)mt_consume<3>(L, buf, ready, done, info, lane, rg, R);
+    else if (re == 2) (void)mt_consume<2>(L, buf, ready, done, info, lane, rg, R);
+    else (void)mt_consume<1>(L, buf, ready, done, info, lane, rg, R);
+}
+
 // Slab copy of marching axis dir (0: slices along x, in-plane axis y; 1:
 // slices along y, in-plane axis x) as z-pairs: texel (s, k1, k2) holds
 // (v[k2], v[k2 + 1] - v[k2]) at (s * py + k1 + 2) * pz + k2 + 2, written for
@@ -683,6 +1103,122 @@ b2t_status fp_slab_project(const b2t_geom3d *g, const b2t_params3d *p, const voi
     }
     delete Lp;
     return st;
+}
+
+// ---- the FP's transpose (matched BP) for the views the slab FP takes
+
+static std::atomic<unsigned long long> g_mt_launches{0};
+
+bool matched_slab_eligible(const b2t_geom3d *g, const b2t_params3d *p, int dir, const std::vector<int> &dirs)
+{
+    // opt-in (B2T_MATCHED_PATH=slab): the per-sample global reductions of
+    // matched.cu are faster on this hardware, see the kernel's comment
+    const char *e = std::getenv("B2T_MATCHED_PATH");
+    if (!(e && std::string(e) == "slab") || dir > 1 || p->det_supersample != 1) return false;
+    const b2t_dims3d &d = g->dims;
+    for (uint32_t a = 0; a < d.angles; ++a) {
+        if (dirs[a] != dir) continue;
+        FPView w;
+        fp_view_coeffs(g->kind, g->views[a], d, dir, w);
+        if (w.e[2] != 0.0f || w.m1[2] != 0.0f || w.n1[2] != 0.0f) return false;
+    }
+    return true;
+}
+
+void matched_slab_dims(const b2t_dims3d &d, int dir, long long &ay, long long &az)
+{
+    // room for a whole box past the far border: no TMA reduce leaves the array
+    ay = (long long)(dir == 0 ? d.vol_y : d.vol_x) + 4 + SLAB_BY;
+    az = ((long long)d.vol_z + 4 + MT_WB + 3) & ~3ll;
+}
+
+size_t matched_slab_acc_bytes(const b2t_dims3d &d, int dir)
+{
+    long long ay, az;
+    matched_slab_dims(d, dir, ay, az);
+    return (size_t)(dir == 0 ? d.vol_x : d.vol_y) * (size_t)ay * (size_t)az * sizeof(float);
+}
+
+template <typename T> static b2t_status launch_mt(const SlabLaunch &L, dim3 grid, size_t smem, cudaStream_t s)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        B2T_CUDA_TRY(cudaFuncSetAttribute(bp3d_slab_matched_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem),
+                     "slab matched BP shared memory attribute");
+        attr_set = true;
+    }
+    bp3d_slab_matched_kernel<T><<<grid, SLAB_THREADS, smem, s>>>(L);
+    count_launches(1);
+    g_mt_launches.fetch_add(1);
+    B2T_CUDA_TRY(cudaGetLastError(), "bp3d_slab_matched_kernel launch");
+    return B2T_OK;
+}
+
+b2t_status matched_slab_scatter(const b2t_geom3d *g, const b2t_params3d *p, const void *proj, size_t proj_pitch,
+                                int32_t dtype, int dir, const std::vector<int> &dirs, float *acc, cudaStream_t s)
+{
+    const b2t_dims3d &d = g->dims;
+    SlabLaunch *Lp = new SlabLaunch;
+    SlabLaunch &L = *Lp;
+    L.n0 = dir == 0 ? d.vol_x : d.vol_y;
+    L.n1 = dir == 0 ? d.vol_y : d.vol_x;
+    L.n2 = d.vol_z;
+    L.copy = nullptr;
+    L.py = L.pz = 0;
+    L.acc = acc;
+    matched_slab_dims(d, dir, L.ay, L.az);
+    const uint64_t dims[3] = {(uint64_t)L.az, (uint64_t)L.ay, (uint64_t)L.n0};
+    const uint64_t strides[2] = {(uint64_t)L.az * sizeof(float), (uint64_t)(L.az * L.ay) * sizeof(float)};
+    b2t_status st = B2T_OK;
+    for (int k = 0; k < 2 && st == B2T_OK; ++k) {
+        const uint32_t box[3] = {(uint32_t)(k == 0 ? MT_WA : MT_WB), SLAB_BOX_Y, 1};
+        st = encode_tensor_map(&L.tmap[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, acc, dims, strides, box);
+    }
+    if (st != B2T_OK) {
+        delete Lp;
+        return st;
+    }
+    L.proj = const_cast<void *>(proj);
+    L.proj_pitch = (long long)proj_pitch;
+    L.nu = d.det_u;
+    L.nv = d.det_v;
+    L.na = d.angles;
+    L.accumulate = 0;
+    fp_scale(g->kind, dir, g->vol_scale, false, p->output_scale, L.f1, L.f2, L.mul);
+    std::vector<int> views;
+    for (uint32_t a = 0; a < d.angles; ++a)
+        if (dirs[a] == dir) views.push_back((int)a);
+    const size_t smem = (size_t)MT_STAGES * MT_SLOT * sizeof(float) +
+                        MT_STAGES * (2 * sizeof(uint64_t) + sizeof(MTInfo)) + 2 * sizeof(int);
+    for (size_t c0 = 0; c0 < views.size() && st == B2T_OK; c0 += SLAB_MAX_VIEWS) {
+        const size_t cn = std::min(views.size() - c0, (size_t)SLAB_MAX_VIEWS);
+        L.nviews = (int)cn;
+        for (size_t i = 0; i < cn; ++i) {
+            fp_view_coeffs(g->kind, g->views[views[c0 + i]], d, dir, L.views[i]);
+            L.views[i].a = views[c0 + i];
+        }
+        dim3 grid((unsigned)((cn + SLAB_W - 1) / SLAB_W), (d.det_u + SLAB_U - 1) / SLAB_U,
+                  (d.det_v + SLAB_ROWS - 1) / SLAB_ROWS);
+        if (dtype == B2T_F32) st = launch_mt<float>(L, grid, smem, s);
+        else if (dtype == B2T_F16) st = launch_mt<__half>(L, grid, smem, s);
+        else st = launch_mt<__nv_bfloat16>(L, grid, smem, s);
+    }
+    delete Lp;
+    return st;
+}
+
+b2t_status matched_path_stats_impl(uint64_t *stats)
+{
+    unsigned long long v[2] = {0, 0};
+    B2T_CUDA_TRY(cudaMemcpyFromSymbol(v, g_mt_slab_slices, sizeof(v)), "read matched BP path statistics");
+    const unsigned long long zero[2] = {0, 0};
+    B2T_CUDA_TRY(cudaMemcpyToSymbol(g_mt_slab_slices, zero, sizeof(zero)), "clear matched BP path statistics");
+    stats[0] = v[0];
+    stats[1] = v[1];
+    stats[2] = g_mt_launches.exchange(0);
+    stats[3] = matched_scatter_launches_take();
+    return B2T_OK;
 }
 
 }  // namespace b2t

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <vector>
 
@@ -280,10 +281,14 @@ __global__ void __launch_bounds__(256) fp3d_transpose_cols_kernel(const __grid_c
 // accumulator accA[z+2][y+2][x+2]; a voxel's taps are .x of its own cell,
 // .y of the cell before it along k1, .z before it along k2, .w before both.
 // Threads run along z, the cells' contiguous axis.
+// Views of the slab transpose (fp3d_slab.cu) come as plain FP32 sums per
+// voxel in its accumulators m0 (x-major: cell (x, y, z) at (x ay0 + y + 2)
+// az + z + 2) and m1 (y-major: (y ay1 + x + 2) az + z + 2).
 template <typename T>
 __global__ void fold_cells(const float4 *__restrict__ c0, const float4 *__restrict__ c1,
-                           const float *__restrict__ accA, int nx, int ny, int nz, T *__restrict__ out,
-                           size_t pitch, int accumulate)
+                           const float *__restrict__ accA, const float *__restrict__ m0,
+                           const float *__restrict__ m1, long long ay0, long long ay1, long long az, int nx, int ny,
+                           int nz, T *__restrict__ out, size_t pitch, int accumulate)
 {
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
     const int x = blockIdx.y;
@@ -299,6 +304,8 @@ __global__ void fold_cells(const float4 *__restrict__ c0, const float4 *__restri
     if (c0) taps(c0, y + 2, nx, x);
     if (c1) taps(c1, x + 2, ny, y);
     if (accA) r += accA[((size_t)(z + 2) * (ny + 4) + (y + 2)) * (nx + 4) + (x + 2)];
+    if (m0) r += m0[((long long)x * ay0 + y + 2) * az + z + 2];
+    if (m1) r += m1[((long long)y * ay1 + x + 2) * az + z + 2];
     T *o = out + ((size_t)z * ny + y) * pitch + x;
     if (accumulate) r += ldm_plain(o);
     *o = tom<T>(r);
@@ -325,6 +332,8 @@ __global__ void fold_accumulators(const float *__restrict__ accA, const float *_
 // B2T_MATCHED_PLAIN=1 selects the per-lane reductions of
 // fp3d_transpose_cols_kernel (the path of arrays of 2^32 cells or more)
 // instead of the merged ones (same sums, another order; tests compare them).
+std::atomic<unsigned long long> g_scatter_launches{0};
+
 bool matched_force_plain()
 {
     const char *e = getenv("B2T_MATCHED_PLAIN");
@@ -335,6 +344,7 @@ template <typename T> b2t_status launch_T(const FPLaunch &L, dim3 grid, cudaStre
 {
     fp3d_transpose_kernel<T><<<grid, dim3(32, 8), 0, s>>>(L);
     count_launches(1);
+    g_scatter_launches.fetch_add(1);
     B2T_CUDA_TRY(cudaGetLastError(), "matched bp kernel launch");
     return B2T_OK;
 }
@@ -352,6 +362,8 @@ b2t_status launch_fold(const float *a, const float *b, const b2t_dims3d &d, void
 }
 
 }  // namespace
+
+unsigned long long matched_scatter_launches_take() { return g_scatter_launches.exchange(0); }
 
 b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const void *proj,
                              size_t proj_pitch, void *vol, size_t vol_pitch, int32_t dtype,
@@ -375,10 +387,25 @@ b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const v
     {
         // cell-space accumulators for x- and y-major views (one vector
         // reduction per sample); the scalar path below when they do not fit
-        Scratch cacc[2], sz;
+        Scratch cacc[2], sz, macc[2];
         bool ok = true;
+        // the slab transpose for the directions whose views it takes (its
+        // accumulators hold single floats), else cell accumulators
+        bool slab[2] = {false, false};
+        for (int dir = 0; dir < 2; ++dir) {
+            if (!need[dir] || !matched_slab_eligible(g, p, dir, dirs)) continue;
+            const size_t bytes = matched_slab_acc_bytes(d, dir);
+            const b2t_status st = macc[dir].alloc(bytes, s, "matched bp slab accumulator");
+            if (st == B2T_ERR_NO_MEMORY) {
+                clear_error();
+                continue;
+            }
+            B2T_TRY(st);
+            B2T_CUDA_TRY(cudaMemsetAsync(macc[dir].as<void>(), 0, bytes, s), "matched bp memset");
+            slab[dir] = true;
+        }
         for (int dir = 0; dir < 2 && ok; ++dir) {
-            if (!need[dir]) continue;
+            if (!need[dir] || slab[dir]) continue;
             const size_t count = (dir == 0 ? py : px) * (size_t)(dir == 0 ? d.vol_x : d.vol_y) * pz;
             const b2t_status st = cacc[dir].alloc(count * sizeof(float4), s, "matched bp cell accumulator");
             if (st == B2T_ERR_NO_MEMORY) {
@@ -406,6 +433,10 @@ b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const v
             b2t_status st = B2T_OK;
             for (int dir = 0; dir < 3 && st == B2T_OK; ++dir) {
                 if (!need[dir]) continue;
+                if (dir < 2 && slab[dir]) {
+                    st = matched_slab_scatter(g, p, proj, proj_pitch, dtype, dir, dirs, macc[dir].as<float>(), s);
+                    continue;
+                }
                 P.proj = const_cast<void *>(proj);
                 P.proj_pitch = (long long)proj_pitch;
                 P.nu = d.det_u;
@@ -457,6 +488,7 @@ b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const v
                             else fp3d_transpose_cols_kernel<__nv_bfloat16, false><<<grid, dim3(32, 8), 0, s>>>(P);
                         }
                         count_launches(1);
+                        g_scatter_launches.fetch_add(1);
                         if (cudaGetLastError() != cudaSuccess) st = fail(B2T_ERR_CUDA, "matched bp (cells) launch");
                     }
                 }
@@ -465,19 +497,24 @@ b2t_status matched_bp3d_impl(const b2t_geom3d *g, const b2t_params3d *p, const v
             B2T_TRY(st);
             const int accumulate = (mode == B2T_MODE_ADD) ? 1 : 0;
             dim3 grid((d.vol_z + 127) / 128, d.vol_x, d.vol_y);
-            const float4 *c0 = need[0] ? cacc[0].as<float4>() : nullptr;
-            const float4 *c1 = need[1] ? cacc[1].as<float4>() : nullptr;
+            const float4 *c0 = need[0] && !slab[0] ? cacc[0].as<float4>() : nullptr;
+            const float4 *c1 = need[1] && !slab[1] ? cacc[1].as<float4>() : nullptr;
             const float *az = need[2] ? sz.as<float>() : nullptr;
+            const float *m0 = slab[0] ? macc[0].as<float>() : nullptr;
+            const float *m1 = slab[1] ? macc[1].as<float>() : nullptr;
+            long long ay0 = 0, ay1 = 0, mz = 0;
+            matched_slab_dims(d, 0, ay0, mz);
+            matched_slab_dims(d, 1, ay1, mz);
             if (dtype == B2T_F32)
-                fold_cells<float><<<grid, 128, 0, s>>>(c0, c1, az, d.vol_x, d.vol_y, d.vol_z,
+                fold_cells<float><<<grid, 128, 0, s>>>(c0, c1, az, m0, m1, ay0, ay1, mz, d.vol_x, d.vol_y, d.vol_z,
                                                        static_cast<float *>(vol), vol_pitch, accumulate);
             else if (dtype == B2T_F16)
-                fold_cells<__half><<<grid, 128, 0, s>>>(c0, c1, az, d.vol_x, d.vol_y, d.vol_z,
-                                                        static_cast<__half *>(vol), vol_pitch, accumulate);
+                fold_cells<__half><<<grid, 128, 0, s>>>(c0, c1, az, m0, m1, ay0, ay1, mz, d.vol_x, d.vol_y,
+                                                        d.vol_z, static_cast<__half *>(vol), vol_pitch, accumulate);
             else
-                fold_cells<__nv_bfloat16><<<grid, 128, 0, s>>>(c0, c1, az, d.vol_x, d.vol_y, d.vol_z,
-                                                               static_cast<__nv_bfloat16 *>(vol), vol_pitch,
-                                                               accumulate);
+                fold_cells<__nv_bfloat16><<<grid, 128, 0, s>>>(c0, c1, az, m0, m1, ay0, ay1, mz, d.vol_x, d.vol_y,
+                                                               d.vol_z, static_cast<__nv_bfloat16 *>(vol),
+                                                               vol_pitch, accumulate);
             count_launches(1);
             B2T_CUDA_TRY(cudaGetLastError(), "matched bp fold launch");
             return B2T_OK;

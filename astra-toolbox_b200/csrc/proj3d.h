@@ -162,6 +162,19 @@ b2t_status fp_slab_project(const b2t_geom3d *g, const b2t_params3d *p, const voi
 b2t_status fp_slab_errors(uint32_t *flags);
 b2t_status fp_path_stats_impl(uint64_t *stats);
 unsigned long long fp_cell_launches_take();
+
+// The slab FP's transpose (fp3d_slab.cu), the matched BP of the views the
+// slab FP takes (any projection storage type): scatters into an FP32
+// accumulator of matched_slab_acc_bytes (zeroed by the caller), cell (s, k1,
+// k2) at (s * ay + k1 + 2) * az + k2 + 2 with (ay, az) from matched_slab_dims.
+bool matched_slab_eligible(const b2t_geom3d *g, const b2t_params3d *p, int dir, const std::vector<int> &dirs);
+void matched_slab_dims(const b2t_dims3d &d, int dir, long long &ay, long long &az);
+size_t matched_slab_acc_bytes(const b2t_dims3d &d, int dir);
+b2t_status matched_slab_scatter(const b2t_geom3d *g, const b2t_params3d *p, const void *proj, size_t proj_pitch,
+                                int32_t dtype, int dir, const std::vector<int> &dirs, float *acc, cudaStream_t s);
+b2t_status matched_path_stats_impl(uint64_t *stats);
+// launches of matched.cu's scatter kernels since the last call
+unsigned long long matched_scatter_launches_take();
 // proj (=|+=) FP of the volume the cells hold, for the views of g (same
 // volume dimensions as at build time; every view's marching axis built).
 b2t_status fp3d_cells_project(const b2t_geom3d *g, const b2t_params3d *p, const FPCells &c, void *proj,

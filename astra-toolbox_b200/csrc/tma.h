@@ -2,7 +2,8 @@
 // the host-side tensor-map encoder (cuTensorMapEncodeTiled, fetched from the
 // driver at run time so the library does not link libcuda directly).
 //
-// Only plain TMA tile loads are used: no .multicast::cluster form anywhere.
+// Only plain TMA tile loads and tile reduce-adds are used: no
+// .multicast::cluster form anywhere.
 #pragma once
 
 #include <cuda.h>
@@ -128,6 +129,31 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
         "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
         : "memory");
 }
+
+// Element-wise add of a shared-memory box into the tensor at (c0, c1, c2)
+// (cp.reduce.async.bulk.tensor, .add, FP32 in the tensor map), tracked by
+// the issuing thread's bulk groups.  The box must lie inside the tensor and
+// c0 x the element size be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_reduce_add_3d(const CUtensorMap *map, const void *src, int c0, int c1, int c2)
+{
+    asm volatile(
+        "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+            reinterpret_cast<uint64_t>(map)),
+        "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit_group() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// Wait until at most N of this thread's bulk groups still read their
+// shared-memory source (the source may then be overwritten).
+template <int N> __device__ __forceinline__ void bulk_wait_group_read()
+{
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+// Wait until every bulk group of this thread has completed (writes included).
+__device__ __forceinline__ void bulk_wait_group_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void tma_prefetch_map(const CUtensorMap *map)
 {

@@ -934,7 +934,7 @@ def run_workload(args):
 
 
 def run_extra(args):
-    """--workload stream | sart2d | cyl.
+    """--workload stream | sart2d | cyl | matched.
 
     stream: FP + BP of the cone workload from pinned host memory through a
     device budget (--budget-gb, default 4) that forces z-slabs and angle
@@ -946,7 +946,13 @@ def run_extra(args):
     384 detectors), sequential order, CUDA-graph steps; one step = one sweep
     (180 single-view updates); metric sweeps/s.
     cyl: cyl_cone_vec FP + BP, 256^3 volume, 360 views, 256 x 384 detector on
-    a cylinder centred at the source; metric GUPS of the pair."""
+    a cylinder centred at the source; metric GUPS of the pair.
+    matched: the exact transpose of the FP (projection kernel matched_bp, the
+    autograd backward) on the cone workload; one step = one matched BP of the
+    phantom's projections; metric GUPS (Nx Ny Nz Nangles / time), with the
+    dot-product test <A x, y> = <x, A^T y> (FP64 sums) of this run's output
+    and the path statistics (B2T_MATCHED_PATH=slab selects the slab
+    transpose)."""
     import torch
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -1038,6 +1044,37 @@ def run_extra(args):
                  "sweeps_before_residual": args.warmup + args.steps}
         cfgd = {"workload": "SART_CUDA, 256^2 parallel beam, 180 views over pi, 384 detectors, 10 seeded ellipses, "
                             "sequential order", "workload_kind": "sart2d"}
+    elif args.workload == "matched":
+        astra, vg, pg = workload(args.n, args.views, args.det)
+        pr = astra.Projector3D(pg, vg, {'ProjectionKernel': 'matched_bp'})
+        vol = ph.ellipsoids(pr.vol_shape, N_ELL, seed=0, device=dev)
+        proj = torch.zeros(pr.proj_shape, device=dev)
+        pr.fp(vol, proj)
+        rec = torch.zeros(pr.vol_shape, device=dev)
+        for _ in range(args.warmup):
+            pr.bp(proj, rec)
+        st = (ctypes.c_uint64 * 4)()
+        lib.b2t_matched_path_stats(st)
+        sampler.start()
+        time.sleep(0.3)
+        l0 = lib.b2t_kernel_launches()
+        ms = _timed_region(torch, stream, lambda: pr.bp(proj, rec), args.steps)
+        launches = lib.b2t_kernel_launches() - l0
+        clocks = sampler.stop()
+        lib.b2t_matched_path_stats(st)
+        x = ph.ellipsoids(pr.vol_shape, N_ELL, seed=1, device=dev)
+        ax = torch.zeros(pr.proj_shape, device=dev)
+        pr.fp(x, ax)
+        lhs = float(torch.sum(ax.double() * proj.double()))
+        rhs = float(torch.sum(x.double() * rec.double()))
+        ups = float(np.prod(pr.vol_shape)) * pr.proj_shape[1]
+        value, unit, hib = ups / (ms * 1e-3) / 1e9, "GUPS", True
+        metric = "matched BP (exact FP transpose) GUPS at %d^3x%d" % (args.n, args.views)
+        path = "slab" if os.environ.get("B2T_MATCHED_PATH") == "slab" else "scatter"
+        extra = {"path": path, "dot_test_rel": abs(lhs - rhs) / abs(lhs),
+                 "path_stats": {"slices_in_smem": int(st[0]), "slices_global": int(st[1]),
+                                "slab_launches": int(st[2]), "scatter_launches": int(st[3])}}
+        cfgd = config_dict(args.n, args.views, args.det, {"workload_kind": "matched"})
     else:
         n, na, rows, cols = 256, 360, 256, 384
         sod, odd = 600.0, 300.0
@@ -1103,7 +1140,8 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=30,
                     help="iterations of the reference's SIRT3D / CGLS3D whose residual is the target")
     ap.add_argument("--workload", default="fpbp",
-                    choices=["fpbp", "fdk", "sirt3d", "cgls3d", "batch2d", "stream", "sart2d", "cyl", "c1", "c5"])
+                    choices=["fpbp", "fdk", "sirt3d", "cgls3d", "batch2d", "stream", "sart2d", "cyl", "c1", "c5",
+                             "matched"])
     ap.add_argument("--c5-views", type=int, default=1500)
     ap.add_argument("--c5-iters", type=int, default=30)
     ap.add_argument("--c5-types", default="f32,f16,bf16")
@@ -1119,7 +1157,7 @@ def main():
         return run_c1(args)
     if args.workload == "c5":
         return run_c5(args)
-    if args.workload in ("stream", "sart2d", "cyl"):
+    if args.workload in ("stream", "sart2d", "cyl", "matched"):
         return run_extra(args)
     if args.workload != "fpbp":
         return run_workload(args)

@@ -83,6 +83,15 @@ b2t_status b2t_bp_path_stats(uint64_t stats[4]);
  * not take).  Synchronises the device.  A performance diagnostic; the
  * reference has no counterpart. */
 b2t_status b2t_fp_path_stats(uint64_t stats[4]);
+/* Read and clear the path statistics of the matched (exact-transpose)
+ * backprojection since the last call: stats[0] slices whose accumulation box
+ * CTAs of the slab transpose kept in shared memory, stats[1] slices they
+ * scattered straight into global memory (a box too large for a slice
+ * buffer), stats[2] slab transpose launches, stats[3] launches of the
+ * per-sample scatter kernels (views the slab transpose does not take).
+ * Synchronises the device.  A performance diagnostic; the reference has no
+ * counterpart. */
+b2t_status b2t_matched_path_stats(uint64_t stats[4]);
 
 /* Failure-handling test hooks; the reference has no counterpart.
  * b2t_debug_fail_alloc(n), n >= 1: the n-th device allocation the library

@@ -176,15 +176,19 @@ def test_matched_bp_is_exact_transpose(astra, orc, idx):
     assert abs(lhs - rhs) / abs(lhs) < 1e-5, (lhs, rhs)
 
 
-@pytest.mark.parametrize("plain", [False, True])
-def test_matched_bp_fine_detector(astra, orc, plain, monkeypatch):
+@pytest.mark.parametrize("path", ["merged", "plain", "slab"])
+def test_matched_bp_fine_detector(astra, orc, path, monkeypatch):
     """Matched BP with a detector finer than the voxels (pixel 0.25 at
     magnification ~2: about four rays per cell along a detector column), so
     runs of three or more lanes fall on one cell in the merged reductions;
     B2T_MATCHED_PLAIN=1 forces the per-lane reductions of very large
-    arrays.  Against the oracle's transpose and the dot-product test."""
-    if plain:
+    arrays, B2T_MATCHED_PATH=slab the slab transpose (lanes of one shared-
+    memory reduction on one cell).  Against the oracle's transpose and the
+    dot-product test."""
+    if path == "plain":
         monkeypatch.setenv("B2T_MATCHED_PLAIN", "1")
+    if path == "slab":
+        monkeypatch.setenv("B2T_MATCHED_PATH", "slab")
     ang = np.linspace(0, 2 * np.pi, 12, endpoint=False).astype(np.float32)
     vg = astra.create_vol_geom(24, 28, 20)
     pg = astra.create_proj_geom('cone', 0.25, 0.25, 160, 180, ang, 60.0, 60.0)
@@ -442,6 +446,78 @@ def test_slab_fp_vs_oracle_and_cells(astra, orc, case, monkeypatch):
     import importlib
     assert importlib.import_module("astra-toolbox_b200._lib").load().b2t_device_errors(ctypes.byref(flags)) == 0
     assert flags.value == 0
+
+
+def _mt_stats():
+    import importlib
+    L = importlib.import_module("astra-toolbox_b200._lib")
+    out = (ctypes.c_uint64 * 4)()
+    assert L.load().b2t_matched_path_stats(out) == 0
+    return list(out)
+
+
+@pytest.mark.parametrize("case", ["cone", "parallel3d", "oblique", "high_mag", "many_views", "odd"])
+def test_slab_matched_bp_vs_oracle_and_scatter(astra, orc, case, monkeypatch):
+    """The slab FP's transpose (B2T_MATCHED_PATH=slab: shared-memory boxes
+    per slice, TMA reduce-adds into the accumulator) against the FP64
+    oracle's transpose, against the default per-sample scatter kernels and
+    by the dot-product test with the slab FP; boxes too large for a buffer
+    scatter straight into global memory (high_mag); ADD mode."""
+    vg, pg = _slab_cases(astra)[case]
+    pr = _proj(astra, vg, pg, {'ProjectionKernel': 'matched_bp'})
+    rng = np.random.default_rng(41)
+    proj = rng.standard_normal(pr.proj_shape).astype(np.float32)
+    tp = torch.from_numpy(proj).cuda()
+    _mt_stats()
+    b = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(tp, b)
+    assert _mt_stats()[2] == 0
+    monkeypatch.setenv("B2T_MATCHED_PATH", "slab")
+    a = torch.zeros(pr.vol_shape, device='cuda')
+    pr.bp(tp, a)
+    staged, glob, slab_launches, scatter_launches = _mt_stats()
+    assert slab_launches >= 1 and scatter_launches == 0, (case, slab_launches, scatter_launches)
+    if case == "high_mag":
+        assert glob > 0
+    else:
+        assert staged > 0, (staged, glob)
+    ref = orc.fp3d_transpose(_oracle_kind(pr), pr.geom.views_array(), proj, pr.vol_shape, pr.geom.vol_scale)
+    assert rel_l2(a.cpu().numpy(), ref) < TOL_F32, case
+    assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 2e-6, case
+    x = rng.standard_normal(pr.vol_shape).astype(np.float32)
+    ax = torch.zeros(pr.proj_shape, device='cuda')
+    _fp_stats()
+    pr.fp(torch.from_numpy(x).cuda(), ax)
+    assert _fp_stats()[2] >= 1
+    lhs = float(np.dot(ax.cpu().numpy().ravel().astype(np.float64), proj.ravel().astype(np.float64)))
+    rhs = float(np.dot(x.ravel().astype(np.float64), a.cpu().numpy().ravel().astype(np.float64)))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5, (lhs, rhs)
+    c = a.clone()
+    pr.bp(tp, c, mode=0)
+    assert rel_l2(c.cpu().numpy(), 2 * a.cpu().numpy()) < 2e-6
+    flags = ctypes.c_uint32(1)
+    import importlib
+    assert importlib.import_module("astra-toolbox_b200._lib").load().b2t_device_errors(ctypes.byref(flags)) == 0
+    assert flags.value == 0
+
+
+@pytest.mark.parametrize("dtype,tol", [("float16", 1e-3), ("bfloat16", 8e-3)])
+def test_slab_matched_bp_16bit(astra, dtype, tol, monkeypatch):
+    """16-bit projections and volume through the slab transpose
+    (B2T_MATCHED_PATH=slab): the same sums as the scatter kernels up to the
+    rounding of the 16-bit output."""
+    vg, pg = _slab_cases(astra)["cone"]
+    pr = _proj(astra, vg, pg, {'ProjectionKernel': 'matched_bp'})
+    tdt = getattr(torch, dtype)
+    tp = torch.from_numpy(np.random.default_rng(42).random(pr.proj_shape, dtype=np.float32)).cuda().to(tdt)
+    b = torch.zeros(pr.vol_shape, device='cuda', dtype=tdt)
+    pr.bp(tp, b)
+    monkeypatch.setenv("B2T_MATCHED_PATH", "slab")
+    _mt_stats()
+    a = torch.zeros(pr.vol_shape, device='cuda', dtype=tdt)
+    pr.bp(tp, a)
+    assert _mt_stats()[2] >= 1
+    assert rel_l2(a.float().cpu().numpy(), b.float().cpu().numpy()) < tol
 
 
 @pytest.mark.parametrize("dtype", ["float32", "float16"])
