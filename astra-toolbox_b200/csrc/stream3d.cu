@@ -263,6 +263,21 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
         else return bs;
     }
 
+    // The BP's last angle block of a job runs in z-chunks, each downloaded as
+    // soon as it is final, so that the volume's download overlaps the last
+    // block's compute instead of following it (projections padded once).
+    const bool split_tail = R.op == Op::bp && R.params.kernel == B2T_KER_DEFAULT &&
+                            R.params.voxel_supersample >= 1 && R.params.voxel_supersample <= 16;
+    DevBuf tailpad;
+    if (split_tail) {
+        b2t_dims3d db = d;
+        db.angles = R.block;
+        B2T_TRY(tailpad.alloc(padded_proj_bytes(db, B2T_F32, false), cs.s, "streamed BP padded block"));
+    }
+    std::vector<Event> tail_ev(8);
+    for (Event &e : tail_ev) B2T_CUDA_TRY(cudaEventCreateWithFlags(&e.e, cudaEventDisableTiming), "event create");
+    const size_t plane = (size_t)d.vol_x * d.vol_y;
+
     SubGeom sub;
     for (size_t jn = 0; jn < jobs.size(); ++jn) {
         const uint32_t j = jobs[jn];
@@ -286,6 +301,7 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
             B2T_CUDA_TRY(cudaStreamWaitEvent(cs.s, got.e, 0), "wait");
         }
         if (!resident) B2T_TRY(upload(0, 0));
+        bool downloaded = false;
         for (uint32_t c = 0; c < nin; ++c) {
             const int ib = resident ? 0 : (int)(c & 1);
             if (!resident && c + 1 < nin) B2T_TRY(upload(c + 1, (int)((c + 1) & 1)));
@@ -298,6 +314,21 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
                 sub.set(G, o0, on, c0, cn);
                 if (have_cells) B2T_TRY(fp3d_cells_project(&sub.g, &R.params, cells, obuf, 0, mode, cs.s));
                 else B2T_TRY(fp3d_impl(&sub.g, &R.params, inb[ib].f(), 0, obuf, 0, B2T_F32, mode, cs.s));
+            } else if (R.op == Op::bp && split_tail && c + 1 == nin) {
+                sub.set(G, c0, cn, o0, on);
+                B2T_TRY(pad_projections_impl(inb[ib].f(), d.det_u, sub.g.dims, tailpad.p, B2T_F32, false, cs.s));
+                const uint32_t nch = std::min<uint32_t>((uint32_t)tail_ev.size(), std::max<uint32_t>(1, on / 16));
+                const uint32_t zc = (on + nch - 1) / nch;
+                for (uint32_t k = 0; k * zc < on; ++k) {
+                    const uint32_t z0 = o0 + k * zc, nz = std::min(zc, o0 + on - z0);
+                    sub.set(G, c0, cn, z0, nz);
+                    float *part = obuf + (size_t)(z0 - o0) * plane;
+                    B2T_TRY(bp3d_from_padded(&sub.g, &R.params, tailpad.p, part, 0, B2T_F32, mode, cs.s));
+                    B2T_CUDA_TRY(cudaEventRecord(tail_ev[k].e, cs.s), "event record");
+                    B2T_CUDA_TRY(cudaStreamWaitEvent(os.s, tail_ev[k].e, 0), "wait");
+                    B2T_TRY(copy_slab(R.out, part, d, z0, nz, false, os.s));
+                }
+                downloaded = true;
             } else if (R.op == Op::bp) {
                 sub.set(G, c0, cn, o0, on);
                 B2T_TRY(bp3d_impl(&sub.g, &R.params, inb[ib].f(), 0, obuf, 0, B2T_F32, mode, cs.s));
@@ -320,7 +351,7 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
         B2T_CUDA_TRY(cudaEventRecord(out_done[ob].e, cs.s), "event record");
         B2T_CUDA_TRY(cudaStreamWaitEvent(os.s, out_done[ob].e, 0), "wait");
         if (fp) B2T_TRY(copy_block(R.out, obuf, d, o0, on, false, os.s));
-        else B2T_TRY(copy_slab(R.out, obuf, d, o0, on, false, os.s));
+        else if (!downloaded) B2T_TRY(copy_slab(R.out, obuf, d, o0, on, false, os.s));
         B2T_CUDA_TRY(cudaEventRecord(out_copied[ob].e, os.s), "event record");
     }
     for (Stream *st : {&cs, &hs, &os}) B2T_CUDA_TRY(cudaStreamSynchronize(st->s), "stream worker synchronize");
