@@ -69,8 +69,9 @@ static __device__ unsigned long long g_mt_slab_slices[2] = {0, 0};
 namespace {
 
 constexpr int SLAB_W = 2;                   // views per CTA (every warp traces both)
-constexpr int SLAB_U = 14;                  // detector columns per CTA, one compute warp each
-constexpr int SLAB_R = 4;                   // rows per lane and view: v, v + 32, ...
+constexpr int SLAB_U = 11;                  // detector columns per CTA, one compute warp each
+constexpr int SLAB_R = 5;                   // rows per lane and view: v, v + 32, ... (384 threads:
+                                            // 80 registers at two CTAs per SM, no spills)
 constexpr int SLAB_ROWS = 32 * SLAB_R;      // detector rows per CTA
 constexpr int SLAB_WARPS = SLAB_U;          // compute warps; one more produces
 constexpr int SLAB_THREADS = 32 * (SLAB_WARPS + 1);
@@ -456,6 +457,20 @@ __device__ __forceinline__ bool slab_consume(const SlabLaunch &L, const float2 *
     return true;
 }
 
+// slab_consume for the rows in use, re in [1, RE]
+template <int RE>
+__device__ __forceinline__ bool slab_consume_rows(int re, const SlabLaunch &L, const float2 *buf, uint64_t *full,
+                                                  uint64_t *empty, const SlabInfo *info, int lane, const Range &rg,
+                                                  Rays &R)
+{
+    if constexpr (RE == 1) {
+        return slab_consume<1>(L, buf, full, empty, info, lane, rg, R);
+    } else {
+        if (re >= RE) return slab_consume<RE>(L, buf, full, empty, info, lane, rg, R);
+        return slab_consume_rows<RE - 1>(re, L, buf, full, empty, info, lane, rg, R);
+    }
+}
+
 __global__ void __launch_bounds__(SLAB_THREADS, 2) fp3d_slab_kernel(const __grid_constant__ SlabLaunch L)
 {
     extern __shared__ __align__(1024) unsigned char smraw[];
@@ -532,10 +547,7 @@ __global__ void __launch_bounds__(SLAB_THREADS, 2) fp3d_slab_kernel(const __grid
     const int re = min(SLAB_R, (L.nv - (int)blockIdx.z * SLAB_ROWS + 31) >> 5);
     const Range rg{s_lo, s_hi, wlo, whi, ilo, ihi};
     bool ok;
-    if (re >= 4) ok = slab_consume<4>(L, buf, full, empty, info, lane, rg, R);
-    else if (re == 3) ok = slab_consume<3>(L, buf, full, empty, info, lane, rg, R);
-    else if (re == 2) ok = slab_consume<2>(L, buf, full, empty, info, lane, rg, R);
-    else ok = slab_consume<1>(L, buf, full, empty, info, lane, rg, R);
+    ok = slab_consume_rows<SLAB_R>(re, L, buf, full, empty, info, lane, rg, R);
     if (!ok || u_raw >= L.nu) return;
     // ---- results
 #pragma unroll
@@ -863,6 +875,20 @@ __device__ __forceinline__ bool mt_consume(const SlabLaunch &L, const float *buf
     return true;
 }
 
+// mt_consume for the rows in use, re in [1, RE]
+template <int RE>
+__device__ __forceinline__ bool mt_consume_rows(int re, const SlabLaunch &L, const float *buf, uint64_t *ready,
+                                                uint64_t *done, const MTInfo *info, int lane, const Range &rg,
+                                                const TRays &R)
+{
+    if constexpr (RE == 1) {
+        return mt_consume<1>(L, buf, ready, done, info, lane, rg, R);
+    } else {
+        if (re >= RE) return mt_consume<RE>(L, buf, ready, done, info, lane, rg, R);
+        return mt_consume_rows<RE - 1>(re, L, buf, ready, done, info, lane, rg, R);
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(SLAB_THREADS, 2) bp3d_slab_matched_kernel(const __grid_constant__ SlabLaunch L)
 {
@@ -942,10 +968,7 @@ __global__ void __launch_bounds__(SLAB_THREADS, 2) bp3d_slab_matched_kernel(cons
     }
     const int re = min(SLAB_R, (L.nv - (int)blockIdx.z * SLAB_ROWS + 31) >> 5);
     const Range rg{s_lo, s_hi, wlo, whi, ilo, ihi};
-    if (re >= 4) (void)mt_consume<4>(L, buf, ready, done, info, lane, rg, R);
-    else if (re == 3) (void)mt_consume<3>(L, buf, ready, done, info, lane, rg, R);
-    else if (re == 2) (void)mt_consume<2>(L, buf, ready, done, info, lane, rg, R);
-    else (void)mt_consume<1>(L, buf, ready, done, info, lane, rg, R);
+    (void)mt_consume_rows<SLAB_R>(re, L, buf, ready, done, info, lane, rg, R);
 }
 
 // Slab copy of marching axis dir (0: slices along x, in-plane axis y; 1:

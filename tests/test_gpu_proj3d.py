@@ -406,10 +406,12 @@ def _slab_cases(astra):
         # odd sizes, anisotropic voxels
         "odd": (astra.create_vol_geom(17, 23, 9, -9.0, 8.0, -11.0, 12.0, -3.0, 3.0),
                 astra.create_proj_geom('cone', 0.7, 1.3, 13, 21, ang + 0.1, 70.0, 30.0)),
+        # a detector taller than two CTAs' rows: full row blocks and a partial one
+        "tall": (astra.create_vol_geom(32, 36, 60), astra.create_proj_geom('cone', 1.0, 0.4, 44, 340, ang, 150.0, 80.0)),
     }
 
 
-@pytest.mark.parametrize("case", ["cone", "parallel3d", "oblique", "high_mag", "many_views", "odd"])
+@pytest.mark.parametrize("case", ["cone", "parallel3d", "oblique", "high_mag", "many_views", "odd", "tall"])
 def test_slab_fp_vs_oracle_and_cells(astra, orc, case, monkeypatch):
     """The TMA-staged slab FP (the default for x- and y-major views of
     circular orbits) against the FP64 oracle and against the cell kernels:
@@ -456,7 +458,7 @@ def _mt_stats():
     return list(out)
 
 
-@pytest.mark.parametrize("case", ["cone", "parallel3d", "oblique", "high_mag", "many_views", "odd"])
+@pytest.mark.parametrize("case", ["cone", "parallel3d", "oblique", "high_mag", "many_views", "odd", "tall"])
 def test_slab_matched_bp_vs_oracle_and_scatter(astra, orc, case, monkeypatch):
     """The slab FP's transpose (B2T_MATCHED_PATH=slab: shared-memory boxes
     per slice, TMA reduce-adds into the accumulator) against the FP64
