@@ -1385,13 +1385,20 @@ def main():
         peak_on = onchip["smem"]
     alg_bytes = units * 4 * esz
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
-    # DRAM bytes (read + write) of the dominant call's launches, from one ncu
-    # capture of this exact workload (dram__bytes_read.sum + write.sum, one
-    # pass; profiles/dram_traffic_cone_fpbp_512cube_720views.md); null for
-    # other workloads, which were not captured
-    traffic = None
+    # DRAM bytes (read + write) of the dominant call's launches, per call.
+    # FP: the bytes per sample of one ncu capture of the FP kernel at 384^3 x
+    # 360 views, 624^2 (21.43 GB for 744.6 M warp-samples of 32 rays; profiles/
+    # cone_fp_slab_384cube_360views.md) times this call's samples; BP: one
+    # capture of this exact workload (profiles/dram_traffic_cone_fpbp_512cube_
+    # 720views.md).  Null for other workloads and storage types.
+    traffic, traffic_src = None, None
     if (args.n, args.views, args.det, args.dtype) == (N_VOX, N_ANG, N_DET, "float32"):
-        traffic = {"fp": (82.59 + 1.57 + 77.28 + 1.55) * 1e9, "bp": (15.87 + 0.53 + 0.95 + 0.50) * 1e9}[dom]
+        if dom == "fp":
+            traffic = (20.96 + 0.47) * 1e9 / (744633280.0 * 32) * units
+            traffic_src = "scaled by samples from an ncu capture of the FP at 384^3 x 360 views, 624^2"
+        else:
+            traffic = (15.87 + 0.53 + 0.95 + 0.50) * 1e9
+            traffic_src = "ncu capture of this workload"
     hbm_achieved = hbm_bytes / (dom_ms * 1e-3) / 1e9
     roofline = {"bound": "l1" if dom == "fp" else "smem",
                 "kernel": "b2t_fp3d" if dom == "fp" else "b2t_bp3d",
@@ -1399,9 +1406,8 @@ def main():
                 "frac": (achieved / peak_on) if peak_on else None,
                 "traffic": traffic, "units_per_launch": units, "bytes_per_unit": 4 * esz,
                 "traffic_note": "DRAM bytes of one whole call (the FP's x- and y-major launches, or the BP's "
-                                "launches) from one ncu capture of this workload; the "
-                                "slice boxes / tiles are re-read on chip, DRAM moves ~1/25 of the algorithmic "
-                                "bytes",
+                                "launch), %s; the slice boxes / tiles are re-read on chip, DRAM moves about "
+                                "1/18 of the algorithmic bytes" % traffic_src,
                 "peak_source": "measured on this GPU by b2t_onchip_peak (16-byte streaming loads); the FP "
                                "reads its samples from TMA-staged shared memory, whose measured roof is "
                                "within 1 % of the L1 one",
