@@ -335,18 +335,22 @@ template <int P, bool CLAMP, int RE>
 __device__ __forceinline__ void sample_smem(const SlabLaunch &L, uint32_t rb, float sf, Rays &R)
 {
     constexpr uint32_t ROWB = 8u * P;
+    static_assert(SLAB_W == 2, "the two views' in-plane splits share packed instructions");
+    const uint64_t sf2 = pk2(sf, sf), M2 = pk2(SPLIT_M, SPLIT_M), nM2 = pk2(-SPLIT_M, -SPLIT_M);
+    // both views' in-plane position, split and weights in packed f32x2
+    // (130.8 against 133.1 ms one view at a time at 512^3 x 720, same bits)
+    const uint64_t q1p = fma2(pk2(R.A1[0], R.A1[1]), sf2, pk2(R.B1h[0], R.B1h[1]));
+    const uint64_t t1p = add2_rd(q1p, M2);
+    const uint64_t f1p = sub2(q1p, add2(t1p, nM2));
+    const float2 t1u = upk2(t1p), f1u = upk2(f1p), g1u = upk2(sub2(pk2(1.0f, 1.0f), f1p));
 #pragma unroll
     for (int w = 0; w < SLAB_W; ++w) {
-        const float q1 = fmaf(R.A1[w], sf, R.B1h[w]);
-        const float t1 = __fadd_rd(q1, SPLIT_M);
-        const float f1 = q1 - (t1 - SPLIT_M);
-        const float g1 = 1.0f - f1;
-        int b1 = __float_as_int(t1);
+        const float f1 = w == 0 ? f1u.x : f1u.y, g1 = w == 0 ? g1u.x : g1u.y;
+        int b1 = __float_as_int(w == 0 ? t1u.x : t1u.y);
         if (CLAMP) b1 = min(max(b1, SPLIT_BITS - 2), SPLIT_BITS + L.n1);
         const uint32_t row = (uint32_t)b1 * ROWB + rb;
         // rows r, r + 1 in the two halves of packed f32x2 operations (each
         // half rounds as the scalar form of the odd row below)
-        const uint64_t sf2 = pk2(sf, sf), M2 = pk2(SPLIT_M, SPLIT_M), nM2 = pk2(-SPLIT_M, -SPLIT_M);
         const uint64_t f12 = pk2(f1, f1), g12 = pk2(g1, g1);
 #pragma unroll
         for (int r = 0; r + 1 < RE; r += 2) {

@@ -263,13 +263,16 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
         else return bs;
     }
 
-    // The BP's last angle block of a job runs in z-chunks, each downloaded as
-    // soon as it is final, so that the volume's download overlaps the last
-    // block's compute instead of following it (projections padded once).
-    const bool split_tail = R.op == Op::bp && R.params.kernel == B2T_KER_DEFAULT &&
-                            R.params.voxel_supersample >= 1 && R.params.voxel_supersample <= 16;
+    // The BP's and FDK's last angle block of a job runs in z-chunks, each
+    // downloaded as soon as it is final, so that the volume's download
+    // overlaps the last block's compute instead of following it (projections
+    // padded, or weighted and filtered, once).
+    const bool split_tail = (R.op == Op::bp && R.params.kernel == B2T_KER_DEFAULT &&
+                             R.params.voxel_supersample >= 1 && R.params.voxel_supersample <= 16) ||
+                            (R.op == Op::fdk && R.params.voxel_supersample >= 1 &&
+                             R.params.voxel_supersample <= 16);
     DevBuf tailpad;
-    if (split_tail) {
+    if (split_tail && R.op == Op::bp) {
         b2t_dims3d db = d;
         db.angles = R.block;
         B2T_TRY(tailpad.alloc(padded_proj_bytes(db, B2T_F32, false), cs.s, "streamed BP padded block"));
@@ -277,8 +280,25 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
     std::vector<Event> tail_ev(8);
     for (Event &e : tail_ev) B2T_CUDA_TRY(cudaEventCreateWithFlags(&e.e, cudaEventDisableTiming), "event create");
     const size_t plane = (size_t)d.vol_x * d.vol_y;
-
     SubGeom sub;
+    // BP of views [c0, c0 + cn) from a padded block into slab [o0, o0 + on)
+    // of obuf in z-chunks, each downloaded once computed
+    auto bp_tail = [&](const void *pad, const b2t_params3d &p, uint32_t c0, uint32_t cn, uint32_t o0, uint32_t on,
+                       float *obuf, int32_t mode) -> b2t_status {
+        const uint32_t nch = std::min<uint32_t>((uint32_t)tail_ev.size(), std::max<uint32_t>(1, on / 16));
+        const uint32_t zc = (on + nch - 1) / nch;
+        for (uint32_t k = 0; k * zc < on; ++k) {
+            const uint32_t z0 = o0 + k * zc, nz = std::min(zc, o0 + on - z0);
+            sub.set(G, c0, cn, z0, nz);
+            float *part = obuf + (size_t)(z0 - o0) * plane;
+            B2T_TRY(bp3d_from_padded(&sub.g, &p, pad, part, 0, B2T_F32, mode, cs.s));
+            B2T_CUDA_TRY(cudaEventRecord(tail_ev[k].e, cs.s), "event record");
+            B2T_CUDA_TRY(cudaStreamWaitEvent(os.s, tail_ev[k].e, 0), "wait");
+            B2T_TRY(copy_slab(R.out, part, d, z0, nz, false, os.s));
+        }
+        return B2T_OK;
+    };
+
     for (size_t jn = 0; jn < jobs.size(); ++jn) {
         const uint32_t j = jobs[jn];
         uint32_t o0 = j * out_step, on = std::min(out_step, out_n - std::min(o0, out_n));
@@ -317,17 +337,7 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
             } else if (R.op == Op::bp && split_tail && c + 1 == nin) {
                 sub.set(G, c0, cn, o0, on);
                 B2T_TRY(pad_projections_impl(inb[ib].f(), d.det_u, sub.g.dims, tailpad.p, B2T_F32, false, cs.s));
-                const uint32_t nch = std::min<uint32_t>((uint32_t)tail_ev.size(), std::max<uint32_t>(1, on / 16));
-                const uint32_t zc = (on + nch - 1) / nch;
-                for (uint32_t k = 0; k * zc < on; ++k) {
-                    const uint32_t z0 = o0 + k * zc, nz = std::min(zc, o0 + on - z0);
-                    sub.set(G, c0, cn, z0, nz);
-                    float *part = obuf + (size_t)(z0 - o0) * plane;
-                    B2T_TRY(bp3d_from_padded(&sub.g, &R.params, tailpad.p, part, 0, B2T_F32, mode, cs.s));
-                    B2T_CUDA_TRY(cudaEventRecord(tail_ev[k].e, cs.s), "event record");
-                    B2T_CUDA_TRY(cudaStreamWaitEvent(os.s, tail_ev[k].e, 0), "wait");
-                    B2T_TRY(copy_slab(R.out, part, d, z0, nz, false, os.s));
-                }
+                B2T_TRY(bp_tail(tailpad.p, R.params, c0, cn, o0, on, obuf, mode));
                 downloaded = true;
             } else if (R.op == Op::bp) {
                 sub.set(G, c0, cn, o0, on);
@@ -343,7 +353,12 @@ b2t_status run_worker(const Req &R, int device, const std::vector<uint32_t> &job
                 b2t_params3d p = R.params;
                 p.kernel = B2T_KER_FDK_WEIGHTING;
                 p.output_scale = R.fdk_scale;
-                B2T_TRY(bp3d_from_padded(&sub.g, &p, padded.p, obuf, 0, B2T_F32, mode, cs.s));
+                if (split_tail && c + 1 == nin) {
+                    B2T_TRY(bp_tail(padded.p, p, c0, cn, o0, on, obuf, mode));
+                    downloaded = true;
+                } else {
+                    B2T_TRY(bp3d_from_padded(&sub.g, &p, padded.p, obuf, 0, B2T_F32, mode, cs.s));
+                }
             }
             if (!resident) B2T_CUDA_TRY(cudaEventRecord(in_free[ib].e, cs.s), "event record");
         }
