@@ -491,9 +491,13 @@ def test_slab_matched_bp_vs_oracle_and_scatter(astra, orc, case, monkeypatch):
     _fp_stats()
     pr.fp(torch.from_numpy(x).cuda(), ax)
     assert _fp_stats()[2] >= 1
-    lhs = float(np.dot(ax.cpu().numpy().ravel().astype(np.float64), proj.ravel().astype(np.float64)))
+    axv = ax.cpu().numpy().ravel().astype(np.float64)
+    lhs = float(np.dot(axv, proj.ravel().astype(np.float64)))
     rhs = float(np.dot(x.ravel().astype(np.float64), a.cpu().numpy().ravel().astype(np.float64)))
-    assert abs(lhs - rhs) / abs(lhs) < 1e-5, (lhs, rhs)
+    # relative to ||A x|| ||y|| (the usual scale of an adjoint test): with
+    # zero-mean inputs <A x, y> itself can cancel to far below its terms
+    scale = float(np.linalg.norm(axv) * np.linalg.norm(proj.ravel().astype(np.float64)))
+    assert abs(lhs - rhs) / scale < 1e-6, (lhs, rhs, scale)
     c = a.clone()
     pr.bp(tp, c, mode=0)
     assert rel_l2(c.cpu().numpy(), 2 * a.cpu().numpy()) < 2e-6
