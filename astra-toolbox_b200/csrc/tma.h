@@ -2,8 +2,8 @@
 // the host-side tensor-map encoder (cuTensorMapEncodeTiled, fetched from the
 // driver at run time so the library does not link libcuda directly).
 //
-// Only plain TMA tile loads and tile reduce-adds are used: no
-// .multicast::cluster form anywhere.
+// Only plain TMA tile loads and tile reduce-adds are used, none of them
+// multicast across a cluster.
 #pragma once
 
 #include <cuda.h>
